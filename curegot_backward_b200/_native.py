@@ -1,0 +1,100 @@
+"""ctypes binding of the C ABI in ``include/curegot_b200.h``.
+
+The shared library is the product: there is no CPU fallback.  Loading fails
+loudly when the library is missing, and every call that needs a GPU raises
+when CUDA is unavailable.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libcuregot_b200.so")
+
+CG_OK = 0
+CG_ERR_INVALID_ARG = 1
+CG_ERR_CUDA = 2
+CG_ERR_NOT_SPD = 3
+CG_ERR_OOM = 4
+CG_ERR_TIMEOUT = 5
+CG_ERR_NONFINITE = 6
+CG_ERR_INVALID_CONTEXT = 7
+CG_ERR_SOLVER = 8
+CG_ERR_ADMISSION = 9
+
+_STATUS_NAMES = {
+    CG_ERR_INVALID_ARG: "invalid argument",
+    CG_ERR_CUDA: "CUDA error",
+    CG_ERR_NOT_SPD: "direction-solve factorization failed (matrix not SPD)",
+    CG_ERR_OOM: "out of device memory",
+    CG_ERR_TIMEOUT: "bounded device wait expired",
+    CG_ERR_NONFINITE: "non-finite state",
+    CG_ERR_INVALID_CONTEXT: "invalid backward context",
+    CG_ERR_SOLVER: "linear solver error",
+    CG_ERR_ADMISSION: "request exceeds the engine's HBM budget",
+}
+
+_lib = None
+_lock = threading.Lock()
+
+c_int, c_double, c_void_p, c_long = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_long
+c_size_t = ctypes.c_size_t
+c_int_p = ctypes.POINTER(ctypes.c_int)
+
+# name -> argtypes (every exported entry point of include/curegot_b200.h)
+SIGNATURES = {
+    "cg_last_error": [],
+    "cg_version": [],
+    "cg_bcd_f64": [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_double, c_int,
+                   c_int, c_int_p, c_void_p, c_void_p, c_void_p],
+    "cg_bcd_mixed": [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_double, c_int,
+                     c_int, c_int_p, c_void_p, c_void_p, c_void_p],
+    "cg_transport_plan_f64": [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_int,
+                              c_void_p],
+    "cg_transport_plan_mixed": [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_int,
+                                c_void_p],
+    "cg_diag_exp2": [c_void_p, c_void_p, c_int, c_int, c_void_p],
+}
+RESTYPES = {"cg_last_error": ctypes.c_char_p, "cg_version": ctypes.c_char_p}
+
+
+class CuregotError(RuntimeError):
+    """A native entry point returned a non-zero status."""
+
+    def __init__(self, fn: str, status: int, detail: str):
+        self.status = status
+        super().__init__(f"{fn}: {_STATUS_NAMES.get(status, 'error')} (status {status})"
+                         + (f": {detail}" if detail else ""))
+
+
+def lib():
+    """Load the native library (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise ImportError(
+                    f"curegot_backward_b200: native library not found at {LIB_PATH}; "
+                    "build it with `python -m curegot_backward_b200.build`")
+            L = ctypes.CDLL(LIB_PATH)
+            for name, args in SIGNATURES.items():
+                f = getattr(L, name)
+                f.argtypes = args
+                f.restype = RESTYPES.get(name, ctypes.c_int)
+            _lib = L
+    return _lib
+
+
+def check(fn: str, status: int) -> None:
+    if status != CG_OK:
+        detail = lib().cg_last_error()
+        raise CuregotError(fn, status, detail.decode() if detail else "")
+
+
+def call(fn: str, *args) -> None:
+    check(fn, getattr(lib(), fn)(*args))

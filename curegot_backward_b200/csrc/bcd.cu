@@ -1,0 +1,680 @@
+// Sinkhorn BCD on sm_100a: streaming row / column log-sum-exp passes with
+// fused stop tests, batched over problems.
+//
+// Reference behaviour followed (benben-cd/curegot_backward):
+//   optimal_alpha_kernel / optimal_beta_kernel  src/sinkhorn_bcd_kernel.cu:35-192
+//   compute_iter_difference                     src/sinkhorn_bcd_kernel.cu:280-326
+//   compute_marginal_a_kernel + l2 distance     src/sinkhorn_bcd_kernel.cu:329-353
+//   cuda_sinkhorn_bcd loop                      src/sinkhorn_bcd_kernel.cu:532-592
+//
+// Design
+// * Each half-step reads M exactly once, coalesced, in 16-byte vectors.  The
+//   row pass is warp-per-row (up to 8 warps per row for short-n problems);
+//   the column pass streams 512-byte column strips down the rows with one
+//   online (max, sum) pair per column per lane, split over row ranges whose
+//   partials are merged by the last CTA of each strip.
+// * LSEs run in the base-2 exponent domain (duals are also kept scaled by
+//   log2(e)/eta) with a running max updated once per 4-vector chunk, so the
+//   exponentials are branch-free.  FP64 passes use exp2_f64 (table-driven,
+//   ~2 ulp); mixed-precision passes split off the integer part in FP64 and
+//   evaluate only the fraction on the SFU (ex2.approx.f32).
+// * The reference's third pass over M (row marginal for the stop test) is
+//   folded into the next row pass:
+//     rowsum_i(alpha^t, beta^t) = a_i * 2^(s2 * (alpha_i^t - alpha_i^{t+1})),
+//   and the duals are double-buffered so the iterate that passes the test is
+//   the one returned.
+// * The gauge-normalised iterate difference is assembled from per-CTA
+//   (count, mean, M2) statistics combined with Chan's formula (no
+//   cancellation), so no pass needs a second sweep over the duals.
+// * Every reduction has a fixed order: results are bitwise reproducible.
+#include <algorithm>
+
+#include "bcd.cuh"
+
+namespace cg {
+
+namespace {
+constexpr int kUnroll = 4;
+
+// (max, sum) merge in base 2
+__device__ __forceinline__ void lse2_merge(double& mx, double& s, double mx2, double s2,
+                                           const double* tab) {
+  if (s2 == 0.0) return;
+  if (s == 0.0) {
+    mx = mx2;
+    s = s2;
+    return;
+  }
+  if (mx2 > mx) {
+    s = s * exp2_f64(mx - mx2, tab) + s2;
+    mx = mx2;
+  } else {
+    s += s2 * exp2_f64(mx2 - mx, tab);
+  }
+}
+
+// Accumulate K exponents (valid ones only) into the running (mx, s).
+template <bool FAST, int K>
+__device__ __forceinline__ void lse_chunk(const double (&d)[K], const bool (&ok)[K], double& mx,
+                                          double& s, const double* tab) {
+  double cmax = kNegInf;
+#pragma unroll
+  for (int q = 0; q < K; ++q)
+    if (ok[q]) cmax = fmax(cmax, d[q]);
+  if (cmax > mx) {
+    if (s != 0.0) s *= exp2_f64(mx - cmax, tab);
+    mx = cmax;
+  }
+  if (FAST) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int q = 0; q < K; ++q)
+      if (ok[q]) acc += exp2_neg_mixed(d[q] - mx);
+    s += static_cast<double>(acc);
+  } else {
+#pragma unroll
+    for (int q = 0; q < K; ++q)
+      if (ok[q]) s += exp2_neg_f64(d[q] - mx, tab);
+  }
+}
+
+// Same, for a chunk known to be fully in range (no predicates).
+template <bool FAST, int K>
+__device__ __forceinline__ void lse_chunk_full(const double (&d)[K], double& mx, double& s,
+                                               const double* tab) {
+  double cmax = d[0];
+#pragma unroll
+  for (int q = 1; q < K; ++q) cmax = fmax(cmax, d[q]);
+  if (cmax > mx) {
+    if (s != 0.0) s *= exp2_f64(mx - cmax, tab);
+    mx = cmax;
+  }
+  if (FAST) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int q = 0; q < K; ++q) acc += exp2_neg_mixed(d[q] - mx);
+    s += static_cast<double>(acc);
+  } else {
+    double acc = 0.0;
+#pragma unroll
+    for (int q = 0; q < K; ++q) acc += exp2_neg_f64(d[q] - mx, tab);
+    s += acc;
+  }
+}
+
+template <typename TM>
+struct Raw;  // raw 16-byte vector of M
+template <>
+struct Raw<double> {
+  using T = double2;
+  __device__ __forceinline__ static T load(const double* p) {
+    return __ldg(reinterpret_cast<const double2*>(p));
+  }
+  __device__ __forceinline__ static double get(const T& v, int k) { return k == 0 ? v.x : v.y; }
+};
+template <>
+struct Raw<float> {
+  using T = float4;
+  __device__ __forceinline__ static T load(const float* p) {
+    return __ldg(reinterpret_cast<const float4*>(p));
+  }
+  __device__ __forceinline__ static double get(const T& v, int k) {
+    return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
+  }
+};
+
+// Elements per lane per step: 8 (two float4 or four double2 vectors).
+template <typename TM>
+struct RowU {
+  static constexpr int U = (Vec<TM>::N == 4) ? 2 : 4;
+};
+
+// One warp's segment [c0, c1) of row `row`: LSE over j of (betas_j - s2*M_ij).
+// Full chunks run predicate-free with the next chunk's M vectors prefetched.
+template <typename TM, bool FAST>
+__device__ __forceinline__ void row_segment(const TM* __restrict__ Mrow,
+                                            const double* __restrict__ betas, double s2, int c0,
+                                            int c1, int lane, bool vec_ok, const double* tab,
+                                            double& mx, double& s) {
+  constexpr int VN = Vec<TM>::N;
+  if (vec_ok) {
+    constexpr int U = RowU<TM>::U;
+    constexpr int step = 32 * VN;
+    constexpr int span = step * U;
+    using RT = typename Raw<TM>::T;
+    int cb = c0;
+    RT nxt[U];
+    if (cb + span <= c1) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) nxt[u] = Raw<TM>::load(Mrow + cb + lane * VN + u * step);
+    }
+    for (; cb + span <= c1; cb += span) {
+      RT cur[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) cur[u] = nxt[u];
+      if (cb + 2 * span <= c1) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) nxt[u] = Raw<TM>::load(Mrow + cb + span + lane * VN + u * step);
+      }
+      double d[U * VN];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        double bv[VN];
+        ld_duals<VN>(betas + cb + lane * VN + u * step, bv);
+#pragma unroll
+        for (int k = 0; k < VN; ++k) d[u * VN + k] = fma(-Raw<TM>::get(cur[u], k), s2, bv[k]);
+      }
+      lse_chunk_full<FAST, U * VN>(d, mx, s, tab);
+    }
+    // tail (vectors that are in range, then nothing: c1 is a multiple of VN)
+    for (int j = cb + lane * VN; j < c1; j += step) {
+      double d[VN];
+      bool ok[VN];
+      double mv[VN], bv[VN];
+      Vec<TM>::load(Mrow + j, mv);
+      ld_duals<VN>(betas + j, bv);
+#pragma unroll
+      for (int k = 0; k < VN; ++k) {
+        ok[k] = true;
+        d[k] = fma(-mv[k], s2, bv[k]);
+      }
+      lse_chunk<FAST, VN>(d, ok, mx, s, tab);
+    }
+  } else {
+    for (int j0 = c0 + lane; j0 < c1; j0 += 32 * kUnroll) {
+      double d[kUnroll];
+      bool ok[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        const int j = j0 + u * 32;
+        ok[u] = j < c1;
+        d[u] = ok[u] ? fma(-ld1(Mrow + j), s2, betas[j]) : kNegInf;
+      }
+      lse_chunk<FAST, kUnroll>(d, ok, mx, s, tab);
+    }
+  }
+}
+
+// CTA-wide Chan combine; thread 0 ends with the total.  sh: 3 * kThreads.
+__device__ __forceinline__ void cta_chan(double& n, double& mu, double& m2, double* sh) {
+  const int t = threadIdx.x;
+  __syncthreads();
+  sh[t] = n;
+  sh[kThreads + t] = mu;
+  sh[2 * kThreads + t] = m2;
+  __syncthreads();
+  for (int w = kThreads / 2; w > 0; w >>= 1) {
+    if (t < w) {
+      double a = sh[t], b = sh[kThreads + t], c = sh[2 * kThreads + t];
+      chan_combine(a, b, c, sh[t + w], sh[kThreads + t + w], sh[2 * kThreads + t + w]);
+      sh[t] = a;
+      sh[kThreads + t] = b;
+      sh[2 * kThreads + t] = c;
+    }
+    __syncthreads();
+  }
+  n = sh[0];
+  mu = sh[kThreads];
+  m2 = sh[2 * kThreads];
+}
+
+// Two-pass (count, mean, M2) of v over the CTA (invalid entries skipped).
+__device__ __forceinline__ void cta_stats(double v, bool valid, double* red, double& n,
+                                          double& mu, double& m2) {
+  __shared__ double sh_mu;
+  const double cnt = cta_sum(valid ? 1.0 : 0.0, red);
+  const double sum = cta_sum(valid ? v : 0.0, red);
+  if (threadIdx.x == 0) sh_mu = (cnt > 0) ? sum / cnt : 0.0;
+  __syncthreads();
+  const double mean = sh_mu;
+  const double dv = valid ? (v - mean) : 0.0;
+  const double q = cta_sum(dv * dv, red);
+  n = cnt;
+  mu = mean;
+  m2 = q;
+}
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Row pass: alpha^{t+1}_i = eta * (log a_i - LSE_j((beta^t_j - M_ij) / eta))
+// ---------------------------------------------------------------------------
+template <typename TM>
+__global__ void __launch_bounds__(kThreads, 3) bcd_row_kernel(const BcdProb* __restrict__ probs,
+                                                            const int* __restrict__ cta_prob,
+                                                            const int* __restrict__ cta_start) {
+  __shared__ double tab[16];
+  __shared__ double sm_mx[kWarps], sm_s[kWarps];
+  __shared__ double sm_v[kWarps][2];
+  __shared__ double red[kWarps];
+  __shared__ double shc[3 * kThreads];
+  load_exp2_table(tab);
+
+  const int pidx = cta_prob ? cta_prob[blockIdx.x] : 0;
+  const int cta = cta_prob ? (int)blockIdx.x - cta_start[pidx] : (int)blockIdx.x;
+  const BcdProb& P = probs[pidx];
+  BcdState* st = P.st;
+  if (ldcg(&st->done)) return;
+  const int t = ldcg(&st->iter);
+  const bool check = ldcg(&st->check_pending) != 0;
+  const bool fast = ldcg(&st->fast) != 0;
+  const int phase = ldcg(&st->phase);
+  __syncthreads();
+
+  const int n = P.n, m = P.m;
+  const TM* __restrict__ M = static_cast<const TM*>(P.M);
+  const double* __restrict__ betas = P.betas[t & 1];
+  const double* __restrict__ alphas_cur = P.alphas[t & 1];
+  const double* __restrict__ alpha_cur = P.alpha[t & 1];
+  const double s2 = P.s2;
+
+  const int R = P.rows_per_cta;
+  const int wpr = kWarps / R;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int rloc = warp / wpr, seg = warp % wpr;
+  const int row = cta * R + rloc;
+
+  constexpr int VN = Vec<TM>::N;
+  const bool vec_ok = (m % VN) == 0 && (reinterpret_cast<uintptr_t>(M) % 16) == 0;
+
+  double mx = kNegInf, s = 0.0;
+  if (row < n) {
+    const int step = 32 * VN;
+    int chunk = (m + wpr - 1) / wpr;
+    chunk = ((chunk + step - 1) / step) * step;
+    const int c0 = seg * chunk;
+    const int c1 = min(m, c0 + chunk);
+    const TM* __restrict__ Mrow = M + (size_t)row * m;
+    if (fast)
+      row_segment<TM, true>(Mrow, betas, s2, c0, c1, lane, vec_ok, tab, mx, s);
+    else
+      row_segment<TM, false>(Mrow, betas, s2, c0, c1, lane, vec_ok, tab, mx, s);
+  }
+  // warp combine: exact max by butterfly, then one rescale and a sum tree
+  double wmx = mx;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) wmx = fmax(wmx, __shfl_xor_sync(0xffffffffu, wmx, o));
+  double sc = (s != 0.0) ? s * exp2_f64(mx - wmx, tab) : 0.0;
+  sc = warp_sum_down(sc);
+  if (lane == 0) {
+    sm_mx[warp] = wmx;
+    sm_s[warp] = sc;
+  }
+  __syncthreads();
+  if (lane == 0 && seg == 0) {
+    double err2 = 0.0, da = 0.0;
+    if (row < n) {
+      double M0 = sm_mx[warp], S0 = sm_s[warp];
+      for (int q = 1; q < wpr; ++q) lse2_merge(M0, S0, sm_mx[warp + q], sm_s[warp + q], tab);
+      const double a_new = P.eta * P.loga[row] - (P.eta * kLn2) * (M0 + log2(S0));
+      const double as_new = a_new * s2;
+      P.alpha[(t + 1) & 1][row] = a_new;
+      P.alphas[(t + 1) & 1][row] = as_new;
+      if (check) {
+        const double ai = P.a[row];
+        const double e = ai * exp2_f64(alphas_cur[row] - as_new, tab) - ai;
+        err2 = e * e;
+      }
+      da = a_new - alpha_cur[row];
+    }
+    sm_v[rloc][0] = err2;
+    sm_v[rloc][1] = da;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double acc = 0.0, cnt = 0.0, sum = 0.0;
+    for (int q = 0; q < R; ++q) {
+      acc += sm_v[q][0];
+      if (cta * R + q < n) {
+        cnt += 1.0;
+        sum += sm_v[q][1];
+      }
+    }
+    const double mean = cnt > 0 ? sum / cnt : 0.0;
+    double m2 = 0.0;
+    for (int q = 0; q < R; ++q)
+      if (cta * R + q < n) {
+        const double dd = sm_v[q][1] - mean;
+        m2 += dd * dd;
+      }
+    double* out = P.row_part + (size_t)cta * 4;
+    out[0] = cnt;
+    out[1] = mean;
+    out[2] = m2;
+    out[3] = acc;
+  }
+  if (!elect_last(&P.counters[0], (unsigned)P.row_ctas)) return;
+
+  // Last CTA of the row pass.
+  if (phase == 1) {
+    double cn = 0, cmu = 0, cm2 = 0;
+    for (int q0 = threadIdx.x; q0 < P.row_ctas; q0 += 4 * blockDim.x) {
+      double bn[4], bmu[4], bm2[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int q = q0 + u * blockDim.x;
+        const bool in = q < P.row_ctas;
+        bn[u] = in ? ldcg(P.row_part + (size_t)q * 4) : 0.0;
+        bmu[u] = in ? ldcg(P.row_part + (size_t)q * 4 + 1) : 0.0;
+        bm2[u] = in ? ldcg(P.row_part + (size_t)q * 4 + 2) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) chan_combine(cn, cmu, cm2, bn[u], bmu[u], bm2[u]);
+    }
+    cta_chan(cn, cmu, cm2, shc);
+    if (threadIdx.x == 0) {
+      st->stat_a[0] = cn;
+      st->stat_a[1] = cmu;
+      st->stat_a[2] = cm2;
+    }
+  }
+  if (check) {
+    double v = 0.0;
+    for (int q = threadIdx.x; q < P.row_ctas; q += blockDim.x) v += ldcg(P.row_part + (size_t)q * 4 + 3);
+    const double tot = cta_sum(v, red);
+    if (threadIdx.x == 0) {
+      // Marginal test of iterate t (reference :568-589).
+      const double err = sqrt(tot);
+      st->last_err = err;
+      st->check_pending = 0;
+      if (!fast) {
+        if (err < st->tol) {
+          st->done = 1;
+          st->niter = t;
+        }
+      } else {
+        // Mixed precision: the SFU estimate only decides when to switch to
+        // FP64 passes; convergence is always confirmed by an FP64 test.
+        if (err < 0.5 * st->tol) {
+          st->fast = 0;
+        } else if (err < 0.9 * st->best_est) {
+          st->best_est = err;
+          st->stall = 0;
+        } else if (++st->stall >= 8) {
+          st->fast = 0;
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Column pass: beta^{t+1}_j = eta * (log b_j - LSE_i((alpha^{t+1}_i - M_ij)/eta))
+// ---------------------------------------------------------------------------
+template <typename TM, bool FAST>
+__device__ __forceinline__ void col_rows(const TM* __restrict__ M, const double* __restrict__ alphas,
+                                         double s2, int m, int jb, int r0, int r1, int warp,
+                                         bool vec_ok, const double* tab, double* mx, double* s) {
+  constexpr int VN = Vec<TM>::N;
+  constexpr int U = (VN == 4) ? 2 : 4;  // 8 elements per lane per step
+  constexpr int rstep = kWarps * U;
+  if (vec_ok) {
+    using RT = typename Raw<TM>::T;
+    int i0 = r0 + warp;
+    RT nxt[U];
+    if (i0 + (U - 1) * kWarps < r1) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) nxt[u] = Raw<TM>::load(M + (size_t)(i0 + u * kWarps) * m + jb);
+    }
+    for (; i0 + (U - 1) * kWarps < r1; i0 += rstep) {
+      RT cur[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) cur[u] = nxt[u];
+      if (i0 + rstep + (U - 1) * kWarps < r1) {
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          nxt[u] = Raw<TM>::load(M + (size_t)(i0 + rstep + u * kWarps) * m + jb);
+      }
+      double ai[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) ai[u] = alphas[i0 + u * kWarps];
+#pragma unroll
+      for (int k = 0; k < VN; ++k) {
+        double d[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) d[u] = fma(-Raw<TM>::get(cur[u], k), s2, ai[u]);
+        lse_chunk_full<FAST, U>(d, mx[k], s[k], tab);
+      }
+    }
+    // remaining rows of this warp (fewer than U)
+    for (int i = i0; i < r1; i += kWarps) {
+      const double ai = alphas[i];
+      double mv[VN];
+      Vec<TM>::load(M + (size_t)i * m + jb, mv);
+#pragma unroll
+      for (int k = 0; k < VN; ++k) {
+        double d[1] = {fma(-mv[k], s2, ai)};
+        bool ok[1] = {true};
+        lse_chunk<FAST, 1>(d, ok, mx[k], s[k], tab);
+      }
+    }
+  } else {
+    for (int i = r0 + warp; i < r1; i += kWarps) {
+      const double ai = alphas[i];
+      const TM* p = M + (size_t)i * m + jb;
+#pragma unroll
+      for (int k = 0; k < VN; ++k) {
+        double d[1];
+        bool ok[1] = {jb + k < m};
+        d[0] = ok[0] ? fma(-ld1(p + k), s2, ai) : kNegInf;
+        lse_chunk<FAST, 1>(d, ok, mx[k], s[k], tab);
+      }
+    }
+  }
+}
+
+template <typename TM>
+__global__ void __launch_bounds__(kThreads, 3) bcd_col_kernel(const BcdProb* __restrict__ probs,
+                                                            const int* __restrict__ cta_prob,
+                                                            const int* __restrict__ cta_start) {
+  constexpr int VN = Vec<TM>::N;
+  constexpr int W = 32 * VN;
+  constexpr int G = kThreads / W;  // merge groups per column
+  __shared__ double tab[16];
+  __shared__ double sm_mx[kWarps][W];
+  __shared__ double sm_s[kWarps][W];
+  __shared__ double red[kWarps];
+  __shared__ double shc[3 * kThreads];
+  load_exp2_table(tab);
+
+  const int pidx = cta_prob ? cta_prob[blockIdx.x] : 0;
+  const int cta = cta_prob ? (int)blockIdx.x - cta_start[pidx] : (int)blockIdx.x;
+  const BcdProb& P = probs[pidx];
+  BcdState* st = P.st;
+  if (ldcg(&st->done)) return;
+  const int t = ldcg(&st->iter);
+  const bool fast = ldcg(&st->fast) != 0;
+  const int phase = ldcg(&st->phase);
+  __syncthreads();
+
+  const int n = P.n, m = P.m;
+  const TM* __restrict__ M = static_cast<const TM*>(P.M);
+  const double* __restrict__ alphas = P.alphas[(t + 1) & 1];
+  const double s2 = P.s2;
+
+  const int strip = cta % P.col_strips;
+  const int split = cta / P.col_strips;
+  const int rows_per = (n + P.col_splits - 1) / P.col_splits;
+  const int r0 = split * rows_per, r1 = min(n, r0 + rows_per);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int jb = strip * W + lane * VN;
+  const bool vec_ok = (m % VN) == 0 && (reinterpret_cast<uintptr_t>(M) % 16) == 0;
+
+  double mx[VN], s[VN];
+#pragma unroll
+  for (int k = 0; k < VN; ++k) {
+    mx[k] = kNegInf;
+    s[k] = 0.0;
+  }
+  if (jb < m) {
+    if (fast)
+      col_rows<TM, true>(M, alphas, s2, m, jb, r0, r1, warp, vec_ok, tab, mx, s);
+    else
+      col_rows<TM, false>(M, alphas, s2, m, jb, r0, r1, warp, vec_ok, tab, mx, s);
+  }
+#pragma unroll
+  for (int k = 0; k < VN; ++k) {
+    sm_mx[warp][lane * VN + k] = mx[k];
+    sm_s[warp][lane * VN + k] = s[k];
+  }
+  __syncthreads();
+  const int c = threadIdx.x % W;  // column within the strip
+  const int g = threadIdx.x / W;  // merge group
+  const int j = strip * W + c;
+  double Mc = kNegInf, Sc = 0.0;
+  if (g == 0 && j < m) {
+    Mc = sm_mx[0][c];
+    Sc = sm_s[0][c];
+    for (int w = 1; w < kWarps; ++w) lse2_merge(Mc, Sc, sm_mx[w][c], sm_s[w][c], tab);
+  }
+  if (P.col_splits > 1) {
+    if (g == 0 && j < m) {
+      P.col_m[(size_t)split * m + j] = Mc;
+      P.col_s[(size_t)split * m + j] = Sc;
+    }
+    if (!elect_last(&P.counters[2 + strip], (unsigned)P.col_splits)) return;
+    // parallel merge over splits: group g takes splits g, g+G, ...
+    double Mg = kNegInf, Sg = 0.0;
+    if (j < m) {
+      // loads batched 4 at a time so their latencies overlap
+      for (int q0 = g; q0 < P.col_splits; q0 += 4 * G) {
+        double bm[4], bs[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int q = q0 + u * G;
+          bm[u] = (q < P.col_splits) ? ldcg(P.col_m + (size_t)q * m + j) : kNegInf;
+          bs[u] = (q < P.col_splits) ? ldcg(P.col_s + (size_t)q * m + j) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) lse2_merge(Mg, Sg, bm[u], bs[u], tab);
+      }
+    }
+    __syncthreads();
+    sm_mx[g][c] = Mg;
+    sm_s[g][c] = Sg;
+    __syncthreads();
+    if (g == 0 && j < m) {
+      Mc = sm_mx[0][c];
+      Sc = sm_s[0][c];
+      for (int q = 1; q < G; ++q) lse2_merge(Mc, Sc, sm_mx[q][c], sm_s[q][c], tab);
+    }
+  }
+  const bool valid = (g == 0 && j < m);
+  double db = 0.0;
+  if (valid) {
+    const double b_new = P.eta * P.logb[j] - (P.eta * kLn2) * (Mc + log2(Sc));
+    P.beta[(t + 1) & 1][j] = b_new;
+    P.betas[(t + 1) & 1][j] = b_new * s2;
+    db = b_new - P.beta[t & 1][j];
+  }
+  if (phase == 1) {
+    double sn, smu, sm2;
+    cta_stats(db, valid, red, sn, smu, sm2);
+    if (threadIdx.x == 0) {
+      P.col_part[(size_t)strip * 3] = sn;
+      P.col_part[(size_t)strip * 3 + 1] = smu;
+      P.col_part[(size_t)strip * 3 + 2] = sm2;
+    }
+  }
+
+  if (!elect_last(&P.counters[1], (unsigned)P.col_strips)) return;
+
+  // Last strip finisher: iteration bookkeeping (reference :551-591).
+  const int tn = t + 1;
+  if (phase == 1) {
+    double bn = 0, bmu = 0, bm2 = 0;
+    for (int q = threadIdx.x; q < P.col_strips; q += blockDim.x)
+      chan_combine(bn, bmu, bm2, ldcg(P.col_part + (size_t)q * 3),
+                   ldcg(P.col_part + (size_t)q * 3 + 1), ldcg(P.col_part + (size_t)q * 3 + 2));
+    cta_chan(bn, bmu, bm2, shc);
+    if (threadIdx.x == 0) {
+      const double an = ldcg(&st->stat_a[0]), amu = ldcg(&st->stat_a[1]),
+                   am2 = ldcg(&st->stat_a[2]);
+      // K = c - d of the reference = (sum dbeta - sum dalpha) / (n + m)
+      const double K = (bn * bmu - an * amu) / (double)(n + m);
+      const double ea = amu + K, eb = bmu - K;
+      const double diff = sqrt(am2 + an * ea * ea + bm2 + bn * eb * eb);
+      st->last_err = diff;
+      if (diff < st->tol * 10) st->phase = 2;
+    }
+  } else if (threadIdx.x == 0) {
+    st->check_pending = 1;
+  }
+  if (threadIdx.x == 0) {
+    st->iter = tn;
+    st->niter = tn;
+    if (fast) st->fast_iters += 1;
+    if (tn >= st->max_iter) st->done = 1;
+  }
+}
+
+// P = exp((alpha_i + beta_j - M_ij) / eta)
+template <typename TM>
+__global__ void plan_kernel(const TM* __restrict__ M, const double* __restrict__ alpha,
+                            const double* __restrict__ beta, double* __restrict__ P,
+                            double inv_eta, int n, int m) {
+  const size_t total = (size_t)n * m;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(idx / m);
+    const int j = (int)(idx - (size_t)i * m);
+    P[idx] = exp((alpha[i] + beta[j] - ld1(M + idx)) * inv_eta);
+  }
+}
+
+void launch_bcd_row(bool f32, const BcdProb* d_probs, const int* d_cta_prob,
+                    const int* d_cta_start, int total_ctas, cudaStream_t stream) {
+  if (f32)
+    bcd_row_kernel<float><<<total_ctas, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start);
+  else
+    bcd_row_kernel<double><<<total_ctas, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start);
+}
+void launch_bcd_col(bool f32, const BcdProb* d_probs, const int* d_cta_prob,
+                    const int* d_cta_start, int total_ctas, cudaStream_t stream) {
+  if (f32)
+    bcd_col_kernel<float><<<total_ctas, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start);
+  else
+    bcd_col_kernel<double><<<total_ctas, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start);
+}
+template <typename TM>
+void launch_plan(const TM* M, const double* alpha, const double* beta, double* P,
+                 double inv_eta, int n, int m, cudaStream_t stream) {
+  const size_t total = (size_t)n * m;
+  const int blocks = (int)std::min<size_t>((total + kThreads - 1) / kThreads, 148 * 16);
+  plan_kernel<TM><<<std::max(blocks, 1), kThreads, 0, stream>>>(M, alpha, beta, P, inv_eta, n, m);
+}
+template void launch_plan<double>(const double*, const double*, const double*, double*, double,
+                                  int, int, cudaStream_t);
+template void launch_plan<float>(const float*, const double*, const double*, double*, double,
+                                 int, int, cudaStream_t);
+
+int sm_count_current() {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return std::max(sms, 1);
+}
+
+void bcd_geometry(int n, int m, int elem_bytes, int sm_count, BcdProb& p) {
+  const int vn = 16 / elem_bytes;
+  // Row pass: prefer one warp per row; give short-n problems more warps per
+  // row while each warp keeps at least one unrolled vector sweep of work.
+  int R = kWarps;
+  while (R > 1) {
+    const int ctas = (n + R - 1) / R;
+    const int wpr = kWarps / (R / 2);
+    if (ctas >= 2 * sm_count) break;
+    if (m < wpr * 32 * vn * kUnroll) break;
+    R /= 2;
+  }
+  p.rows_per_cta = R;
+  p.row_ctas = (n + R - 1) / R;
+  // Column pass: 512-byte strips; split rows until ~2 CTAs per SM, keeping
+  // at least 256 rows per split (bounds the merge work of the last CTA).
+  const int W = 32 * vn;
+  p.col_strips = (m + W - 1) / W;
+  int splits = (2 * sm_count + p.col_strips - 1) / p.col_strips;
+  splits = std::max(1, std::min(splits, n / 256));
+  p.col_splits = splits;
+}
+
+}  // namespace cg

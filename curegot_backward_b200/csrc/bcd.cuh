@@ -1,0 +1,69 @@
+// Batched Sinkhorn BCD: problem descriptors and pass launchers.
+//
+// One launch of a pass covers every problem of a batch: CTA b of the launch
+// belongs to problem cta_prob[b] (or to problem 0 when cta_prob is null) and
+// is its (b - cta_start[p])-th CTA.  The single-problem solver uses a batch
+// of one; the serving engine packs many problems into the same launches.
+#pragma once
+
+#include "common.cuh"
+
+namespace cg {
+
+// Device-side BCD control state (one per problem).  The loop semantics are
+// those of cuda_sinkhorn_bcd (reference src/sinkhorn_bcd_kernel.cu:532-592).
+struct BcdState {
+  int iter;           // iterations completed so far
+  int phase;          // 1: iterate-difference test; 2: marginal test
+  int check_pending;  // the marginal test of the current iterate is due
+  int done;           // converged or max_iter reached
+  int niter;          // reference niter
+  int max_iter;
+  int fast;           // mixed precision: 1 = SFU exp passes, 0 = FP64 exp passes
+  int stall;          // mixed precision: checks without improvement
+  double tol;
+  double last_err;    // last test value (diff or marginal error)
+  double best_est;    // mixed precision: best fast marginal estimate
+  double stat_a[3];   // (count, mean, M2) of alpha^{t+1} - alpha^t
+  int fast_iters;     // iterations run with SFU passes
+  int pad_;
+};
+
+struct BcdProb {
+  const void* M;        // row-major n x m (float or double, fixed per launch)
+  int n, m;
+  int rows_per_cta;     // row pass: rows per CTA (1, 2, 4 or 8)
+  int row_ctas;         // row pass CTAs
+  int col_splits;       // column pass: row splits per strip
+  int col_strips;       // column pass: strips
+  double eta;
+  double s2;            // log2(e) / eta: scale into the base-2 exponent domain
+  const double* a;      // [n]
+  const double* loga;   // [n]
+  const double* logb;   // [m]
+  double* alpha[2];     // double-buffered duals (natural units)
+  double* beta[2];
+  double* alphas[2];    // the same duals times s2
+  double* betas[2];
+  double* col_m;        // [col_splits * m] partial LSE maxima (base 2)
+  double* col_s;        // [col_splits * m] partial LSE sums
+  double* row_part;     // [row_ctas * 4] marginal / stats partials
+  double* col_part;     // [col_strips * 3] stats partials
+  unsigned int* counters;  // [2 + col_strips], zero-initialised
+  BcdState* st;
+};
+
+void launch_bcd_row(bool f32, const BcdProb* d_probs, const int* d_cta_prob,
+                    const int* d_cta_start, int total_ctas, cudaStream_t stream);
+void launch_bcd_col(bool f32, const BcdProb* d_probs, const int* d_cta_prob,
+                    const int* d_cta_start, int total_ctas, cudaStream_t stream);
+template <typename TM>
+void launch_plan(const TM* M, const double* alpha, const double* beta, double* P,
+                 double inv_eta, int n, int m, cudaStream_t stream);
+
+// Launch geometry for one problem.
+void bcd_geometry(int n, int m, int elem_bytes, int sm_count, BcdProb& p);
+
+int sm_count_current();
+
+}  // namespace cg

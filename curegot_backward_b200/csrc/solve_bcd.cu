@@ -1,0 +1,233 @@
+// Single-problem BCD driver and the C-ABI entry points for it.
+//
+// Follows cuda_sinkhorn_bcd (reference src/sinkhorn_bcd_kernel.cu:429-634)
+// with input and output on the device.  The loop runs on the device: the
+// host queues chunks of iterations (one row pass + one column pass each)
+// and reads the 48-byte state once per chunk; passes after convergence exit
+// immediately.  No host synchronisation happens inside an iteration.
+#include <algorithm>
+#include <cstring>
+#include <string>
+
+#include "bcd.cuh"
+#include "workspace.cuh"
+
+namespace cg {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_last_error(const char* msg, const char* file, int line) {
+  g_last_error = std::string(msg) + " (" + file + ":" + std::to_string(line) + ")";
+}
+
+__global__ void bcd_init_kernel(const double* __restrict__ a, const double* __restrict__ b,
+                                const double* __restrict__ x0, int n, int m, double s2,
+                                double* __restrict__ loga, double* __restrict__ logb,
+                                double* __restrict__ alpha0, double* __restrict__ beta0,
+                                double* __restrict__ alphas0, double* __restrict__ betas0,
+                                unsigned int* counters, int ncounters, BcdState* st,
+                                int max_iter, double tol, int fast) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = tid; i < n; i += stride) {
+    loga[i] = log(a[i]);
+    const double v = x0 ? x0[i] : 0.0;
+    alpha0[i] = v;
+    alphas0[i] = v * s2;
+  }
+  for (int j = tid; j < m; j += stride) {
+    logb[j] = log(b[j]);
+    const double v = x0 ? x0[n + j] : 0.0;
+    beta0[j] = v;
+    betas0[j] = v * s2;
+  }
+  for (int q = tid; q < ncounters; q += stride) counters[q] = 0u;
+  if (tid == 0) {
+    st->iter = 0;
+    st->phase = 1;
+    st->check_pending = 0;
+    st->done = (max_iter <= 0) ? 1 : 0;
+    st->niter = 0;
+    st->max_iter = max_iter;
+    st->fast = fast;
+    st->stall = 0;
+    st->tol = tol;
+    st->last_err = 0.0;
+    st->best_est = INFINITY;
+    st->stat_a[0] = st->stat_a[1] = st->stat_a[2] = 0.0;
+    st->fast_iters = 0;
+  }
+}
+
+// The returned iterate lives in buffer (niter & 1); resolved on the device.
+template <typename TM>
+__global__ void plan_from_state_kernel(const TM* __restrict__ M, const BcdState* st,
+                                       const BcdProb* p, double* __restrict__ P) {
+  const int k = st->niter & 1;
+  const double* __restrict__ al = p->alpha[k];
+  const double* __restrict__ be = p->beta[k];
+  const int n = p->n, m = p->m;
+  const double inv_eta = 1.0 / p->eta;
+  const size_t total = (size_t)n * m;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(idx / m);
+    const int j = (int)(idx - (size_t)i * m);
+    P[idx] = exp((al[i] + be[j] - ld1(M + idx)) * inv_eta);
+  }
+}
+
+__global__ void dual_from_state_kernel(const BcdState* st, const BcdProb* p, double* dual) {
+  const int k = st->niter & 1;
+  const double* al = p->alpha[k];
+  const double* be = p->beta[k];
+  const int n = p->n, m = p->m;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += gridDim.x * blockDim.x)
+    dual[i] = (i < n) ? al[i] : be[i - n];
+}
+
+template <typename TM>
+int bcd_solve(const TM* M, const double* a, const double* b, double* Pout, double reg,
+              int max_iter, double tol, int n, int m, int* niter, const double* x0,
+              double* dual, cudaStream_t stream) {
+  if (!M || !a || !b || !niter || n <= 0 || m <= 0 || !(reg > 0.0) || !std::isfinite(reg)) {
+    set_last_error("cg_bcd: invalid argument", __FILE__, __LINE__);
+    return CG_ERR_INVALID_ARG;
+  }
+  const int sms = sm_count_current();
+  BcdProb hp{};
+  bcd_geometry(n, m, (int)sizeof(TM), sms, hp);
+  const int ncount = 2 + hp.col_strips;
+
+  Workspace ws(stream);
+  const size_t o_loga = ws.reserve<double>(n), o_logb = ws.reserve<double>(m);
+  size_t o_al[2], o_be[2], o_als[2], o_bes[2];
+  for (int k = 0; k < 2; ++k) {
+    o_al[k] = ws.reserve<double>(n);
+    o_be[k] = ws.reserve<double>(m);
+    o_als[k] = ws.reserve<double>(n);
+    o_bes[k] = ws.reserve<double>(m);
+  }
+  const size_t parts = (hp.col_splits > 1) ? (size_t)hp.col_splits * m : 1;
+  const size_t o_cm = ws.reserve<double>(parts), o_cs = ws.reserve<double>(parts);
+  const size_t o_rp = ws.reserve<double>((size_t)hp.row_ctas * 4);
+  const size_t o_cp = ws.reserve<double>((size_t)hp.col_strips * 3);
+  const size_t o_cnt = ws.reserve<unsigned int>(ncount);
+  const size_t o_st = ws.reserve<BcdState>(1);
+  const size_t o_prob = ws.reserve<BcdProb>(1);
+  CG_TRY(ws.allocate());
+
+  hp.M = M;
+  hp.n = n;
+  hp.m = m;
+  hp.eta = reg;
+  hp.s2 = kLog2e / reg;
+  hp.a = a;
+  hp.loga = ws.at<double>(o_loga);
+  hp.logb = ws.at<double>(o_logb);
+  for (int k = 0; k < 2; ++k) {
+    hp.alpha[k] = ws.at<double>(o_al[k]);
+    hp.beta[k] = ws.at<double>(o_be[k]);
+    hp.alphas[k] = ws.at<double>(o_als[k]);
+    hp.betas[k] = ws.at<double>(o_bes[k]);
+  }
+  hp.col_m = ws.at<double>(o_cm);
+  hp.col_s = ws.at<double>(o_cs);
+  hp.row_part = ws.at<double>(o_rp);
+  hp.col_part = ws.at<double>(o_cp);
+  hp.counters = ws.at<unsigned int>(o_cnt);
+  hp.st = ws.at<BcdState>(o_st);
+  BcdProb* dprob = ws.at<BcdProb>(o_prob);
+
+  const bool f32 = sizeof(TM) == 4;
+  bcd_init_kernel<<<64, 256, 0, stream>>>(a, b, x0, n, m, hp.s2, const_cast<double*>(hp.loga),
+                                          const_cast<double*>(hp.logb), hp.alpha[0], hp.beta[0],
+                                          hp.alphas[0], hp.betas[0], hp.counters, ncount, hp.st,
+                                          max_iter, tol, f32 ? 1 : 0);
+  CG_TRY_CUDA(cudaGetLastError());
+  CG_TRY_CUDA(cudaMemcpyAsync(dprob, &hp, sizeof(BcdProb), cudaMemcpyHostToDevice, stream));
+
+  BcdState hs{};
+  int chunk = 4;
+  int queued = 0;
+  while (true) {
+    const int todo = std::min(chunk, std::max(max_iter - queued, 0));
+    for (int c = 0; c < todo; ++c) {
+      launch_bcd_row(f32, dprob, nullptr, nullptr, hp.row_ctas, stream);
+      launch_bcd_col(f32, dprob, nullptr, nullptr, hp.col_strips * hp.col_splits, stream);
+    }
+    queued += todo;
+    CG_TRY_CUDA(cudaGetLastError());
+    CG_TRY_CUDA(cudaMemcpyAsync(&hs, hp.st, sizeof(BcdState), cudaMemcpyDeviceToHost, stream));
+    CG_TRY_CUDA(cudaStreamSynchronize(stream));
+    if (hs.done || queued >= max_iter) break;
+    chunk = std::min(chunk * 2, 64);
+  }
+  *niter = hs.niter;
+
+  if (Pout) {
+    const size_t total = (size_t)n * m;
+    const int blocks = (int)std::max<size_t>(1, std::min<size_t>((total + 255) / 256, sms * 16));
+    plan_from_state_kernel<TM><<<blocks, 256, 0, stream>>>(M, hp.st, dprob, Pout);
+  }
+  if (dual) dual_from_state_kernel<<<std::max(1, (n + m + 255) / 256), 256, 0, stream>>>(hp.st, dprob, dual);
+  CG_TRY_CUDA(cudaGetLastError());
+  ws.release();
+  return CG_OK;
+}
+
+__global__ void diag_exp2_kernel(const double* x, double* y, int n, int mode) {
+  __shared__ double tab[16];
+  load_exp2_table(tab);
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = (mode == 0) ? exp2_f64(x[i], tab) : (double)exp2_neg_mixed(x[i]);
+}
+
+}  // namespace cg
+
+extern "C" {
+
+const char* cg_last_error(void) { return cg::g_last_error.c_str(); }
+
+const char* cg_version(void) { return "curegot_b200 0.1.0 (sm_100a)"; }
+
+int cg_bcd_f64(const double* M, const double* a, const double* b, double* P, double reg,
+               int max_iter, double tol, int n, int m, int* niter, const double* x0,
+               double* dual, cudaStream_t stream) {
+  return cg::bcd_solve<double>(M, a, b, P, reg, max_iter, tol, n, m, niter, x0, dual, stream);
+}
+
+int cg_bcd_mixed(const float* M, const double* a, const double* b, double* P, double reg,
+                 int max_iter, double tol, int n, int m, int* niter, const double* x0,
+                 double* dual, cudaStream_t stream) {
+  return cg::bcd_solve<float>(M, a, b, P, reg, max_iter, tol, n, m, niter, x0, dual, stream);
+}
+
+int cg_transport_plan_f64(const double* M, const double* alpha, const double* beta, double* P,
+                          double reg, int n, int m, cudaStream_t stream) {
+  if (!M || !alpha || !beta || !P || n <= 0 || m <= 0 || !(reg > 0.0)) return CG_ERR_INVALID_ARG;
+  cg::launch_plan<double>(M, alpha, beta, P, 1.0 / reg, n, m, stream);
+  CG_TRY_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
+int cg_transport_plan_mixed(const float* M, const double* alpha, const double* beta, double* P,
+                            double reg, int n, int m, cudaStream_t stream) {
+  if (!M || !alpha || !beta || !P || n <= 0 || m <= 0 || !(reg > 0.0)) return CG_ERR_INVALID_ARG;
+  cg::launch_plan<float>(M, alpha, beta, P, 1.0 / reg, n, m, stream);
+  CG_TRY_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
+int cg_diag_exp2(const double* x, double* y, int n, int mode, cudaStream_t stream) {
+  if (!x || !y || n < 0 || mode < 0 || mode > 1) return CG_ERR_INVALID_ARG;
+  if (n == 0) return CG_OK;
+  cg::diag_exp2_kernel<<<(n + 255) / 256, 256, 0, stream>>>(x, y, n, mode);
+  CG_TRY_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,151 @@
+"""GPU parity of the Sinkhorn BCD path against the CPU oracle and against the
+reference's own GPU BCD solver (oracle/_ref, built from the reference sources).
+
+Bar (FP64 plain path): identical niter, duals within 1e-10 relative (to the
+largest dual magnitude), plan within 1e-12 absolute.
+"""
+import numpy as np
+import pytest
+import torch
+
+import curegot_backward_b200 as cg
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+DUAL_RTOL = 1e-10
+PLAN_ATOL = 1e-12
+
+
+def config0(seed=0):
+    rng = np.random.default_rng(seed)
+    n, m = 512, 640
+    X = rng.uniform(size=(n, 8)); Y = rng.uniform(size=(m, 8))
+    M = ((X[:, None, :] - Y[None, :, :]) ** 2).mean(-1)
+    return M, np.full(n, 1.0 / n), np.full(m, 1.0 / m)
+
+
+def rand_problem(n, m, seed):
+    rng = np.random.default_rng(seed)
+    M = rng.uniform(size=(n, m))
+    a = rng.uniform(0.5, 1.5, size=n); a /= a.sum()
+    b = rng.uniform(0.5, 1.5, size=m); b /= b.sum()
+    return M, a, b
+
+
+def assert_close(got, ref):
+    assert got["niter"] == ref["niter"], (got["niter"], ref["niter"])
+    scale = max(np.abs(ref["dual"]).max(), 1e-300)
+    assert np.abs(got["dual"] - ref["dual"]).max() <= DUAL_RTOL * scale
+    assert np.abs(got["plan"] - ref["plan"]).max() <= PLAN_ATOL
+
+
+def test_config0_matches_oracle(cuda_dev):
+    M, a, b = config0()
+    got = cg.numpy.sinkhorn_bcd(M, a, b, 0.05, tol=1e-8, max_iter=1000)
+    ref = oracle.bcd(M, a, b, 0.05, tol=1e-8, max_iter=1000)
+    assert_close(got, ref)
+    assert np.linalg.norm(got["plan"].sum(1) - a) < 1e-8
+
+
+@pytest.mark.parametrize("n,m,reg,tol", [
+    (80, 60, 0.01, 1e-6), (60, 80, 0.01, 1e-8), (50, 40, 0.05, 1e-8), (1, 1, 0.1, 1e-8),
+    (1, 7, 0.1, 1e-8), (7, 1, 0.1, 1e-8), (33, 31, 0.02, 1e-8), (3, 1000, 0.05, 1e-8),
+    (1000, 3, 0.05, 1e-8), (257, 129, 0.03, 1e-9), (2048, 96, 0.05, 1e-8),
+    (96, 4099, 0.05, 1e-8),
+])
+def test_shapes_match_oracle(cuda_dev, n, m, reg, tol):
+    M, a, b = rand_problem(n, m, n * 1000 + m)
+    got = cg.numpy.sinkhorn_bcd(M, a, b, reg, tol=tol, max_iter=3000)
+    ref = oracle.bcd(M, a, b, reg, tol=tol, max_iter=3000)
+    assert_close(got, ref)
+
+
+def test_truncation_and_zero_iterations(cuda_dev):
+    M, a, b = rand_problem(50, 40, 456)
+    got = cg.numpy.sinkhorn_bcd(M, a, b, 0.01, tol=1e-12, max_iter=10)
+    assert got["niter"] == 10
+    assert_close(got, oracle.bcd(M, a, b, 0.01, tol=1e-12, max_iter=10))
+    z = cg.numpy.sinkhorn_bcd(M, a, b, 0.01, tol=1e-8, max_iter=0)
+    assert z["niter"] == 0
+    assert_close(z, oracle.bcd(M, a, b, 0.01, tol=1e-8, max_iter=0))
+
+
+def test_warm_start(cuda_dev):
+    M, a, b = rand_problem(50, 40, 789)
+    r = cg.numpy.sinkhorn_bcd(M, a, b, 0.01, tol=1e-8, max_iter=5000)
+    r2 = cg.numpy.sinkhorn_bcd(M, a, b, 0.01, tol=1e-8, max_iter=5000, x0=r["dual"])
+    assert r2["niter"] <= r["niter"]
+    assert np.abs(r2["plan"] - r["plan"]).max() <= 1e-8
+    assert_close(r2, oracle.bcd(M, a, b, 0.01, tol=1e-8, max_iter=5000, x0=r["dual"]))
+
+
+def test_torch_api_dtype_device_roundtrip(cuda_dev):
+    M, a, b = rand_problem(64, 48, 3)
+    Mt = torch.tensor(M, dtype=torch.float32)  # CPU float32 in -> CPU float32 out
+    out = cg.torch.sinkhorn_bcd(Mt, torch.tensor(a), torch.tensor(b), 0.05, tol=1e-8)
+    assert out["plan"].dtype == torch.float32 and out["plan"].device.type == "cpu"
+    Mc = torch.tensor(M, device=cuda_dev)
+    out = cg.torch.sinkhorn_bcd(Mc, torch.tensor(a, device=cuda_dev),
+                                torch.tensor(b, device=cuda_dev), 0.05, tol=1e-8)
+    assert out["plan"].is_cuda and out["plan"].dtype == torch.float64
+    ref = oracle.bcd(Mt.double().numpy(), a, b, 0.05, tol=1e-8)
+    assert out["niter"] == ref["niter"]
+
+
+def test_deterministic(cuda_dev):
+    M, a, b = rand_problem(300, 500, 11)
+    r1 = cg.numpy.sinkhorn_bcd(M, a, b, 0.02, tol=1e-9, max_iter=2000)
+    r2 = cg.numpy.sinkhorn_bcd(M, a, b, 0.02, tol=1e-9, max_iter=2000)
+    assert np.array_equal(r1["dual"], r2["dual"])
+
+
+def test_mixed_precision_fp64_checked(cuda_dev):
+    M, a, b = rand_problem(700, 900, 5)
+    M32 = M.astype(np.float32)
+    got = cg.numpy.sinkhorn_bcd(M32, a, b, 0.05, tol=1e-8, max_iter=3000, precision="mixed")
+    ref = oracle.bcd(M32.astype(np.float64), a, b, 0.05, tol=1e-8, max_iter=3000)
+    # FP64-checked marginal error of the returned duals on the FP32-valued M
+    al, be = got["dual"][:700], got["dual"][700:]
+    P = np.exp((al[:, None] + be[None, :] - M32.astype(np.float64)) / 0.05)
+    assert np.linalg.norm(P.sum(1) - a) < 1e-8
+    assert np.linalg.norm(P.sum(0) - b) < 1e-8
+    assert got["niter"] < 3000
+    # duals agree with the FP64 oracle's to the accuracy a 1e-8 marginal allows
+    g = got["dual"] - ref["dual"]
+    g -= g.mean()  # gauge
+    assert np.abs(g).max() < 1e-6
+
+
+def test_exp2_implementations_vs_cuda(cuda_dev):
+    from curegot_backward_b200 import _native
+    x = torch.linspace(-1019.0, 1023.0, 2_000_003, dtype=torch.float64, device=cuda_dev)
+    y = torch.empty_like(x)
+    _native.call("cg_diag_exp2", x.data_ptr(), y.data_ptr(), x.numel(), 0,
+                 torch.cuda.current_stream().cuda_stream)
+    ref = torch.exp2(x)
+    rel = ((y - ref).abs() / ref).max().item()
+    assert rel < 2e-15, rel
+    xn = torch.linspace(-120.0, 0.0, 1_000_003, dtype=torch.float64, device=cuda_dev)
+    yn = torch.empty_like(xn)
+    _native.call("cg_diag_exp2", xn.data_ptr(), yn.data_ptr(), xn.numel(), 1,
+                 torch.cuda.current_stream().cuda_stream)
+    refn = torch.exp2(xn)
+    reln = ((yn - refn).abs() / refn).max().item()
+    assert reln < 5e-7, reln
+
+
+@pytest.mark.skipif(not oracle.ref_bcd_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("which", ["config0", "rand"])
+def test_matches_reference_gpu_solver(cuda_dev, which):
+    if which == "config0":
+        M, a, b = config0()
+        reg = 0.05
+    else:
+        M, a, b = rand_problem(120, 90, 7)
+        reg = 0.02
+    ref = oracle.ref_bcd(M, a, b, reg, tol=1e-8, max_iter=2000)
+    got = cg.numpy.sinkhorn_bcd(M, a, b, reg, tol=1e-8, max_iter=2000)
+    assert_close(got, ref)
+    # and the oracle agrees with the reference's own solver
+    assert_close(oracle.bcd(M, a, b, reg, tol=1e-8, max_iter=2000), ref)
