@@ -21,6 +21,10 @@ import sys as _sys
 import types as _types
 
 from . import _native, _solvers
+from ._context import SPLRBackwardContext
+from . import backward, autograd
+from .autograd import SPLROT, splr_ot, splr_ot_batch, splr_ot_with_info
+from .backward import solve_backward
 
 __version__ = "0.1.0"
 
@@ -35,12 +39,24 @@ def _namespace(name: str, doc: str, members: dict) -> _types.ModuleType:
 
 numpy = _namespace("numpy", "NumPy interface.", {
     "sinkhorn_bcd": _solvers.numpy_sinkhorn_bcd,
+    "sinkhorn_splr": _solvers.numpy_sinkhorn_splr,
 })
 
 torch = _namespace("torch", "PyTorch interface.", {
     "sinkhorn_bcd": _solvers.torch_sinkhorn_bcd,
+    "sinkhorn_splr": _solvers.torch_sinkhorn_splr,
+    "sinkhorn_splr_bwd": _solvers.torch_sinkhorn_splr_bwd,
+    "SPLRBackwardContext": SPLRBackwardContext,
+    "splr_ot": splr_ot,
+    "splr_ot_with_info": splr_ot_with_info,
+    "splr_ot_batch": splr_ot_batch,
+    "SPLROT": SPLROT,
+    "solve_backward": solve_backward,
 })
 
-tests = _namespace("tests", "Test functions.", {})
+tests = _namespace("tests", "Test functions.", {
+    "test_T_computation_sparsify": _solvers.test_T_computation_sparsify,
+    "test_sparse_cholesky_solve": _solvers.test_sparse_cholesky_solve,
+})
 
 CuregotError = _native.CuregotError

@@ -43,6 +43,25 @@ _lock = threading.Lock()
 c_int, c_double, c_void_p, c_long = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_long
 c_size_t = ctypes.c_size_t
 c_int_p = ctypes.POINTER(ctypes.c_int)
+c_ll_p = ctypes.POINTER(ctypes.c_longlong)
+c_void_pp = ctypes.POINTER(ctypes.c_void_p)
+
+
+class CtxInfo(ctypes.Structure):
+    """cg_ctx_info_t of include/curegot_b200.h."""
+    _fields_ = [("n", ctypes.c_int), ("m", ctypes.c_int), ("dim", ctypes.c_int),
+                ("nnz", ctypes.c_longlong), ("reg", ctypes.c_double), ("ys", ctypes.c_double),
+                ("low_rank", ctypes.c_int), ("fallback", ctypes.c_int), ("valid", ctypes.c_int),
+                ("has_diag", ctypes.c_int), ("has_point", ctypes.c_int),
+                ("adopted", ctypes.c_int)]
+
+
+CG_PRECOND_NONE, CG_PRECOND_DIAG, CG_PRECOND_SPLR = 0, 1, 2
+(CG_CTX_CSR_VALUES, CG_CTX_CSR_COLIND, CG_CTX_CSR_ROWPTR, CG_CTX_SECANT_S, CG_CTX_SECANT_Y,
+ CG_CTX_INV_DIAG, CG_CTX_POINT, CG_CTX_INVA_Y) = range(8)
+_SPLR_ARGS = [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_double, c_int, c_int,
+              c_int_p, c_double, c_double, c_int, c_int, c_int, c_void_p, c_void_p, c_void_pp,
+              c_int_p, c_void_p, c_void_p]
 
 # name -> argtypes (every exported entry point of include/curegot_b200.h)
 SIGNATURES = {
@@ -57,6 +76,22 @@ SIGNATURES = {
     "cg_transport_plan_mixed": [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_int,
                                 c_void_p],
     "cg_diag_exp2": [c_void_p, c_void_p, c_int, c_int, c_void_p],
+    "cg_splr_f64": _SPLR_ARGS,
+    "cg_splr_mixed": _SPLR_ARGS,
+    "cg_ctx_info": [c_void_p, ctypes.POINTER(CtxInfo)],
+    "cg_ctx_setup_diag": [c_void_p, c_void_p],
+    "cg_ctx_apply": [c_void_p, c_void_p, c_void_p, c_int, c_void_p],
+    "cg_ctx_copy": [c_void_p, c_int, c_void_p, c_void_p],
+    "cg_ctx_destroy": [c_void_p],
+    "cg_backward_f64": [c_void_p, c_void_p, c_void_p, c_double, c_int, c_double, c_int, c_int,
+                        c_int, c_void_p, c_void_p, c_int_p, c_int_p, c_void_p],
+    "cg_t_values_f64": [c_void_p, c_void_p, c_void_p, c_int, c_int, c_double, c_void_p,
+                        c_void_p, c_void_p],
+    "cg_test_t_sparsify_f64": [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_double,
+                               c_double, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p,
+                               c_void_p, c_void_p, c_void_p, c_void_p, c_ll_p, c_void_p],
+    "cg_test_spd_solve_f64": [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p,
+                              c_void_p],
 }
 RESTYPES = {"cg_last_error": ctypes.c_char_p, "cg_version": ctypes.c_char_p}
 

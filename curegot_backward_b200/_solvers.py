@@ -131,3 +131,200 @@ def numpy_sinkhorn_bcd(M, a, b, reg, tol=1e-6, max_iter=1000, verbose=0, **kwarg
     if verbose > 0:
         _verbose_report("sinkhorn_bcd", n, m, reg, tol, max_iter, niter)
     return {"niter": niter, "plan": P.cpu().numpy(), "dual": dual.cpu().numpy()}
+
+
+# ---------------------------------------------------------------------------
+# SPLR
+# ---------------------------------------------------------------------------
+
+def _splr_kwargs(kwargs, n, m):
+    """Reference kwarg parsing (src/solvers_torch.cpp:212-243, :814-838)."""
+    density_max = min(10.0 / min(n, m), 1.0)
+    if "density" in kwargs and kwargs["density"] is not None:
+        density_max = min(max(float(kwargs["density"]), 0.0), 1.0)
+    shift_max = 0.001
+    if "shift" in kwargs and kwargs["shift"] is not None:
+        shift_max = max(float(kwargs["shift"]), 0.0)
+    cycle = int(kwargs.get("sparsity_pattern_cycle", 30))
+    cand = int(kwargs.get("candidate_sinkhorn_iter", 3))
+    return density_max, shift_max, cycle, cand
+
+
+def _splr_device(M, a, b, reg, tol, max_iter, verbose, x0, precision, density_max, shift_max,
+                 cycle, cand, want_ctx=False, want_plan=True, trace=False):
+    dev = M.device
+    n, m = int(M.shape[0]), int(M.shape[1])
+    opts = dict(device=dev, dtype=torch.float64)
+    P = torch.empty((n, m), **opts) if want_plan else None
+    dual = torch.empty(n + m, **opts)
+    niter = ctypes.c_int(0)
+    conv = ctypes.c_int(0)
+    ctx = ctypes.c_void_p(0)
+    tr = np.zeros((max(int(max_iter), 1), 8)) if trace else None
+    fn = "cg_splr_mixed" if precision == "mixed" else "cg_splr_f64"
+    with torch.cuda.device(dev):
+        _native.call(fn, M.data_ptr(), a.data_ptr(), b.data_ptr(),
+                     P.data_ptr() if P is not None else None, float(reg), int(max_iter),
+                     float(tol), n, m, ctypes.byref(niter), float(density_max), float(shift_max),
+                     int(cycle), int(cand), int(verbose),
+                     x0.data_ptr() if x0 is not None else None, dual.data_ptr(),
+                     ctypes.byref(ctx) if want_ctx else None, ctypes.byref(conv),
+                     tr.ctypes.data if tr is not None else None, _stream_of(dev))
+    out = {"niter": int(niter.value), "converged": bool(conv.value), "plan": P, "dual": dual,
+           "ctx_handle": ctx.value}
+    if tr is not None:
+        out["trace"] = tr[: out["niter"]]
+    return out
+
+
+def _prep_torch(M, a, b, kwargs):
+    n, m = _check_shapes(M, a, b)
+    dev = _target_device(M)
+    precision = _precision(kwargs)
+    mdt = torch.float32 if precision == "mixed" else torch.float64
+    Md = M.detach().to(device=dev, dtype=mdt).contiguous()
+    ad = a.detach().to(device=dev, dtype=torch.float64).contiguous()
+    bd = b.detach().to(device=dev, dtype=torch.float64).contiguous()
+    x0 = _x0(kwargs, n, m, dev)
+    return n, m, dev, precision, Md, ad, bd, x0
+
+
+def torch_sinkhorn_splr(M, a, b, reg, tol=1e-6, max_iter=1000, verbose=0, **kwargs):
+    """SPLR solver (reference src/solvers_torch.cpp:138-288)."""
+    n, m, dev, precision, Md, ad, bd, x0 = _prep_torch(M, a, b, kwargs)
+    dmax, smax, cycle, cand = _splr_kwargs(kwargs, n, m)
+    out = _splr_device(Md, ad, bd, reg, tol, max_iter, verbose, x0, precision, dmax, smax,
+                       cycle, cand, trace=bool(kwargs.get("return_trace", False)))
+    if verbose > 0:
+        _verbose_report("torch_sinkhorn_splr", n, m, reg, tol, max_iter, out["niter"])
+    res = {"niter": out["niter"], "plan": out["plan"].to(device=M.device, dtype=M.dtype),
+           "dual": out["dual"].to(device=M.device, dtype=M.dtype)}
+    if "trace" in out:
+        res["trace"] = out["trace"]
+    return res
+
+
+def numpy_sinkhorn_splr(M, a, b, reg, tol=1e-6, max_iter=1000, verbose=0, **kwargs):
+    """SPLR solver with host arrays (reference src/solvers_numpy.cpp:113-244)."""
+    M = np.asarray(M, dtype=np.float64)
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    n, m = _check_shapes(torch.from_numpy(M), torch.from_numpy(a), torch.from_numpy(b),
+                         kind="array")
+    if "x0" in kwargs and kwargs["x0"] is not None:
+        x0a = np.asarray(kwargs["x0"], dtype=np.float64)
+        if x0a.ndim != 1 or x0a.shape[0] != n + m:
+            raise RuntimeError("x0 must be a 1D array of length n + m")
+    precision = _precision(kwargs)
+    dev = _target_device(torch.empty(0))
+    mdt = torch.float32 if precision == "mixed" else torch.float64
+    Md = torch.from_numpy(np.ascontiguousarray(M)).to(device=dev, dtype=mdt)
+    ad = torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    bd = torch.from_numpy(np.ascontiguousarray(b)).to(dev)
+    x0 = _x0(kwargs, n, m, dev, kind="array")
+    dmax, smax, cycle, cand = _splr_kwargs(kwargs, n, m)
+    out = _splr_device(Md, ad, bd, reg, tol, max_iter, verbose, x0, precision, dmax, smax,
+                       cycle, cand, trace=bool(kwargs.get("return_trace", False)))
+    if verbose > 0:
+        _verbose_report("sinkhorn_splr", n, m, reg, tol, max_iter, out["niter"])
+    res = {"niter": out["niter"], "plan": out["plan"].cpu().numpy(),
+           "dual": out["dual"].cpu().numpy()}
+    if "trace" in out:
+        res["trace"] = out["trace"]
+    return res
+
+
+def torch_sinkhorn_splr_bwd(M, a, b, reg, tol=1e-6, max_iter=1000, verbose=0, **kwargs):
+    """SPLR with backward-context export (reference src/solvers_torch.cpp:707-912)."""
+    from ._context import SPLRBackwardContext
+    n, m, dev, precision, Md, ad, bd, x0 = _prep_torch(M, a, b, kwargs)
+    dmax, smax, cycle, cand = _splr_kwargs(kwargs, n, m)
+    return_validation = bool(kwargs.get("return_validation", False))
+    context_mode = kwargs.get("context_mode", "adopt")
+    if context_mode not in ("adopt", "snapshot"):
+        raise RuntimeError('context_mode must be "adopt" or "snapshot"')
+    out = _splr_device(Md, ad, bd, reg, tol, max_iter, verbose, x0, precision, dmax, smax,
+                       cycle, cand, want_ctx=True,
+                       trace=bool(kwargs.get("return_trace", False)))
+    ctx = SPLRBackwardContext(out["ctx_handle"], dev, return_validation)
+    if not ctx.is_valid:
+        raise RuntimeError("torch_sinkhorn_splr_bwd: forward pass failed (non-finite "
+                           "objective value); no backward context available")
+    ctx.setup_diagonal_preconditioner()
+    if verbose > 0:
+        _verbose_report("torch_sinkhorn_splr_bwd", n, m, reg, tol, max_iter, out["niter"])
+    res = {"niter": out["niter"], "converged": out["converged"],
+           "plan": out["plan"].to(device=M.device, dtype=M.dtype),
+           "dual": out["dual"].to(device=M.device, dtype=M.dtype), "context": ctx}
+    if "trace" in out:
+        res["trace"] = out["trace"]
+    return res
+
+
+# ---------------------------------------------------------------------------
+# Test hooks (reference src/tests.cpp:36-200)
+# ---------------------------------------------------------------------------
+
+def test_T_computation_sparsify(alpha, beta, M, a, b, reg, shift, K, nrun=1):
+    alpha, beta, M, a, b = (np.asarray(x, dtype=np.float64) for x in (alpha, beta, M, a, b))
+    if alpha.ndim != 1 or beta.ndim != 1 or a.ndim != 1 or b.ndim != 1:
+        raise RuntimeError("alpha, beta, a, and b must be 1D arrays")
+    if M.ndim != 2:
+        raise RuntimeError("M must be a 2D array")
+    n, m = alpha.shape[0], beta.shape[0]
+    if M.shape != (n, m):
+        raise RuntimeError("Shape mismatch: M should be [n x m], where n=len(alpha) and m=len(beta)")
+    if a.shape[0] != n or b.shape[0] != m:
+        raise RuntimeError("Shape mismatch: a should be [n], and b should be [m], where "
+                           "n=len(alpha) and m=len(beta)")
+    dev = _target_device(torch.empty(0))
+    t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+    al, be, Md, ad, bd = t(alpha), t(beta), t(M), t(a), t(b)
+    H, Te = n + m - 1, n * (m - 1)
+    Ks = min(max(int(K), 1), Te)
+    f64 = dict(device=dev, dtype=torch.float64)
+    rows, cols, grad = torch.empty(n, **f64), torch.empty(m, **f64), torch.empty(H, **f64)
+    fg = torch.empty(2, **f64)
+    val = torch.empty(Ks + H, **f64)
+    col = torch.empty(Ks + H, device=dev, dtype=torch.int32)
+    rowptr = torch.empty(H + 1, device=dev, dtype=torch.int32)
+    tv = torch.empty(max(Te, 1), **f64)
+    ti = torch.empty(max(Te, 1), device=dev, dtype=torch.int32)
+    ka = ctypes.c_longlong(0)
+    with torch.cuda.device(dev):
+        st = _stream_of(dev)
+        for _ in range(max(int(nrun), 1)):
+            _native.call("cg_test_t_sparsify_f64", al.data_ptr(), be.data_ptr(), Md.data_ptr(),
+                         ad.data_ptr(), bd.data_ptr(), float(reg), float(shift), int(K), n, m,
+                         rows.data_ptr(), cols.data_ptr(), grad.data_ptr(), fg.data_ptr(),
+                         val.data_ptr(), col.data_ptr(), rowptr.data_ptr(), ctypes.byref(ka), st)
+        _native.call("cg_t_values_f64", al.data_ptr(), be.data_ptr(), Md.data_ptr(), n, m,
+                     float(reg), tv.data_ptr(), ti.data_ptr(), st)
+    fgh = fg.cpu().numpy()
+    return {"Trowsums": rows.cpu().numpy(), "Tcolsums": cols.cpu().numpy(),
+            "objfn": float(fgh[0]), "grad": grad.cpu().numpy(), "gnorm": float(fgh[1]),
+            "Tvalues": tv.cpu().numpy()[:Te], "Tflatind": ti.cpu().numpy()[:Te],
+            "csr_val": val.cpu().numpy(), "csr_rowptr": rowptr.cpu().numpy(),
+            "csr_colind": col.cpu().numpy(), "K_actual": int(ka.value)}
+
+
+def test_sparse_cholesky_solve(values, colind, rowptr, rhs):
+    values = np.asarray(values, dtype=np.float64)
+    colind = np.asarray(colind, dtype=np.int32)
+    rowptr = np.asarray(rowptr, dtype=np.int32)
+    rhs = np.asarray(rhs, dtype=np.float64)
+    if values.ndim != 1 or colind.ndim != 1 or rowptr.ndim != 1 or rhs.ndim != 1:
+        raise RuntimeError("All inputs must be 1D arrays")
+    n = rowptr.shape[0] - 1
+    if colind.shape[0] != values.shape[0]:
+        raise RuntimeError("values and colind must have the same length")
+    if rhs.shape[0] != n:
+        raise RuntimeError("rhs length must equal matrix dimension (rowptr length - 1)")
+    dev = _target_device(torch.empty(0))
+    t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+    v, c, r, b = t(values), t(colind), t(rowptr), t(rhs)
+    x = torch.empty(n, device=dev, dtype=torch.float64)
+    with torch.cuda.device(dev):
+        _native.call("cg_test_spd_solve_f64", v.data_ptr(), c.data_ptr(), r.data_ptr(), n,
+                     b.data_ptr(), x.data_ptr(), _stream_of(dev))
+    return x.cpu().numpy()

@@ -1,0 +1,203 @@
+"""Differentiable entropic-OT plan (``splr_ot``) on the native SPLR solver.
+
+Public surface and contract of the reference's curegot/autograd.py:
+``splr_ot``, ``splr_ot_with_info``, ``splr_ot_batch``, ``SPLROT`` and
+``SPLROTFunction``.  Forward = ``sinkhorn_splr_bwd`` (adopt semantics);
+backward = ``solve_backward`` (native PCG adjoint).
+
+Contract (reference autograd.py:57-126, :214-298):
+  * M, a, b are CUDA float64 tensors on one device; only M is
+    differentiable (a/b requiring grad -> NotImplementedError);
+  * wrong device/dtype -> RuntimeError, non-tensor -> TypeError, bad shapes
+    or scalars -> ValueError, autocast active -> RuntimeError;
+  * forward or backward non-convergence raises RuntimeError;
+  * double backward is unsupported (once_differentiable).
+"""
+
+from __future__ import annotations
+
+import math
+
+import torch
+from torch.autograd.function import once_differentiable
+
+from . import _solvers
+from .backward import _VALID_PRECONDITIONERS, solve_backward
+
+__all__ = ["splr_ot", "splr_ot_with_info", "splr_ot_batch", "SPLROT", "SPLROTFunction"]
+
+
+def _check_inputs(M, a, b):
+    for name, t in (("M", M), ("a", a), ("b", b)):
+        if not isinstance(t, torch.Tensor):
+            raise TypeError(f"splr_ot: {name} must be a torch.Tensor, got {type(t).__name__}")
+        if not t.is_cuda:
+            raise RuntimeError(f"splr_ot: {name} must be a CUDA tensor (CUDA float64 only)")
+        if t.dtype != torch.float64:
+            raise RuntimeError(f"splr_ot: {name} must be float64, got {t.dtype}; silent "
+                               "conversion would make the gradient dtype misleading")
+    if M.dim() != 2:
+        raise ValueError(f"splr_ot: M must be 2D (one problem per call; splr_ot_batch takes "
+                         f"[B, n, m]), got shape {tuple(M.shape)}")
+    n, m = M.shape
+    if a.dim() != 1 or a.shape[0] != n:
+        raise ValueError(f"splr_ot: a must be 1D of length {n}, got shape {tuple(a.shape)}")
+    if b.dim() != 1 or b.shape[0] != m:
+        raise ValueError(f"splr_ot: b must be 1D of length {m}, got shape {tuple(b.shape)}")
+    if not (M.device == a.device == b.device):
+        raise ValueError(f"splr_ot: M/a/b must share one device, got {M.device}, {a.device}, "
+                         f"{b.device}")
+
+
+def _validate_scalars(eta, tol, max_iter, density, candidate_sinkhorn_iter, backward_tol,
+                      backward_max_iter):
+    if not (math.isfinite(eta) and eta > 0):
+        raise ValueError(f"splr_ot: eta must be a positive finite scalar, got {eta}")
+    if not (math.isfinite(tol) and tol > 0):
+        raise ValueError(f"splr_ot: tol must be positive, got {tol}")
+    if not int(max_iter) > 0:
+        raise ValueError(f"splr_ot: max_iter must be positive, got {max_iter}")
+    if density is not None and not (0.0 < float(density) <= 1.0):
+        raise ValueError(f"splr_ot: density must be in (0, 1], got {density}")
+    if not int(candidate_sinkhorn_iter) >= 0:
+        raise ValueError(f"splr_ot: candidate_sinkhorn_iter must be >= 0, got "
+                         f"{candidate_sinkhorn_iter}")
+    if not (math.isfinite(backward_tol) and backward_tol > 0):
+        raise ValueError(f"splr_ot: backward_tol must be positive, got {backward_tol}")
+    if not int(backward_max_iter) > 0:
+        raise ValueError(f"splr_ot: backward_max_iter must be positive, got "
+                         f"{backward_max_iter}")
+
+
+def _forward_native(M, a, b, eta, tol, max_iter, density, candidate_sinkhorn_iter):
+    kwargs = {"candidate_sinkhorn_iter": int(candidate_sinkhorn_iter), "context_mode": "adopt"}
+    if density is not None:
+        kwargs["density"] = density
+    return _solvers.torch_sinkhorn_splr_bwd(M, a, b, eta, tol, max_iter, 0, **kwargs)
+
+
+class SPLROTFunction(torch.autograd.Function):
+    """Forward: native SPLR solve keeping its backward context on the autograd
+    ctx.  Backward: native implicit-gradient PCG with the chosen preconditioner."""
+
+    @staticmethod
+    def forward(ctx, M, a, b, eta, tol, max_iter, density, candidate_sinkhorn_iter,
+                backward_preconditioner, backward_tol, backward_max_iter):
+        out = _forward_native(M, a, b, eta, tol, max_iter, density, candidate_sinkhorn_iter)
+        if not bool(out["converged"]):
+            raise RuntimeError(f"splr_ot: forward solver did not converge (niter="
+                               f"{int(out['niter'])}, max_iter={max_iter}, tol={tol}); relax "
+                               "tol or increase max_iter")
+        T = out["plan"]
+        ctx.save_for_backward(T)
+        # the native context lives exactly as long as this autograd node
+        ctx.backward_context = out["context"]
+        ctx.eta = eta
+        ctx.backward_preconditioner = backward_preconditioner
+        ctx.backward_tol = backward_tol
+        ctx.backward_max_iter = backward_max_iter
+        return T
+
+    @staticmethod
+    @once_differentiable
+    def backward(ctx, grad_output):
+        (T,) = ctx.saved_tensors
+        G = grad_output if grad_output.is_contiguous() else grad_output.contiguous()
+        res = solve_backward(T, G, ctx.backward_context, ctx.eta,
+                             preconditioner=ctx.backward_preconditioner,
+                             tol=ctx.backward_tol, max_iter=ctx.backward_max_iter)
+        if not res["converged"]:
+            raise RuntimeError(f"splr_ot: backward PCG did not converge (iterations="
+                               f"{res['iterations']}, max_iter={ctx.backward_max_iter}, "
+                               f"tol={ctx.backward_tol}, "
+                               f"preconditioner='{ctx.backward_preconditioner}')")
+        return (res["grad"], None, None, None, None, None, None, None, None, None, None)
+
+
+def splr_ot(M, a, b, *, eta, tol=1e-6, max_iter=1000, density=None, candidate_sinkhorn_iter=3,
+            backward_preconditioner="diag", backward_tol=1e-12, backward_max_iter=2000):
+    """Differentiable entropic-OT plan T(M) via the SPLR solver.
+
+    M: [n, m] CUDA float64 cost (the only differentiable input); a: [n], b: [m]
+    CUDA float64 marginals (constants); eta > 0.  Returns T [n, m] with a
+    grad_fn when M requires grad.  Defaults follow the reference
+    (tol 1e-6, max_iter 1000, density min(10/min(n,m), 1), 3 candidate
+    Sinkhorn iterations, diagonal-preconditioned PCG to 1e-12, 2000 iterations).
+    """
+    if torch.is_autocast_enabled():
+        raise RuntimeError("splr_ot: AMP/autocast is unsupported (float64 solver); disable "
+                           "autocast for this call")
+    _check_inputs(M, a, b)
+    _validate_scalars(eta, tol, max_iter, density, candidate_sinkhorn_iter, backward_tol,
+                      backward_max_iter)
+    if a.requires_grad or b.requires_grad:
+        raise NotImplementedError("splr_ot: gradients w.r.t. a/b are not supported (only "
+                                  "dL/dM); detach them or use the lower-level API")
+    if backward_preconditioner not in _VALID_PRECONDITIONERS:
+        raise ValueError(f"splr_ot: invalid backward_preconditioner "
+                         f"'{backward_preconditioner}'; expected one of: "
+                         f"{' | '.join(_VALID_PRECONDITIONERS)}")
+    return SPLROTFunction.apply(M, a, b, float(eta), float(tol), int(max_iter), density,
+                                int(candidate_sinkhorn_iter), backward_preconditioner,
+                                float(backward_tol), int(backward_max_iter))
+
+
+def splr_ot_with_info(M, a, b, *, eta, tol=1e-6, max_iter=1000, density=None,
+                      candidate_sinkhorn_iter=3):
+    """Plan plus solver metadata; not differentiable, never raises on
+    non-convergence (reports ``converged`` instead)."""
+    _check_inputs(M, a, b)
+    _validate_scalars(eta, tol, max_iter, density, candidate_sinkhorn_iter, 1.0, 1)
+    with torch.no_grad():
+        out = _forward_native(M, a, b, float(eta), float(tol), int(max_iter), density,
+                              int(candidate_sinkhorn_iter))
+    return {"plan": out["plan"].detach(), "dual": out["dual"].detach(),
+            "niter": int(out["niter"]), "converged": bool(out["converged"])}
+
+
+def splr_ot_batch(M, a, b, *, eta, **kwargs):
+    """[B, n, m] costs, [B, n] and [B, m] marginals -> [B, n, m] plans;
+    gradients flow to M (one native solve per problem)."""
+    if M.dim() != 3:
+        raise ValueError(f"splr_ot_batch: M must be [B, n, m], got shape {tuple(M.shape)}")
+    B = M.shape[0]
+    if tuple(a.shape) != (B, M.shape[1]):
+        raise ValueError(f"splr_ot_batch: a must be [B, n], got shape {tuple(a.shape)}")
+    if tuple(b.shape) != (B, M.shape[2]):
+        raise ValueError(f"splr_ot_batch: b must be [B, m], got shape {tuple(b.shape)}")
+    return torch.stack([splr_ot(M[i], a[i], b[i], eta=eta, **kwargs) for i in range(B)])
+
+
+class SPLROT(torch.nn.Module):
+    """Module form of ``splr_ot`` holding its hyper-parameters (no parameters,
+    no buffers; the backward context belongs to each forward's graph)."""
+
+    def __init__(self, eta, *, tol=1e-6, max_iter=1000, density=None,
+                 candidate_sinkhorn_iter=3, backward_preconditioner="diag",
+                 backward_tol=1e-12, backward_max_iter=2000):
+        super().__init__()
+        _validate_scalars(float(eta), float(tol), int(max_iter), density,
+                          int(candidate_sinkhorn_iter), float(backward_tol),
+                          int(backward_max_iter))
+        if backward_preconditioner not in _VALID_PRECONDITIONERS:
+            raise ValueError(f"SPLROT: invalid backward_preconditioner "
+                             f"'{backward_preconditioner}'; expected one of: "
+                             f"{' | '.join(_VALID_PRECONDITIONERS)}")
+        self.eta = float(eta)
+        self.tol = float(tol)
+        self.max_iter = int(max_iter)
+        self.density = density
+        self.candidate_sinkhorn_iter = int(candidate_sinkhorn_iter)
+        self.backward_preconditioner = backward_preconditioner
+        self.backward_tol = float(backward_tol)
+        self.backward_max_iter = int(backward_max_iter)
+
+    def forward(self, M, a, b):
+        return splr_ot(M, a, b, eta=self.eta, tol=self.tol, max_iter=self.max_iter,
+                       density=self.density, candidate_sinkhorn_iter=self.candidate_sinkhorn_iter,
+                       backward_preconditioner=self.backward_preconditioner,
+                       backward_tol=self.backward_tol, backward_max_iter=self.backward_max_iter)
+
+    def extra_repr(self):
+        return (f"eta={self.eta}, tol={self.tol}, density={self.density}, "
+                f"backward_preconditioner='{self.backward_preconditioner}'")

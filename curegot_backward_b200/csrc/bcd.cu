@@ -596,7 +596,7 @@ __global__ void __launch_bounds__(kThreads, 3) bcd_col_kernel(const BcdProb* __r
       st->last_err = diff;
       if (diff < st->tol * 10) st->phase = 2;
     }
-  } else if (threadIdx.x == 0) {
+  } else if (phase == 2 && threadIdx.x == 0) {
     st->check_pending = 1;
   }
   if (threadIdx.x == 0) {

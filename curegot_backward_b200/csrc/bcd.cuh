@@ -14,7 +14,7 @@ namespace cg {
 // those of cuda_sinkhorn_bcd (reference src/sinkhorn_bcd_kernel.cu:532-592).
 struct BcdState {
   int iter;           // iterations completed so far
-  int phase;          // 1: iterate-difference test; 2: marginal test
+  int phase;          // 0: no test (fixed sweeps); 1: iterate-difference test; 2: marginal test
   int check_pending;  // the marginal test of the current iterate is due
   int done;           // converged or max_iter reached
   int niter;          // reference niter
@@ -64,6 +64,5 @@ void launch_plan(const TM* M, const double* alpha, const double* beta, double* P
 // Launch geometry for one problem.
 void bcd_geometry(int n, int m, int elem_bytes, int sm_count, BcdProb& p);
 
-int sm_count_current();
 
 }  // namespace cg

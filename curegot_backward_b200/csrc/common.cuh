@@ -38,6 +38,9 @@ inline int status_from_cuda(cudaError_t e) {
 
 void set_last_error(const char* msg, const char* file, int line);
 
+// Number of SMs of the current device.
+int sm_count_current();
+
 // Warp reductions: the result is valid in lane 0 (shfl_down tree, a fixed
 // association order, so results are bitwise reproducible).
 __device__ __forceinline__ double warp_sum_down(double v) {

@@ -1,0 +1,836 @@
+// SPLR (sparse-plus-low-rank quasi-Newton) solver driver and C ABI.
+//
+// Follows cuda_sinkhorn_splr_bwd (reference benben-cd/curegot_backward
+// src/sinkhorn_splr.cu:1305-1611; the iterate sequence is that of
+// cuda_sinkhorn_splr, :1064-1279) decision for decision: the same gauge
+// (beta_{m-1} = 0), density / shift / pattern-cycle schedule, low-rank rule,
+// candidate-Sinkhorn acceptance rule and More-Thuente style line search
+// (:667-920 with utils.h:76-230).  The host runs only that scalar control
+// flow; every vector and matrix operation runs on the device:
+//   plan pass + objective/gradient       tpass.cu
+//   sparsification into CSR              sparsify.cu
+//   direction solve                      schur.cu (cuSOLVER FP64 Cholesky)
+//   secant pair, BFGS/Woodbury, scaling  kernels below (one CTA, device scalars)
+//   candidate Sinkhorn iterate           bcd.cu passes
+// The host reads 32-64 bytes per line-search trial and per direction step.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+#include "bcd.cuh"
+#include "splr.cuh"
+#include "tpass.cuh"
+#include "workspace.cuh"
+
+namespace cg {
+
+namespace {
+
+constexpr double kInf = std::numeric_limits<double>::infinity();
+
+// ---------------------------------------------------------------------------
+// Small single-CTA vector kernels (H <= a few 10^4): fixed-order reductions.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double block_sum1024(double v, double* sh) {
+  v = warp_sum_down(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x < 32) {
+    r = sh[threadIdx.x];
+    r = warp_sum_down(r);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) sh[0] = r;
+  __syncthreads();
+  const double out = sh[0];
+  __syncthreads();
+  return out;
+}
+
+// y = g - g_prev, s = gamma - gamma_prev, ys, yy, low-rank rule
+// (sinkhorn_splr_kernel_low_rank.cu:92-206, sinkhorn_splr.cu:1378-1382).
+__global__ void __launch_bounds__(1024) lowrank_kernel(const double* g, const double* gp,
+                                                       const double* gam, const double* gamp,
+                                                       double* y, double* s, int H, int iter,
+                                                       DirRes* out) {
+  __shared__ double sh[32];
+  double ys = 0.0, yy = 0.0;
+  for (int k = threadIdx.x; k < H; k += blockDim.x) {
+    const double yv = g[k] - gp[k], sv = gam[k] - gamp[k];
+    y[k] = yv;
+    s[k] = sv;
+    ys += yv * sv;
+    yy += yv * yv;
+  }
+  ys = block_sum1024(ys, sh);
+  yy = block_sum1024(yy, sh);
+  if (threadIdx.x == 0) {
+    out->ys = ys;
+    out->yy = yy;
+    out->low_rank = (iter > 0) && (ys > 1e-6 * yy);
+  }
+}
+
+// BFGS / Woodbury correction of x = A^{-1} g with u = A^{-1} y, then
+// d = -reg * x and dg_init = <g, d>
+// (launch_low_rank_search_direc, sinkhorn_splr_kernel_low_rank.cu:296-390;
+//  compute_scaling_inplace_cuda; dot in line_search_wolfe :690).
+__global__ void __launch_bounds__(1024) woodbury_kernel(double* x, const double* u,
+                                                        const double* g, const double* y,
+                                                        const double* s, int H, double reg,
+                                                        int scale, DirRes* dr) {
+  __shared__ double sh[32];
+  const bool lr = dr->low_rank != 0;
+  if (lr) {
+    double sg = 0, yu = 0, yx = 0;
+    for (int k = threadIdx.x; k < H; k += blockDim.x) {
+      sg += s[k] * g[k];
+      yu += y[k] * u[k];
+      yx += y[k] * x[k];
+    }
+    sg = block_sum1024(sg, sh);
+    yu = block_sum1024(yu, sh);
+    yx = block_sum1024(yx, sh);
+    const double ys = dr->ys;
+    const double sg_ys = sg / ys;
+    const double term1 = (1.0 / reg + yu / ys) * sg_ys - yx / ys;
+    const double term2 = sg_ys;
+    for (int k = threadIdx.x; k < H; k += blockDim.x) x[k] += (term1 * s[k] - term2 * u[k]);
+    __syncthreads();
+  }
+  if (scale) {
+    double dg = 0.0;
+    for (int k = threadIdx.x; k < H; k += blockDim.x) {
+      const double d = -reg * x[k];
+      x[k] = d;
+      dg += g[k] * d;
+    }
+    dg = block_sum1024(dg, sh);
+    if (threadIdx.x == 0) dr->dg_init = dg;
+  }
+}
+
+// gamma <- (alpha + beta_{m-1}, beta - beta_{m-1}, 0)   (shift_gamma,
+// sinkhorn_splr_kernel.cu:156-197), from separate alpha / beta sources.
+__global__ void shift_assemble_kernel(double* gamma, const double* alpha, const double* beta,
+                                      int n, int m) {
+  const double sh = beta[m - 1];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n + m; k += gridDim.x * blockDim.x) {
+    if (k < n) gamma[k] = alpha[k] + sh;
+    else if (k < n + m - 1) gamma[k] = beta[k - n] - sh;
+    else gamma[k] = 0.0;
+  }
+}
+
+// gamma (in place) shift, for a user-supplied x0.
+__global__ void shift_inplace_kernel(double* gamma, int n, int m) {
+  __shared__ double sh;
+  if (threadIdx.x == 0) sh = gamma[n + m - 1];
+  __syncthreads();
+  const double v = sh;
+  __syncthreads();
+  for (int k = threadIdx.x; k < n + m - 1; k += blockDim.x) gamma[k] += (k < n) ? v : -v;
+  __syncthreads();
+  if (threadIdx.x == 0) gamma[n + m - 1] = 0.0;
+}
+
+// Candidate / init BCD setup: beta^0 <- beta (scaled copy too), state reset.
+__global__ void bcd_seed_kernel(const double* beta_src, int zero, double* beta0, double* betas0,
+                                int m, double s2, BcdState* st, unsigned int* counters, int nc) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+    const double v = zero ? 0.0 : beta_src[j];
+    beta0[j] = v;
+    betas0[j] = v * s2;
+  }
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nc; q += gridDim.x * blockDim.x)
+    counters[q] = 0u;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->iter = 0;
+    st->phase = 0;
+    st->check_pending = 0;
+    st->done = 0;
+    st->niter = 0;
+    st->max_iter = 1 << 30;
+    st->fast = 0;
+    st->stall = 0;
+    st->tol = 0.0;
+    st->last_err = 0.0;
+    st->best_est = 0.0;
+    st->fast_iters = 0;
+  }
+}
+
+__global__ void log_kernel(const double* a, double* out, int len) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < len; k += gridDim.x * blockDim.x)
+    out[k] = log(a[k]);
+}
+
+__global__ void inv_diag_kernel(const double* val, const int* rowptr, int n, int H, double* inv,
+                                int* err) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < H; r += gridDim.x * blockDim.x) {
+    const double v = (r < n) ? val[r] : val[rowptr[r + 1] - 1];
+    if (!(v > 0.0) || !isfinite(v)) {
+      atomicMin(err, r);
+      inv[r] = 0.0;
+    } else {
+      inv[r] = 1.0 / v;
+    }
+  }
+}
+
+template <typename T>
+int read_dev(T* host, const T* dev, cudaStream_t st) {
+  CG_TRY_CUDA(cudaMemcpyAsync(host, dev, sizeof(T), cudaMemcpyDeviceToHost, st));
+  CG_TRY_CUDA(cudaStreamSynchronize(st));
+  return CG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Line-search step selection (utils.h:76-230), identical arithmetic.
+// ---------------------------------------------------------------------------
+double quad_min_fg(double a, double b, double fa, double ga, double fb) {
+  const double ba = b - a;
+  const double w = 0.5 * ba * ga / (fa - fb + ba * ga);
+  return a + w * ba;
+}
+double quad_min_gg(double a, double b, double ga, double gb) {
+  const double w = ga / (ga - gb);
+  return a + w * (b - a);
+}
+double cubic_min(double a, double b, double fa, double fb, double ga, double gb, bool& exists) {
+  const double apb = a + b, ba = b - a, ba2 = ba * ba;
+  const double fba = fb - fa, gba = gb - ga;
+  const double z3 = (ga + gb) * ba - 2.0 * fba;
+  const double z2 = 0.5 * (gba * ba2 - 3.0 * apb * z3);
+  const double z1 = fba * ba2 - apb * z2 - (a * apb + b * b) * z3;
+  const double eps = std::numeric_limits<double>::epsilon();
+  if (std::fabs(z3) < eps * std::fabs(z2) || std::fabs(z3) < eps * std::fabs(z1)) {
+    exists = (z2 * ba > 0.0);
+    return exists ? (-0.5 * z1 / z2) : b;
+  }
+  const double u = z2 / (3.0 * z3), v = z1 / z2;
+  const double vu = v / u;
+  exists = (vu <= 1.0);
+  if (!exists) return b;
+  double r1, r2;
+  if (std::fabs(u) >= std::fabs(v)) {
+    const double w = 1.0 + std::sqrt(1.0 - vu);
+    r1 = -u * w;
+    r2 = -v / w;
+  } else {
+    const double sq = std::sqrt(std::fabs(u)) * std::sqrt(std::fabs(v)) * std::sqrt(1 - u / v);
+    r1 = -u - sq;
+    r2 = -u + sq;
+  }
+  return (z3 * ba > 0.0) ? std::max(r1, r2) : std::min(r1, r2);
+}
+double step_selection(double al, double au, double at, double fl, double fu, double ft, double gl,
+                      double gu, double gt) {
+  if (al == au) return al;
+  if (!std::isfinite(ft) || !std::isfinite(gt)) return (al + at) / 2.0;
+  bool ac_exists;
+  const double ac = cubic_min(al, at, fl, ft, gl, gt, ac_exists);
+  const double aq = quad_min_fg(al, at, fl, gl, ft);
+  if (ft > fl) {
+    if (!ac_exists) return aq;
+    return (std::fabs(ac - al) < std::fabs(aq - al)) ? ac : ((aq + ac) / 2.0);
+  }
+  const double as = quad_min_gg(al, at, gl, gt);
+  if (gt * gl < 0.0) return (std::fabs(ac - at) >= std::fabs(as - at)) ? ac : as;
+  const double deltal = 1.1, deltau = 0.66;
+  if (std::fabs(gt) < std::fabs(gl)) {
+    const bool choose_ac = ac_exists && ((ac - at) * (at - al) > 0.0) &&
+                           (std::fabs(ac - at) < std::fabs(as - at));
+    const double res = choose_ac ? ac : as;
+    return (at > al) ? std::min(at + deltau * (au - at), res)
+                     : std::max(at + deltau * (au - at), res);
+  }
+  if (!std::isfinite(au) || !std::isfinite(fu) || !std::isfinite(gu))
+    return at + deltal * (at - al);
+  bool ae_exists;
+  const double ae = cubic_min(at, au, ft, fu, gt, gu, ae_exists);
+  return (at > al) ? std::min(at + deltau * (au - at), ae) : std::max(at + deltau * (au - at), ae);
+}
+
+int grid_for(long long work, int per_block, int cap) {
+  long long g = (work + per_block - 1) / per_block;
+  return (int)std::max<long long>(1, std::min<long long>(g, cap));
+}
+
+}  // namespace
+
+// Bytes of the context-capable block (Hessian, factor, secant pair, scratch).
+static size_t hblock_bytes(int n, int m, long long kcap, int k, int lwork) {
+  const int H = n + m - 1;
+  size_t b = 0;
+  auto add = [&](size_t x) { b += (x + 255) & ~size_t(255); };
+  add((kcap + H) * sizeof(double));
+  add((kcap + H) * sizeof(int));
+  add((size_t)(H + 1) * sizeof(int));
+  add((size_t)(n + 1) * sizeof(int));
+  add(std::max<long long>(kcap, 1) * sizeof(int));
+  add(std::max<long long>(kcap, 1) * sizeof(double));
+  add((size_t)k * k * sizeof(double));
+  add(sizeof(int));
+  add((size_t)std::max(lwork, 1) * sizeof(double));
+  add(2 * (size_t)H * sizeof(double));  // rhs2 = [g, y]
+  add(2 * (size_t)H * sizeof(double));  // sol2 = [x, u]
+  add((size_t)H * sizeof(double));      // s
+  add((size_t)H * sizeof(double));      // inv_diag
+  add((size_t)H * sizeof(double));      // point
+  add((size_t)std::max(2 * k, 1) * sizeof(double));  // tmp
+  add((size_t)H * sizeof(double));      // xtmp
+  add(sizeof(DirRes));
+  add(sizeof(int));
+  return b;
+}
+
+struct HBlock {
+  SpHess A;
+  SchurFactor F;
+  double *rhs2, *sol2, *s, *inv_diag, *point, *tmp, *xtmp;
+  DirRes* dres;
+  int* err;
+};
+
+static void hblock_carve(void* base, int n, int m, long long kcap, int k, bool big_alpha,
+                         int lwork, HBlock& hb) {
+  const int H = n + m - 1;
+  char* p = static_cast<char*>(base);
+  auto take = [&](size_t x) {
+    char* q = p;
+    p += (x + 255) & ~size_t(255);
+    return q;
+  };
+  hb.A.n = n;
+  hb.A.m = m;
+  hb.A.H = H;
+  hb.A.kcap = kcap;
+  hb.A.val = reinterpret_cast<double*>(take((kcap + H) * sizeof(double)));
+  hb.A.col = reinterpret_cast<int*>(take((kcap + H) * sizeof(int)));
+  hb.A.rowptr = reinterpret_cast<int*>(take((size_t)(H + 1) * sizeof(int)));
+  hb.A.ipt = reinterpret_cast<int*>(take((size_t)(n + 1) * sizeof(int)));
+  hb.A.ij = reinterpret_cast<int*>(take(std::max<long long>(kcap, 1) * sizeof(int)));
+  hb.A.iv = reinterpret_cast<double*>(take(std::max<long long>(kcap, 1) * sizeof(double)));
+  hb.F.n = n;
+  hb.F.m = m;
+  hb.F.H = H;
+  hb.F.k = k;
+  hb.F.big_alpha = big_alpha;
+  hb.F.S = reinterpret_cast<double*>(take((size_t)k * k * sizeof(double)));
+  hb.F.info = reinterpret_cast<int*>(take(sizeof(int)));
+  hb.F.work = reinterpret_cast<double*>(take((size_t)std::max(lwork, 1) * sizeof(double)));
+  hb.F.lwork = lwork;
+  hb.rhs2 = reinterpret_cast<double*>(take(2 * (size_t)H * sizeof(double)));
+  hb.sol2 = reinterpret_cast<double*>(take(2 * (size_t)H * sizeof(double)));
+  hb.s = reinterpret_cast<double*>(take((size_t)H * sizeof(double)));
+  hb.inv_diag = reinterpret_cast<double*>(take((size_t)H * sizeof(double)));
+  hb.point = reinterpret_cast<double*>(take((size_t)H * sizeof(double)));
+  hb.tmp = reinterpret_cast<double*>(take((size_t)std::max(2 * k, 1) * sizeof(double)));
+  hb.xtmp = reinterpret_cast<double*>(take((size_t)H * sizeof(double)));
+  hb.dres = reinterpret_cast<DirRes*>(take(sizeof(DirRes)));
+  hb.err = reinterpret_cast<int*>(take(sizeof(int)));
+}
+
+template <typename TM>
+int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int n, int m,
+                      const SplrParams& prm, const double* x0, double* dual, int* niter_out,
+                      int* converged_out, cg_ctx_s** ctx_out, double* trace,
+                      cudaStream_t st) {
+  const bool f32 = sizeof(TM) == 4;
+  const double reg = prm.reg;
+  if (!M || !a || !b || n <= 0 || m <= 0 || !(reg > 0.0) || !std::isfinite(reg) ||
+      prm.cycle <= 0) {
+    set_last_error("cg_splr: invalid argument", __FILE__, __LINE__);
+    return CG_ERR_INVALID_ARG;
+  }
+  if ((long long)(n + m) * (n + m) >= (1LL << 31)) {
+    set_last_error("cg_splr: n + m too large for 32-bit Hsl indices", __FILE__, __LINE__);
+    return CG_ERR_INVALID_ARG;
+  }
+  const int H = n + m - 1;
+  const long long Te = (long long)n * (m - 1);
+  const int cand = prm.cand_iter < 0 ? 3 : prm.cand_iter;
+  double density_max = std::min(std::max(prm.density_max, 0.0), 1.0);
+  const double density_min = 0.01 * density_max;
+  double density = 0.1 * density_max;
+  long long Kmax = (long long)(density_max * n * (m - 1));
+  Kmax = std::max(Kmax, 1LL);
+  const double s2 = kLog2e / reg;
+  const int sms = sm_count_current();
+
+  int k = 0;
+  bool big_alpha = true;
+  schur_dims(n, m, k, big_alpha);
+  cusolverDnHandle_t sol = nullptr;
+  CG_TRY(solver_handle(&sol));
+  int lwork = 0;
+  CG_TRY(schur_lwork(sol, k, lwork));
+
+  // context-capable block (plain cudaMalloc: it may outlive the stream)
+  const size_t hbytes = hblock_bytes(n, m, Kmax, k, lwork);
+  void* hbase = nullptr;
+  CG_TRY_CUDA(cudaMalloc(&hbase, hbytes));
+  HBlock hb;
+  hblock_carve(hbase, n, m, Kmax, k, big_alpha, lwork, hb);
+  struct Guard {
+    void*& p;
+    ~Guard() {
+      if (p) cudaFree(p);
+    }
+  } hguard{hbase};
+
+  // per-solve workspace
+  int tstrips = 1, tsplits = 1;
+  tpass_geometry(n, m, sms, tstrips, tsplits);
+  BcdProb cp{};
+  bcd_geometry(n, m, (int)sizeof(TM), sms, cp);
+  const int bcount = 2 + cp.col_strips;
+  Workspace ws(st);
+  const size_t o_ab = ws.reserve<double>(n + m), o_logab = ws.reserve<double>(n + m);
+  const size_t o_g = ws.reserve<double>(n + m), o_gp = ws.reserve<double>(n + m);
+  const size_t o_gb = ws.reserve<double>(n + m);
+  const size_t o_gr = ws.reserve<double>(H), o_grp = ws.reserve<double>(H);
+  const size_t o_grc = ws.reserve<double>(H);
+  const size_t o_rows = ws.reserve<double>(n), o_cols = ws.reserve<double>(m);
+  const size_t o_rowsc = ws.reserve<double>(n), o_colsc = ws.reserve<double>(m);
+  const size_t o_res = ws.reserve<TResult>(2);
+  const size_t o_tw = ws.reserve<double>(tpass_workspace_doubles(n, m, tstrips, tsplits));
+  const size_t o_tc = ws.reserve<unsigned int>(tsplits + tstrips + 1);
+  const size_t o_sw = ws.reserve<char>(sparsify_work_bytes(n, m));
+  size_t o_bal[2], o_bbe[2], o_bals[2], o_bbes[2];
+  for (int q = 0; q < 2; ++q) {
+    o_bal[q] = ws.reserve<double>(n);
+    o_bbe[q] = ws.reserve<double>(m);
+    o_bals[q] = ws.reserve<double>(n);
+    o_bbes[q] = ws.reserve<double>(m);
+  }
+  const size_t bparts = (cp.col_splits > 1) ? (size_t)cp.col_splits * m : 1;
+  const size_t o_bcm = ws.reserve<double>(bparts), o_bcs = ws.reserve<double>(bparts);
+  const size_t o_brp = ws.reserve<double>((size_t)cp.row_ctas * 4);
+  const size_t o_bcp = ws.reserve<double>((size_t)cp.col_strips * 3);
+  const size_t o_bcnt = ws.reserve<unsigned int>(bcount);
+  const size_t o_bst = ws.reserve<BcdState>(1);
+  const size_t o_bprob = ws.reserve<BcdProb>(1);
+  CG_TRY(ws.allocate());
+
+  double* ab = ws.at<double>(o_ab);
+  double* logab = ws.at<double>(o_logab);
+  double* gamma = ws.at<double>(o_g);
+  double* gamma_prev = ws.at<double>(o_gp);
+  double* gamma_bcd = ws.at<double>(o_gb);
+  double* grad = ws.at<double>(o_gr);
+  double* grad_prev = ws.at<double>(o_grp);
+  double* grad_c = ws.at<double>(o_grc);
+  double* rows = ws.at<double>(o_rows);
+  double* cols = ws.at<double>(o_cols);
+  double* rows_c = ws.at<double>(o_rowsc);
+  double* cols_c = ws.at<double>(o_colsc);
+  TResult* res = ws.at<TResult>(o_res);
+  TResult* res_c = res + 1;
+  double* tw = ws.at<double>(o_tw);
+  unsigned int* tcnt = ws.at<unsigned int>(o_tc);
+  SparsifyWork sw;
+  sparsify_work_carve(ws.at<char>(o_sw), n, m, sw);
+
+  cp.M = M;
+  cp.n = n;
+  cp.m = m;
+  cp.eta = reg;
+  cp.s2 = s2;
+  cp.a = ab;
+  cp.loga = logab;
+  cp.logb = logab + n;
+  for (int q = 0; q < 2; ++q) {
+    cp.alpha[q] = ws.at<double>(o_bal[q]);
+    cp.beta[q] = ws.at<double>(o_bbe[q]);
+    cp.alphas[q] = ws.at<double>(o_bals[q]);
+    cp.betas[q] = ws.at<double>(o_bbes[q]);
+  }
+  cp.col_m = ws.at<double>(o_bcm);
+  cp.col_s = ws.at<double>(o_bcs);
+  cp.row_part = ws.at<double>(o_brp);
+  cp.col_part = ws.at<double>(o_bcp);
+  cp.counters = ws.at<unsigned int>(o_bcnt);
+  cp.st = ws.at<BcdState>(o_bst);
+  BcdProb* dcp = ws.at<BcdProb>(o_bprob);
+
+  CG_TRY_CUDA(cudaMemcpyAsync(ab, a, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  CG_TRY_CUDA(cudaMemcpyAsync(ab + n, b, m * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  log_kernel<<<grid_for(n + m, 256, 1024), 256, 0, st>>>(ab, logab, n + m);
+  CG_TRY_CUDA(cudaMemcpyAsync(dcp, &cp, sizeof(BcdProb), cudaMemcpyHostToDevice, st));
+  CG_TRY_CUDA(cudaMemsetAsync(tcnt, 0, (tsplits + tstrips + 1) * sizeof(unsigned int), st));
+  CG_TRY_CUDA(cudaMemsetAsync(gamma_prev, 0, (n + m) * sizeof(double), st));
+  CG_TRY_CUDA(cudaMemsetAsync(grad_prev, 0, H * sizeof(double), st));
+  CG_TRY_CUDA(cudaMemsetAsync(hb.dres, 0, sizeof(DirRes), st));
+
+  // T-pass launcher
+  TPassArgs ta{};
+  ta.M = M;
+  ta.n = n;
+  ta.m = m;
+  ta.eta = reg;
+  ta.s2 = s2;
+  ta.ab = ab;
+  ta.strips = tstrips;
+  ta.splits = tsplits;
+  ta.rowpart = tw;
+  ta.colpart = tw + (size_t)tstrips * n;
+  ta.scal = tw + (size_t)tstrips * n + (size_t)tsplits * m;
+  ta.counters = tcnt;
+  auto eval_at = [&](double* g, double* gr, double* r, double* c, TResult* out, TResult& host,
+                     const double* dir) -> int {
+    TPassArgs x = ta;
+    x.gamma = g;
+    x.gamma_prev = nullptr;
+    x.direc = dir;
+    x.step = 0.0;
+    x.trial = 0;
+    x.rows = r;
+    x.cols = c;
+    x.grad = gr;
+    x.res = out;
+    CG_TRY(launch_tpass(f32, x, st));
+    return read_dev(&host, out, st);
+  };
+  auto trial_at = [&](double step, TResult& host) -> int {
+    TPassArgs x = ta;
+    x.gamma = gamma;
+    x.gamma_prev = gamma_prev;
+    x.direc = hb.sol2;
+    x.step = step;
+    x.trial = 1;
+    x.rows = rows;
+    x.cols = cols;
+    x.grad = grad;
+    x.res = res;
+    CG_TRY(launch_tpass(f32, x, st));
+    return read_dev(&host, res, st);
+  };
+  const int bgrid = grid_for(m, 256, 1024);
+  // alpha_bcd = A(beta) then `sweeps` x (beta, alpha): BCD passes, phase 0.
+  auto bcd_sweeps = [&](const double* beta_src, bool zero_beta, int sweeps) {
+    bcd_seed_kernel<<<bgrid, 256, 0, st>>>(beta_src, zero_beta ? 1 : 0, cp.beta[0], cp.betas[0],
+                                           m, s2, cp.st, cp.counters, bcount);
+    launch_bcd_row(f32, dcp, nullptr, nullptr, cp.row_ctas, st);
+    for (int q = 0; q < sweeps; ++q) {
+      launch_bcd_col(f32, dcp, nullptr, nullptr, cp.col_strips * cp.col_splits, st);
+      launch_bcd_row(f32, dcp, nullptr, nullptr, cp.row_ctas, st);
+    }
+  };
+
+  // init_dual (sinkhorn_splr.cu:330-359)
+  if (x0) {
+    CG_TRY_CUDA(cudaMemcpyAsync(gamma, x0, (n + m) * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    shift_inplace_kernel<<<1, 1024, 0, st>>>(gamma, n, m);
+  } else {
+    bcd_sweeps(nullptr, true, 0);
+    // alpha in buffer 1, beta = 0
+    CG_TRY_CUDA(cudaMemcpyAsync(gamma, cp.alpha[1], n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CG_TRY_CUDA(cudaMemsetAsync(gamma + n, 0, m * sizeof(double), st));
+  }
+  CG_TRY_CUDA(cudaGetLastError());
+
+  TResult tr{};
+  CG_TRY(eval_at(gamma, grad, rows, cols, res, tr, nullptr));
+  double objfn = tr.f, gnorm = tr.gnorm;
+  const double gnorm_init = gnorm;
+  double shift = std::min(gnorm, prm.shift_max);
+  long long Kcur = 0;
+
+  auto dual_sphess = [&](double dens, double sh, bool fixed) -> int {
+    dens = std::min(std::max(dens, 0.0), 1.0);
+    long long K = (long long)(dens * (double)Te);
+    K = std::min(K, Kmax);
+    K = std::max(K, 1LL);
+    long long Ks = std::min(std::max(K, 1LL), Te);
+    Kcur = Ks;
+    if (fixed) return sparsify_refresh(f32, M, gamma, rows, cols, n, m, s2, sh, hb.A, st);
+    return sparsify_select_and_build(f32, M, gamma, rows, cols, n, m, s2, sh, Ks, hb.A, sw, st);
+  };
+  CG_TRY(dual_sphess(density, shift * reg, false));
+
+  double alpha_step = 1.0;
+  double ys = 0.0, yy = 0.0;
+  bool low_rank = false, converged = false, invalid_state = false;
+  int niter = 0;
+  for (int iter = 0; iter < prm.max_iter; ++iter) {
+    if (prm.verbose >= 1)
+      printf("iter = %d, objval = %.10g, ||grad|| = %.10g\n", iter, objfn, gnorm);
+    if (gnorm < prm.tol) {
+      converged = true;
+      break;
+    }
+    if (!std::isfinite(objfn)) break;
+
+    lowrank_kernel<<<1, 1024, 0, st>>>(grad, grad_prev, gamma, gamma_prev, hb.rhs2 + H, hb.s, H,
+                                       iter, hb.dres);
+    const bool analyze = (iter % prm.cycle == 0);
+    const bool update = (iter % prm.cycle == (prm.cycle - 1));
+
+    // candidate Sinkhorn iterate from the current beta (sinkhorn_splr.cu:441-526)
+    TResult trc{};
+    const bool use_cand = analyze && (cand != 0);
+    if (use_cand) {
+      bcd_sweeps(gamma + n, false, cand);
+      shift_assemble_kernel<<<grid_for(n + m, 256, 1024), 256, 0, st>>>(
+          gamma_bcd, cp.alpha[(cand + 1) & 1], cp.beta[cand & 1], n, m);
+      CG_TRY(eval_at(gamma_bcd, grad_c, rows_c, cols_c, res_c, trc, nullptr));
+    }
+
+    // search direction (sinkhorn_splr.cu:538-649)
+    CG_TRY_CUDA(cudaMemcpyAsync(hb.rhs2, grad, H * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CG_TRY(schur_factor(sol, hb.A, hb.F, st));
+    const int nrhs = (iter > 0) ? 2 : 1;
+    CG_TRY(schur_solve(sol, hb.A, hb.F, hb.rhs2, hb.sol2, nrhs, hb.tmp, st));
+    woodbury_kernel<<<1, 1024, 0, st>>>(hb.sol2, hb.sol2 + H, grad, hb.rhs2 + H, hb.s, H, reg, 1,
+                                        hb.dres);
+    CG_TRY_CUDA(cudaGetLastError());
+    DirRes dr{};
+    int info = 0;
+    CG_TRY_CUDA(cudaMemcpyAsync(&info, hb.F.info, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CG_TRY(read_dev(&dr, hb.dres, st));
+    if (info != 0) {
+      set_last_error("direction solve: Schur complement not positive definite", __FILE__,
+                     __LINE__);
+      return CG_ERR_NOT_SPD;
+    }
+    ys = dr.ys;
+    yy = dr.yy;
+    low_rank = dr.low_rank != 0;
+
+    // save_history (first H entries)
+    CG_TRY_CUDA(cudaMemcpyAsync(gamma_prev, gamma, H * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CG_TRY_CUDA(cudaMemcpyAsync(grad_prev, grad, H * sizeof(double), cudaMemcpyDeviceToDevice, st));
+
+    // line_search_wolfe (sinkhorn_splr.cu:667-920)
+    bool recompute_fg = false;
+    int trials = 0;
+    double step_out = 0.0;
+    double last_trial_gnorm = gnorm;
+    {
+      const double c1 = 1e-4, c2 = 0.9;
+      const int ls_max = 20;
+      const double step_min = 1e-10, step_max = 2.0;
+      double init_step = std::min(1.0, 1.5 * alpha_step);
+      init_step = std::max(init_step, step_min);
+      init_step = std::min(init_step, step_max);
+      double step = init_step;
+      double dg = dr.dg_init;
+      double fx = objfn;
+      const double fx_init = objfn;
+      const double dg_init = dg;
+      bool done = false;
+      if (dg_init > 0.0) {
+        recompute_fg = true;
+        step_out = init_step;
+        done = true;
+      }
+      if (!done) {
+        const double test_decr = c1 * dg_init;
+        const double test_curv = -c2 * dg_init;
+        double I_lo = 0.0, I_hi = kInf;
+        double fI_lo = 0.0, fI_hi = kInf;
+        double gI_lo = (1.0 - c1) * dg_init, gI_hi = kInf;
+        double psiI_lo = fI_lo;
+        bool bracketed = false;
+        bool use_step_min_safeguard = (step_min > 0.0);
+        double I_width = kInf, I_width_prev = kInf;
+        int I_shrink_fail_count = 0;
+        const double delta_max = 1.1, delta_min = 7.0 / 12, shrink = 0.66;
+        for (int it = 0; it < ls_max && !done; ++it) {
+          TResult t{};
+          CG_TRY(trial_at(step, t));
+          ++trials;
+          fx = t.f;
+          dg = t.dg;
+          objfn = fx;
+          last_trial_gnorm = t.gnorm;
+          const double psit = fx - fx_init - step * test_decr;
+          const double dpsit = dg - test_decr;
+          if (psit <= 0.0 && std::fabs(dg) <= test_curv) { step_out = step; done = true; break; }
+          if (step <= step_min && (psit > 0.0 || dpsit >= 0.0)) { step_out = step; done = true; break; }
+          if (step >= step_max && (psit <= 0.0 && dpsit < 0.0)) { step_out = step; done = true; break; }
+          const double ft = psit, gt = dpsit;  // f is psi (reference keeps f_is_psi = true)
+          if (use_step_min_safeguard && (psit <= 0.0 && dpsit < 0.0)) use_step_min_safeguard = false;
+          double new_step;
+          const bool in_case_2 = (psit <= psiI_lo) && (dpsit * (I_lo - step) > 0.0);
+          if (in_case_2) {
+            new_step = std::min(step_max, step + delta_max * (step - I_lo));
+          } else {
+            new_step = step_selection(I_lo, I_hi, step, fI_lo, fI_hi, ft, gI_lo, gI_hi, gt);
+            new_step = std::max(new_step, step_min);
+            new_step = std::min(new_step, step_max);
+            if (use_step_min_safeguard) {
+              const double lower = step_min;
+              const double upper = std::max(step_min, delta_min * step);
+              new_step = std::max(new_step, lower);
+              new_step = std::min(new_step, upper);
+            }
+          }
+          if (psit > psiI_lo) {
+            I_hi = step; fI_hi = ft; gI_hi = gt;
+          } else if (in_case_2) {
+            I_lo = step; fI_lo = ft; gI_lo = gt; psiI_lo = psit;
+          } else {
+            I_hi = I_lo; fI_hi = fI_lo; gI_hi = gI_lo;
+            I_lo = step; fI_lo = ft; gI_lo = gt; psiI_lo = psit;
+          }
+          if (!bracketed && !in_case_2) {
+            const double I_left = std::min(I_lo, I_hi);
+            const double I_right = std::max(I_lo, I_hi);
+            bracketed = (I_left >= step_min && I_right <= step_max);
+          }
+          if (bracketed) {
+            I_width_prev = I_width;
+            I_width = std::fabs(I_hi - I_lo);
+            if (I_width_prev < kInf && I_width > shrink * I_width_prev) I_shrink_fail_count += 1;
+            else I_shrink_fail_count = 0;
+            if (I_shrink_fail_count >= 2) {
+              new_step = (I_lo + I_hi) / 2.0;
+              I_shrink_fail_count = 0;
+            }
+          }
+          step = new_step;
+        }
+        if (!done) {
+          const double psit = fx - fx_init - step * test_decr;
+          if (psit <= psiI_lo) {
+            step_out = step;
+          } else if (I_lo <= 0.0) {
+            recompute_fg = true;
+            step_out = init_step;
+          } else {
+            recompute_fg = true;
+            step_out = I_lo;
+          }
+        }
+      }
+    }
+    alpha_step = step_out;
+
+    const double gnorm_pre = gnorm;
+    if (recompute_fg) {
+      TResult t{};
+      CG_TRY(trial_at(alpha_step, t));
+      objfn = t.f;
+      gnorm = t.gnorm;
+    } else {
+      gnorm = last_trial_gnorm;  // f, g and ||g|| of the last trial are current
+    }
+
+    bool cand_accepted = false;
+    if (use_cand) {
+      if ((trc.f < objfn) && (trc.gnorm < 10 * gnorm)) {
+        cand_accepted = true;
+        CG_TRY_CUDA(cudaMemcpyAsync(gamma, gamma_bcd, H * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        TResult t{};
+        CG_TRY(eval_at(gamma, grad, rows, cols, res, t, nullptr));
+        objfn = t.f;
+        gnorm = t.gnorm;
+      }
+    }
+
+    if (update) {
+      const bool bad_move = (gnorm_pre < gnorm_init) && (gnorm > gnorm_pre);
+      density *= (bad_move ? 1.1 : 0.99);
+      density = std::min(density_max, std::max(density_min, density));
+    }
+
+    if (trace) {
+      double* t = trace + (size_t)iter * 8;
+      t[0] = objfn; t[1] = gnorm; t[2] = alpha_step; t[3] = (double)Kcur;
+      t[4] = low_rank; t[5] = recompute_fg; t[6] = cand_accepted; t[7] = trials;
+    }
+
+    const bool converged_after = std::isfinite(gnorm) && (gnorm < prm.tol);
+    const bool max_iter_reached = (iter + 1 >= prm.max_iter);
+    const bool invalid_after = !std::isfinite(objfn) || !std::isfinite(gnorm);
+    const bool stop_after = converged_after || max_iter_reached || invalid_after;
+    if (!stop_after) {
+      shift = std::min(gnorm, prm.shift_max);
+      CG_TRY(dual_sphess(density, shift * reg, !update));
+    }
+    niter = iter + 1;
+    if (stop_after) {
+      if (invalid_after) invalid_state = true;
+      if (!max_iter_reached && converged_after) converged = true;
+      break;
+    }
+  }
+
+  if (niter_out) *niter_out = niter;
+  if (converged_out) *converged_out = converged ? 1 : 0;
+  if (Pout) launch_plan<TM>(M, gamma, gamma + n, Pout, 1.0 / reg, n, m, st);
+  if (dual) CG_TRY_CUDA(cudaMemcpyAsync(dual, gamma, (n + m) * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  CG_TRY_CUDA(cudaGetLastError());
+
+  if (ctx_out) {
+    *ctx_out = nullptr;
+    cg_ctx_s* c = new cg_ctx_s();
+    CG_TRY_CUDA(cudaGetDevice(&c->device));
+    c->n = n;
+    c->m = m;
+    c->H = H;
+    c->reg = reg;
+    c->valid = !(invalid_state || !std::isfinite(objfn));
+    c->fallback = (niter == 0);
+    if (c->fallback) {
+      // immediate convergence: factor the sparsified Hessian at the final
+      // point, no low-rank correction (sinkhorn_splr.cu:1592-1600)
+      c->ys = 0.0;
+      c->low_rank = false;
+      if (c->valid) {
+        int rc = schur_factor(sol, hb.A, hb.F, st);
+        if (rc != CG_OK) {
+          delete c;
+          return rc;
+        }
+      }
+    } else {
+      c->ys = ys;
+      c->low_rank = low_rank;
+    }
+    c->A = hb.A;
+    c->F = hb.F;
+    c->s = hb.s;
+    c->y = hb.rhs2 + H;
+    c->u = hb.sol2 + H;
+    c->inv_diag = hb.inv_diag;
+    c->point = hb.point;
+    c->tmp = hb.tmp;
+    c->xtmp = hb.xtmp;
+    c->dres = hb.dres;
+    c->err = hb.err;
+    int rp = 0;
+    CG_TRY_CUDA(cudaMemcpyAsync(&rp, hb.A.rowptr + H, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CG_TRY_CUDA(cudaMemcpyAsync(c->point, c->fallback ? gamma : gamma_prev, H * sizeof(double),
+                                cudaMemcpyDeviceToDevice, st));
+    int info = 0;
+    CG_TRY_CUDA(cudaMemcpyAsync(&info, hb.F.info, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CG_TRY_CUDA(cudaStreamSynchronize(st));
+    c->nnz = rp;
+    c->has_point = true;
+    if (info != 0) c->valid = false;
+    c->block = hbase;
+    hbase = nullptr;  // ownership moves to the context
+    *ctx_out = c;
+  }
+  ws.release();
+  return CG_OK;
+}
+
+template int splr_solve<double>(const double*, const double*, const double*, double*, int, int,
+                                const SplrParams&, const double*, double*, int*, int*,
+                                cg_ctx_s**, double*, cudaStream_t);
+template int splr_solve<float>(const float*, const double*, const double*, double*, int, int,
+                               const SplrParams&, const double*, double*, int*, int*,
+                               cg_ctx_s**, double*, cudaStream_t);
+
+}  // namespace cg

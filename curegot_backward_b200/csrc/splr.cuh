@@ -1,0 +1,57 @@
+// SPLR solver internals shared by the driver, the backward context and the
+// adjoint (PCG) solver.
+#pragma once
+
+#include "schur.cuh"
+
+struct cg_ctx_s;
+
+namespace cg {
+
+// Small device-side results of the direction step.
+struct DirRes {
+  double ys, yy, dg_init;
+  int low_rank;
+  int pad;
+};
+
+struct SplrParams {
+  double reg, tol;
+  int max_iter;
+  double density_max, shift_max;
+  int cycle, cand_iter, verbose;
+};
+
+// The SPLR solve (splr.cu).  M is float (mixed) or double; everything else FP64.
+template <typename TM>
+int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int n, int m,
+               const SplrParams& prm, const double* x0, double* dual, int* niter_out,
+               int* converged_out, cg_ctx_s** ctx_out, double* trace, cudaStream_t st);
+
+}  // namespace cg
+
+// Backward context (opaque to C callers).  Owns the sparsified Hessian A_k of
+// the last forward direction solve (CSR + per-row lists), its Schur factor,
+// the secant pair and A_k^{-1} y_k -- the state the reference's
+// SPLRBackwardContext adopts from the forward solver
+// (src/backward_context.h:83-376).
+struct cg_ctx_s {
+  int device = 0;
+  int n = 0, m = 0, H = 0;
+  double reg = 0.0, ys = 0.0;
+  bool low_rank = false, fallback = false, valid = false, has_point = false;
+  bool diag_ready = false;
+  long long nnz = 0;
+  void* block = nullptr;  // single allocation owning every device buffer below
+  cg::SpHess A;
+  cg::SchurFactor F;
+  double* s = nullptr;
+  double* y = nullptr;
+  double* u = nullptr;  // A^{-1} y
+  double* inv_diag = nullptr;
+  double* point = nullptr;
+  double* tmp = nullptr;  // [k] solve scratch
+  double* xtmp = nullptr; // [H] solve scratch
+  cg::DirRes* dres = nullptr;
+  int* err = nullptr;
+};

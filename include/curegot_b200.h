@@ -78,6 +78,108 @@ int cg_transport_plan_mixed(const float* M, const double* alpha, const double* b
                             double* P, double reg, int n, int m, cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
+/* SPLR (sparse-plus-low-rank quasi-Newton) and its backward context.        */
+/* ------------------------------------------------------------------------ */
+
+/* Opaque backward context: the sparsified Hessian A_k of the last forward
+ * direction solve with its factorization, the secant pair (s, y), A_k^{-1} y
+ * and ys.  Replaces SPLRBackwardContext (src/backward_context.h:83-376). */
+typedef struct cg_ctx_s cg_ctx;
+
+typedef struct {
+  int n, m, dim;          /* dim = n + m - 1 (reduced dual)                  */
+  long long nnz;          /* entries of the context CSR                      */
+  double reg, ys;
+  int low_rank;           /* rank-2 correction active                         */
+  int fallback;           /* immediate convergence: factor at the final point */
+  int valid;              /* forward state finite; usable for backward        */
+  int has_diag;           /* diagonal preconditioner set up                   */
+  int has_point;          /* context point available                          */
+  int adopted;            /* forward factorization adopted (not a fallback)   */
+} cg_ctx_info_t;
+
+enum { CG_PRECOND_NONE = 0, CG_PRECOND_DIAG = 1, CG_PRECOND_SPLR = 2 };
+enum {
+  CG_CTX_CSR_VALUES = 0, CG_CTX_CSR_COLIND = 1, CG_CTX_CSR_ROWPTR = 2, CG_CTX_SECANT_S = 3,
+  CG_CTX_SECANT_Y = 4, CG_CTX_INV_DIAG = 5, CG_CTX_POINT = 6, CG_CTX_INVA_Y = 7
+};
+
+/*
+ * Plain FP64 SPLR.  Replaces cuda_sinkhorn_splr / cuda_sinkhorn_splr_bwd
+ * (src/solvers.h:11-33; src/sinkhorn_splr.cu:1064-1611) on device pointers.
+ * density_max, shift_max, sparsity_pattern_cycle and candidate_sinkhorn_iter
+ * mean what the reference's kwargs mean (src/solvers_torch.cpp:212-243).
+ * ctx_out (nullable): export the backward context (adopt semantics; fallback
+ * factorization when niter == 0).  converged (nullable): the reference's
+ * converged flag.  trace (nullable, HOST, 8 doubles x max_iter): per
+ * iteration f, ||g||, step, K, low_rank, recompute_fg, candidate accepted,
+ * line-search trials.  The direction solve is an exact FP64 solve with the
+ * sparsified Hessian (Schur complement + cuSOLVER Cholesky) in place of cuDSS.
+ */
+int cg_splr_f64(const double* M, const double* a, const double* b, double* P, double reg,
+                int max_iter, double tol, int n, int m, int* niter, double density_max,
+                double shift_max, int sparsity_pattern_cycle, int candidate_sinkhorn_iter,
+                int verbose, const double* x0, double* dual, cg_ctx** ctx_out, int* converged,
+                double* trace, cudaStream_t stream);
+/* Same with M in FP32 (all arithmetic, duals, line search and solve in FP64). */
+int cg_splr_mixed(const float* M, const double* a, const double* b, double* P, double reg,
+                  int max_iter, double tol, int n, int m, int* niter, double density_max,
+                  double shift_max, int sparsity_pattern_cycle, int candidate_sinkhorn_iter,
+                  int verbose, const double* x0, double* dual, cg_ctx** ctx_out,
+                  int* converged, double* trace, cudaStream_t stream);
+
+/* Context properties (reg, dim, low_rank_enabled, is_fallback, ...;
+ * src/solvers_torch.cpp:691-696). */
+int cg_ctx_info(const cg_ctx* ctx, cg_ctx_info_t* out);
+/* One-time D_A^{-1} extraction, validated (backward_context.cu:616-640). */
+int cg_ctx_setup_diag(cg_ctx* ctx, cudaStream_t stream);
+/* z = B^{-1} r (mode CG_PRECOND_SPLR: factor solve + rank-2 Woodbury,
+ * backward_context.cu:543-581) or z = D_A^{-1} r (CG_PRECOND_DIAG,
+ * backward_context.cu:642-655).  r, z: device [dim]. */
+int cg_ctx_apply(cg_ctx* ctx, const double* r, double* z, int mode, cudaStream_t stream);
+/* Copies a context array (CG_CTX_*) to device memory dst
+ * (csr_values/csr_colind/csr_rowptr/secant_s/secant_y/inv_diag/ctx_point,
+ * src/solvers_torch.cpp:583-647). */
+int cg_ctx_copy(const cg_ctx* ctx, int what, void* dst, cudaStream_t stream);
+/* Releases the context (factorization first, then its buffers). */
+int cg_ctx_destroy(cg_ctx* ctx);
+
+/*
+ * Implicit backward: solves Q(T) lambda = mu with PCG and assembles
+ * dL/dM = T * (lambda_a 1^T + 1 lambda_b^T - G) / eta.  Replaces
+ * solve_backward / pcg / q_matvec / rhs_Q_scale / assemble_grad
+ * (curegot/backward.py:72-144, curegot/_backward_core.py:31-83).
+ * precond: CG_PRECOND_NONE | CG_PRECOND_DIAG | CG_PRECOND_SPLR (ctx may be
+ * NULL for NONE).  T, G: device n x m; lambda: device [n+m-1]; grad: device
+ * n x m.  iterations / converged: host.  A PCG breakdown (p^T A p <= 0)
+ * returns CG_ERR_NOT_SPD.
+ */
+int cg_backward_f64(const double* T, const double* G, cg_ctx* ctx, double eta, int precond,
+                    double tol, int max_iter, int n, int m, double* lambda, double* grad,
+                    int* iterations, int* converged, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Test hooks of the reference (curegot.tests, src/tests.cpp:36-200).        */
+/* ------------------------------------------------------------------------ */
+
+/* T_t values and flat Hsl indices (i*(m-1)+j -> (n+j)*(n+m-1)+i); the
+ * Tvalues / Tflatind outputs of T_computation_sparsify_host. */
+int cg_t_values_f64(const double* alpha, const double* beta, const double* M, int n, int m,
+                    double reg, double* Tvalues, int* Tflatind, cudaStream_t stream);
+/* T pass + objective/gradient + top-K sparsification into CSR
+ * (T_computation_sparsify_host, src/sinkhorn_splr_kernel.cu:909-1032).
+ * Device arrays; objfn_gnorm: device [2]; k_actual: host. */
+int cg_test_t_sparsify_f64(const double* alpha, const double* beta, const double* M,
+                           const double* a, const double* b, double reg, double shift, int K,
+                           int n, int m, double* rows, double* cols, double* grad,
+                           double* objfn_gnorm, double* csr_val, int* csr_colind,
+                           int* csr_rowptr, long long* k_actual, cudaStream_t stream);
+/* SPD solve with a CSR matrix (full or lower storage, lower triangle read)
+ * (sparse_cholesky_solve_host, src/linsolve.cu:312-350).  Device arrays. */
+int cg_test_spd_solve_f64(const double* values, const int* colind, const int* rowptr, int n,
+                          const double* rhs, double* x, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
 /* Diagnostics (no reference counterpart).                                   */
 /* ------------------------------------------------------------------------ */
 

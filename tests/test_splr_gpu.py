@@ -1,0 +1,173 @@
+"""GPU parity of the SPLR path: reference golden fixtures through the
+reference's test-hook API, and full solves against the CPU oracle
+(identical niter and sparsity pattern, duals within 1e-10 relative, plan
+within 1e-12 absolute)."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import curegot_backward_b200 as cg
+import oracle
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_T_computation_sparsify_golden(cuda_dev):
+    g = np.load(os.path.join(GOLD, "csr_n6_m3.npz"))
+    r = cg.tests.test_T_computation_sparsify(g["alpha"], g["beta"], g["M"], g["a"], g["b"],
+                                             float(g["reg"]), float(g["shift"]), int(g["K"]))
+    for k in ("Trowsums", "Tcolsums", "grad", "csr_val"):
+        assert np.linalg.norm(r[k] - g[k]) < 1e-8, k
+    assert np.array_equal(r["csr_colind"], g["csr_colind"])
+    assert np.array_equal(r["csr_rowptr"], g["csr_rowptr"])
+    assert abs(r["objfn"] - g["objfn"]) < 1e-8 and abs(r["gnorm"] - g["gnorm"]) < 1e-8
+    assert r["K_actual"] == 10
+    # T_t values / flat indices (reference layout)
+    n, m = g["M"].shape
+    T = np.exp((g["alpha"][:, None] + g["beta"][None, :] - g["M"]) / float(g["reg"]))
+    assert np.allclose(r["Tvalues"], T[:, :-1].ravel(), rtol=1e-14, atol=0)
+    jj, ii = np.meshgrid(np.arange(m - 1), np.arange(n))
+    assert np.array_equal(r["Tflatind"], ((n + jj) * (n + m - 1) + ii).ravel())
+
+
+@pytest.mark.parametrize("n", [10, 100, 1000, 10000])
+def test_sparse_cholesky_golden(cuda_dev, n):
+    s = np.load(os.path.join(GOLD, f"spd_n{n}.npz"))
+    for kind in ("full", "lower"):
+        x = cg.tests.test_sparse_cholesky_solve(s[f"{kind}_val"], s[f"{kind}_col"],
+                                                s[f"{kind}_rowptr"], s["rhs"])
+        assert np.linalg.norm(x - s["x"]) < 1e-8
+
+
+@pytest.mark.parametrize("n,m,K,seed", [(50, 40, 37, 1), (40, 70, 400, 2), (129, 65, 1, 3),
+                                        (33, 2, 5, 4), (64, 64, 64 * 63, 5)])
+def test_sparsify_matches_oracle(cuda_dev, n, m, K, seed):
+    rng = np.random.default_rng(seed)
+    alpha, beta = rng.normal(scale=0.1, size=n), rng.normal(scale=0.1, size=m)
+    M = rng.uniform(size=(n, m))
+    a = rng.uniform(size=n); a /= a.sum()
+    b = rng.uniform(size=m); b /= b.sum()
+    r = cg.tests.test_T_computation_sparsify(alpha, beta, M, a, b, 0.05, 1e-3, K)
+    o = oracle.t_sparsify(alpha, beta, M, a, b, 0.05, 1e-3, K)
+    assert r["K_actual"] == o["K_actual"]
+    assert np.array_equal(r["csr_rowptr"], o["csr_rowptr"])
+    assert np.array_equal(r["csr_colind"], o["csr_colind"])
+    assert np.abs(r["csr_val"] - o["csr_val"]).max() <= 1e-12 * np.abs(o["csr_val"]).max()
+    assert abs(r["objfn"] - o["objfn"]) <= 1e-12 * max(1.0, abs(o["objfn"]))
+
+
+def test_sparsify_ties_prefer_smaller_flat_index(cuda_dev):
+    # identical T values everywhere: selection must take the smallest flat
+    # Hsl indices, i.e. the first columns j, rows i ascending
+    n, m, K = 6, 5, 7
+    M = np.ones((n, m))
+    a = np.full(n, 1.0 / n); b = np.full(m, 1.0 / m)
+    r = cg.tests.test_T_computation_sparsify(np.zeros(n), np.zeros(m), M, a, b, 0.1, 0.0, K)
+    o = oracle.t_sparsify(np.zeros(n), np.zeros(m), M, a, b, 0.1, 0.0, K)
+    assert np.array_equal(r["csr_colind"], o["csr_colind"])
+    assert np.array_equal(r["csr_rowptr"], o["csr_rowptr"])
+
+
+def problem(n, m, seed, kind="uniform"):
+    rng = np.random.default_rng(seed)
+    if kind == "uniform":
+        M = rng.uniform(size=(n, m))
+    else:  # config-1 style: squared distances of Gaussian clouds / max
+        X, Y = rng.normal(size=(n, 16)), rng.normal(size=(m, 16))
+        M = ((X[:, None, :] - Y[None, :, :]) ** 2).sum(-1)
+        M /= M.max()
+    a = rng.uniform(0.5, 1.5, size=n); a /= a.sum()
+    b = rng.uniform(0.5, 1.5, size=m); b /= b.sum()
+    return M, a, b
+
+
+@pytest.mark.parametrize("n,m,reg,kind", [(80, 60, 0.01, "uniform"), (60, 80, 0.01, "uniform"),
+                                          (120, 90, 0.05, "gauss"), (90, 150, 0.01, "gauss"),
+                                          (40, 33, 0.1, "uniform")])
+def test_splr_matches_oracle(cuda_dev, n, m, reg, kind):
+    M, a, b = problem(n, m, n + 7 * m, kind)
+    got = cg.numpy.sinkhorn_splr(M, a, b, reg, tol=1e-8, max_iter=300, return_trace=True)
+    ref = oracle.splr(M, a, b, reg, tol=1e-8, max_iter=300)
+    assert got["niter"] == ref["niter"]
+    # same K schedule, same candidate decisions, same line-search trial counts
+    np.testing.assert_array_equal(got["trace"][:, [3, 4, 5, 6, 7]], ref["trace"][:, [3, 4, 5, 6, 7]])
+    scale = np.abs(ref["dual"]).max()
+    assert np.abs(got["dual"] - ref["dual"]).max() <= 1e-10 * scale
+    assert np.abs(got["plan"] - ref["plan"]).max() <= 1e-12
+
+
+def test_splr_bwd_context_matches_oracle(cuda_dev):
+    n, m, reg = 70, 50, 0.02
+    M, a, b = problem(n, m, 11, "gauss")
+    Mt = torch.tensor(M, device=cuda_dev)
+    at, bt = torch.tensor(a, device=cuda_dev), torch.tensor(b, device=cuda_dev)
+    # tol 1e-8: below ~1e-9 the line search works at the FP64 resolution of f
+    # and equally valid implementations may take different paths
+    out = cg.torch.sinkhorn_splr_bwd(Mt, at, bt, reg, 1e-8, 500, 0, return_validation=True)
+    ref = oracle.splr(M, a, b, reg, tol=1e-8, max_iter=500)
+    ctx = out["context"]
+    rc = ref["context"]
+    assert out["niter"] == ref["niter"] and out["converged"] == ref["converged"]
+    assert ctx.dim == n + m - 1 and ctx.is_fallback == rc["fallback"]
+    assert ctx.low_rank_enabled == rc["low_rank"]
+    assert np.array_equal(ctx.csr_rowptr().cpu().numpy(), rc["csr_rowptr"])
+    assert np.array_equal(ctx.csr_colind().cpu().numpy(), rc["csr_colind"])
+    v = ctx.csr_values().cpu().numpy()
+    assert np.abs(v - rc["csr_values"]).max() <= 1e-10 * np.abs(rc["csr_values"]).max()
+    if rc["low_rank"]:
+        assert np.allclose(ctx.secant_s().cpu().numpy(), rc["s"], rtol=1e-6, atol=1e-14)
+    inv = oracle.inv_diag_from_csr(rc["csr_values"], rc["csr_colind"], rc["csr_rowptr"])
+    assert np.allclose(ctx.inv_diag().cpu().numpy(), inv, rtol=1e-10)
+    # B^{-1} applied to a random vector: check B z = r with the dense B
+    r = torch.randn(ctx.dim, dtype=torch.float64, device=cuda_dev)
+    z = ctx.apply_preconditioner(r).cpu().numpy()
+    H = n + m - 1
+    A = np.zeros((H, H))
+    val, col, rp = rc["csr_values"], rc["csr_colind"], rc["csr_rowptr"]
+    for row in range(H):
+        for q in range(rp[row], rp[row + 1]):
+            A[row, col[q]] = val[q]
+            A[col[q], row] = val[q]
+    Bz = A @ z
+    if rc["low_rank"]:
+        s, y, ys = rc["s"], rc["y"], rc["ys"]
+        As = A @ s
+        Bz = Bz + (reg / ys) * y * (y @ z) - As * (As @ z) / (s @ As)
+    assert np.linalg.norm(Bz - r.cpu().numpy()) <= 1e-8 * np.linalg.norm(r.cpu().numpy())
+
+
+def test_splr_immediate_convergence_fallback(cuda_dev):
+    n, m, reg = 30, 25, 0.05
+    M, a, b = problem(n, m, 5)
+    first = cg.numpy.sinkhorn_splr(M, a, b, reg, tol=1e-10, max_iter=500)
+    Mt = torch.tensor(M, device=cuda_dev)
+    out = cg.torch.sinkhorn_splr_bwd(Mt, torch.tensor(a, device=cuda_dev),
+                                     torch.tensor(b, device=cuda_dev), reg, 1e-6, 500, 0,
+                                     x0=torch.tensor(first["dual"]))
+    assert out["niter"] == 0 and out["converged"]
+    assert out["context"].is_fallback and not out["context"].low_rank_enabled
+
+
+def test_splr_vs_bcd_reference_tolerances(cuda_dev):
+    # reference test/test_sinkhorn_splr.py:45-120 at its two larger shapes
+    for (n, m, reg) in ((800, 600, 0.01), (600, 800, 0.001)):
+        M, a, b = problem(n, m, n * m % 97)
+        s = cg.numpy.sinkhorn_splr(M, a, b, reg, tol=1e-6, max_iter=5000)
+        c = cg.numpy.sinkhorn_bcd(M, a, b, reg, tol=1e-6, max_iter=100000)
+        rel = np.linalg.norm(s["plan"] - c["plan"]) / np.linalg.norm(c["plan"])
+        assert rel < 1e-3
+        assert np.linalg.norm(s["plan"].sum(1) - a) < 1e-4
+        assert np.linalg.norm(s["plan"].sum(0) - b) < 1e-4
+
+
+def test_splr_mixed_precision(cuda_dev):
+    n, m, reg = 300, 260, 0.02
+    M, a, b = problem(n, m, 9, "gauss")
+    M32 = M.astype(np.float32)
+    got = cg.numpy.sinkhorn_splr(M32, a, b, reg, tol=1e-8, max_iter=500, precision="mixed")
+    ref = oracle.splr(M32.astype(np.float64), a, b, reg, tol=1e-8, max_iter=500)
+    assert got["niter"] == ref["niter"]
+    assert np.abs(got["dual"] - ref["dual"]).max() <= 1e-10 * np.abs(ref["dual"]).max()
