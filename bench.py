@@ -1,0 +1,495 @@
+#!/usr/bin/env python
+"""Serving-stream benchmark: solves/s and p50/p99 latency of mixed-size
+entropic-OT requests at <= 1e-8 marginal error (FP64-checked), compared with
+the plain FP64 path.
+
+Workload (one "step" = one batch of requests of the serving stream):
+n, m log-uniform in [64, 8192], d in {8, 32}, costs = squared distances of
+Gaussian point clouds / max, eta in {0.1, 0.05, 0.01}, 70% Sinkhorn (BCD) /
+30% SPLR, tol 1e-8, uniform marginals, all requests of a step arriving at its
+start (saturation) unless --rate is given (Poisson arrivals).  Seeded
+synthetic data with the stream's shapes and distributions.
+
+Arms
+  ours (default)   the continuous-batching engine (FP32 cost matrix, FP64 duals,
+                   FP64-confirmed stop test); `value` with inputs resident in
+                   HBM, `e2e` with host inputs (H2D / D2H inside the timed
+                   region); plus the plain FP64 path one request at a time on
+                   the same requests.
+  --impl reference the reference algorithm on the host cores (the CPU
+                   restatement in oracle/, the reference ships no CPU solver),
+                   on a bounded sample of each step, scaled to solves/s.
+
+Multi-GPU: requests are independent, so ranks are replicas that each take
+their own share of the stream (no collective on the data path); timing is
+the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "solves/s + p99 latency, mixed-size OT stream @1e-8 marginal err, vs plain FP64"
+TOL = 1e-8
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--requests", type=int, default=48, help="requests per step per GPU")
+    p.add_argument("--rate", type=float, default=0.0, help="Poisson rate (req/s); 0 = saturation")
+    p.add_argument("--n-hi", type=int, default=8192)
+    p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU work")
+    p.add_argument("--budget-gb", type=float, default=120.0)
+    p.add_argument("--seed", type=int, default=4)
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_setup(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def step_specs(args, step, rank, warm):
+    from curegot_backward_b200.synthetic import stream_specs
+    count = max(4, args.requests // 4) if warm else args.requests
+    n_hi = min(args.n_hi, 2048) if warm else args.n_hi
+    seed = args.seed * 1000003 + (step + (1 << 16 if warm else 0)) * 131 + rank
+    return stream_specs(count, seed=seed, rate=args.rate or None, n_hi=n_hi)
+
+
+def make_step(specs, device):
+    import torch
+    from curegot_backward_b200.synthetic import stream_problem
+    probs = []
+    for s in specs:
+        M, a, b = stream_problem(s, device=device)
+        probs.append((s, M, a, b))
+    torch.cuda.synchronize()
+    return probs
+
+
+def to_host_pinned(probs):
+    out = []
+    for s, M, a, b in probs:
+        out.append((s, M.cpu().pin_memory(), a.cpu().pin_memory(), b.cpu().pin_memory()))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"cg_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx.append(float(f[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        except OSError:
+            return None
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# engine passes
+# ---------------------------------------------------------------------------
+def run_engine_step(eng, probs, host, rate):
+    """Submit a step's requests (arrival offsets honoured) and wait for all."""
+    import torch
+    t0 = eng.clock()
+    pending = {}
+    k = 0
+    results = []
+    while k < len(probs) or pending:
+        now = eng.clock() - t0
+        while k < len(probs) and (not rate or probs[k][0].arrival <= now):
+            s, M, a, b = probs[k]
+            rid = eng.submit(M, a, b, eta=s.eta, algo=s.algo, tol=TOL, tag=k)
+            pending[rid] = (s, t0 + (s.arrival if rate else 0.0))
+            k += 1
+        wait = 1 if (k < len(probs) and rate) else 50
+        for r in eng.poll(wait_ms=wait):
+            s, arr = pending.pop(r["id"])
+            r["latency"] = r["t_done"] - arr
+            r["spec"] = s
+            results.append(r)
+    return results
+
+
+def timed_engine_pass(eng, steps, host, rate, world):
+    import torch
+    step_ms, results = [], []
+    for probs in steps:
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = run_engine_step(eng, probs, host, rate)
+        e1.record()
+        torch.cuda.synchronize()
+        barrier(world)
+        step_ms.append(max_over_ranks(e0.elapsed_time(e1), world))
+        results.extend(res)
+    return step_ms, results
+
+
+def plain_fp64_pass(steps, world):
+    """The plain FP64 path, one request at a time, inputs resident in HBM."""
+    import torch
+    from curegot_backward_b200 import _solvers
+    step_ms = []
+    for probs in steps:
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for s, M64, a, b in probs:
+            if s.algo == "bcd":
+                _solvers._bcd_device(M64, a, b, s.eta, TOL, 100000, None, "fp64", want_plan=False)
+            else:
+                dmax = min(10.0 / min(s.n, s.m), 1.0)
+                _solvers._splr_device(M64, a, b, s.eta, TOL, 1000, 0, None, "fp64", dmax, 1e-3,
+                                      30, 3, want_plan=False)
+        e1.record()
+        torch.cuda.synchronize()
+        barrier(world)
+        step_ms.append(max_over_ranks(e0.elapsed_time(e1), world))
+    return step_ms
+
+
+def marginal_errors(probs, results):
+    """FP64-checked marginal errors of the engine's duals (on the FP32-valued M)."""
+    import torch
+    errs = []
+    by_tag = {r["tag"]: r for r in results}
+    for k, (s, M, a, b) in enumerate(probs):
+        r = by_tag[k]
+        dual = r["dual"].to(M.device)
+        al, be = dual[: s.n], dual[s.n:]
+        P = torch.exp((al[:, None] + be[None, :] - M.double()) / s.eta)
+        e_r = float(torch.linalg.norm(P.sum(1) - a))
+        e_c = float(torch.linalg.norm(P.sum(0) - b))
+        errs.append((s.algo, e_r, e_c, r["niter"], r["converged"]))
+        del P
+    return errs
+
+
+# ---------------------------------------------------------------------------
+# CPU restatement (reference algorithm on the host cores)
+# ---------------------------------------------------------------------------
+def cpu_sample(probs_host, budget_s, niters=None):
+    """Run the CPU oracle on a bounded sample of the requests (random order,
+    skipping requests predicted to exceed the remaining budget); returns
+    (solves/s scaled to the whole request set, cores, description)."""
+    import oracle
+    rng = np.random.default_rng(0)
+    order = rng.permutation(len(probs_host))
+    cores = oracle.num_threads()
+    work = []  # (elem-iterations, seconds)
+    # calibration: cost per element-iteration on the smallest request
+    small = min(range(len(probs_host)), key=lambda i: probs_host[i][0].n * probs_host[i][0].m)
+    t_used = 0.0
+    per_ei = None
+    done_idx = []
+    for i in [small] + [int(j) for j in order if j != small]:
+        s, M, a, b = probs_host[i]
+        est_iters = (niters[i] if niters is not None and niters[i] else 200)
+        if per_ei is not None:
+            pred = per_ei * s.n * s.m * est_iters * (3.0 if s.algo == "splr" else 1.0)
+            if t_used + pred > budget_s:
+                continue
+        Mn, an, bn = M.double().numpy(), a.numpy(), b.numpy()
+        t = time.perf_counter()
+        if s.algo == "bcd":
+            r = oracle.bcd(Mn, an, bn, s.eta, tol=TOL, max_iter=100000, want_plan=False)
+        else:
+            r = oracle.splr(Mn, an, bn, s.eta, tol=TOL, max_iter=1000, want_plan=False)
+        dt = time.perf_counter() - t
+        t_used += dt
+        ei = s.n * s.m * max(r["niter"], 1)
+        work.append((ei, dt, i))
+        done_idx.append(i)
+        per_ei = sum(w for _, w, _ in work) / max(sum(e for e, _, _ in work), 1)
+        if t_used > budget_s:
+            break
+    # scale: CPU element-iterations per second -> solves/s on this request set
+    rate_ei = sum(e for e, _, _ in work) / max(sum(w for _, w, _ in work), 1e-9)
+    if niters is not None:
+        total_ei = sum(p[0].n * p[0].m * max(niters[i], 1) for i, p in enumerate(probs_host))
+        solves_per_s = len(probs_host) * rate_ei / total_ei
+    else:
+        solves_per_s = len(work) / max(sum(w for _, w, _ in work), 1e-9)
+    desc = (f"{len(work)} of {len(probs_host)} stream requests solved by the CPU restatement "
+            f"in {sum(w for _, w, _ in work):.1f} s on {cores} threads; element-iterations/s "
+            f"scaled to the full request set with its GPU-measured iteration counts")
+    return solves_per_s, cores, desc
+
+
+def reference_arm(args, world, rank):
+    """--impl reference: the reference algorithm on the host cores."""
+    if rank != 0:
+        return
+    import oracle
+    import torch
+    oracle.set_num_threads(os.cpu_count() or 1)
+    step_rates = []
+    for st in range(args.warmup + args.steps):
+        warm = st < args.warmup
+        specs = step_specs(args, st if not warm else st, 0, warm)
+        if warm:
+            continue
+        from curegot_backward_b200.synthetic import stream_problem
+        probs = []
+        for s in specs:
+            M, a, b = stream_problem(s, device="cpu")
+            probs.append((s, M, a, b))
+        sps, cores, desc = cpu_sample(probs, args.cpu_budget / max(args.steps, 1))
+        step_rates.append(sps)
+    value = float(np.mean(step_rates)) if step_rates else 0.0
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * args.requests / value if value else None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": "serving stream: n,m log-uniform [64,8192], d in {8,32}, "
+                                   "Gaussian clouds/max, eta in {0.1,0.05,0.01}, 70% BCD / 30% "
+                                   "SPLR, tol 1e-8", "requests_per_step": args.requests},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": oracle.num_threads(),
+                             "kind": "port", "sample": desc},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def measured_hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def main():
+    args = parse()
+    import torch
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        reference_arm(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    from curegot_backward_b200 import _native
+    from curegot_backward_b200.serving import OTEngine
+    dev = torch.device("cuda", local if world > 1 else 0)
+    _native.lib().cg_launch_count_reset()
+    eng = OTEngine(budget_bytes=args.budget_gb * 1e9, max_batch=64, splr_workers=3, chunk=8)
+
+    # warm-up steps (untimed)
+    for st in range(args.warmup):
+        probs = make_step(step_specs(args, st, rank, True), dev)
+        run_engine_step(eng, probs, False, 0.0)
+    # timed steps: data generated up front (each step streams far more than L2)
+    steps = [make_step(step_specs(args, st, rank, False), dev) for st in range(args.steps)]
+    n_req = sum(len(p) for p in steps)
+    sampler = ClockSampler(torch.cuda.current_device())
+    s0 = eng.stats()
+    l0 = _native.lib().cg_launch_count()
+    sampler.start()
+    step_ms, results = timed_engine_pass(eng, steps, False, args.rate, world)
+    clocks = sampler.stop()
+    launches = _native.lib().cg_launch_count() - l0
+    s1 = eng.stats()
+    total_ms = sum(step_ms)
+    total_req = sum_over_ranks(n_req, world)
+    value = total_req / (total_ms / 1000.0)
+    lat = np.array([r["latency"] for r in results]) * 1000.0
+    ok = all(r["status"] == 0 for r in results)
+
+    # roofline of the dominant kernels (Sinkhorn row/column passes)
+    bytes_ = s1["bcd_bytes"] - s0["bcd_bytes"]
+    gms = s1["bcd_gpu_ms"] - s0["bcd_gpu_ms"]
+    peak, peak_kind = measured_hbm_peak()
+    achieved = bytes_ / (gms / 1000.0) / 1e9 if gms > 0 else 0.0
+    launches_per_chunk = 2 * 8
+    n_chunks = s1["chunks"] - s0["chunks"]
+
+    # e2e: host inputs, copies inside the timed region
+    e2e = None
+    if not args.no_e2e:
+        hsteps = [to_host_pinned(p) for p in steps]
+        h2d = sum(p[1].numel() * 4 + (p[0].n + p[0].m) * 8 for st in hsteps for p in st)
+        d2h = sum((p[0].n + p[0].m) * 8 for st in hsteps for p in st)
+        e_ms, _ = timed_engine_pass(eng, hsteps, True, args.rate, world)
+        e2e = {"value": total_req / (sum(e_ms) / 1000.0), "unit": "solves/s",
+               "h2d_bytes_per_step": int(h2d / max(args.steps, 1)),
+               "d2h_bytes_per_step": int(d2h / max(args.steps, 1))}
+        del hsteps
+
+    # accuracy (FP64-checked, untimed)
+    errs = []
+    for k, probs in enumerate(steps):
+        sub = [r for r in results if any(r["spec"] is p[0] for p in probs)]
+        errs.extend(marginal_errors(probs, sub))
+    max_row = max(e[1] for e in errs)
+    max_col = max(e[2] for e in errs if e[0] == "bcd") if any(e[0] == "bcd" for e in errs) else 0
+    frac_ok = float(np.mean([e[1] <= TOL for e in errs]))
+
+    # plain FP64 path on the same requests
+    plain = None
+    if not args.no_plain:
+        p64 = [[(s, M.double(), a, b) for (s, M, a, b) in probs] for probs in steps]
+        p_ms = plain_fp64_pass(p64, world)
+        pv = total_req / (sum(p_ms) / 1000.0)
+        plain = {"value": pv, "unit": "solves/s", "ms_per_step": float(np.mean(p_ms)),
+                 "engine_over_plain": value / pv}
+        del p64
+
+    cpu = None
+    if rank == 0:
+        import oracle
+        oracle.set_num_threads(os.cpu_count() or 1)
+        host = [(p[0], p[1].cpu(), p[2].cpu(), p[3].cpu()) for p in steps[0]]
+        tags0 = {r["tag"]: r for r in results if any(r["spec"] is p[0] for p in steps[0])}
+        niters = [tags0[k]["niter"] if k in tags0 else None for k in range(len(host))]
+        sps, cores, desc = cpu_sample(host, args.cpu_budget, niters)
+        cpu = {"value": sps, "unit": "solves/s", "cores": cores, "kind": "port", "sample": desc}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(step_ms)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32-M/f64", "data": "synthetic",
+            "config": {"workload": "serving stream: n,m log-uniform [64,8192], d in {8,32}, "
+                                   "Gaussian clouds/max, eta in {0.1,0.05,0.01}, 70% BCD / 30% "
+                                   "SPLR, tol 1e-8, uniform marginals",
+                       "requests_per_step": args.requests,
+                       "arrivals": f"poisson {args.rate}/s" if args.rate else "saturation",
+                       "l2": "inputs larger than L2 (each step streams > 126 MB of M)",
+                       "engine": "max_batch 64, 3 SPLR workers, 8 ticks per graph launch",
+                       "parallelism": f"replicas x{world}"},
+            "latency_ms": {"p50": float(np.percentile(lat, 50)),
+                           "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
+            "accuracy": {"max_row_marginal_err": max_row, "max_col_marginal_err_bcd": max_col,
+                         "frac_le_1e-8": frac_ok, "all_status_ok": ok},
+            "plain_fp64": plain,
+            "e2e": e2e,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak if peak else None, "traffic": None,
+                         "peak_kind": peak_kind,
+                         "kernel": "bcd_row_kernel<float> + bcd_col_kernel<float> (batched)",
+                         "note": f"{bytes_/1e9:.2f} GB algorithmic over {n_chunks} chunks of "
+                                 f"{launches_per_chunk} launches ({gms:.1f} ms device time)"},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": int(launches),
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

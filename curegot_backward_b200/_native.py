@@ -56,6 +56,34 @@ class CtxInfo(ctypes.Structure):
                 ("adopted", ctypes.c_int)]
 
 
+class Request(ctypes.Structure):
+    """cg_request_t."""
+    _fields_ = [("algo", ctypes.c_int), ("n", ctypes.c_int), ("m", ctypes.c_int),
+                ("m_f32", ctypes.c_int), ("host_inputs", ctypes.c_int),
+                ("max_iter", ctypes.c_int), ("eta", ctypes.c_double), ("tol", ctypes.c_double),
+                ("M", ctypes.c_void_p), ("a", ctypes.c_void_p), ("b", ctypes.c_void_p),
+                ("dual_out", ctypes.c_void_p), ("tag", ctypes.c_uint64)]
+
+
+class Result(ctypes.Structure):
+    """cg_result_t."""
+    _fields_ = [("id", ctypes.c_uint64), ("tag", ctypes.c_uint64), ("status", ctypes.c_int),
+                ("niter", ctypes.c_int), ("converged", ctypes.c_int),
+                ("fast_iters", ctypes.c_int), ("last_err", ctypes.c_double),
+                ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double),
+                ("t_done", ctypes.c_double)]
+
+
+class EngineStats(ctypes.Structure):
+    """cg_engine_stats_t."""
+    _fields_ = [("in_use_bytes", ctypes.c_size_t), ("budget_bytes", ctypes.c_size_t),
+                ("queued", ctypes.c_longlong), ("active_bcd", ctypes.c_longlong),
+                ("active_splr", ctypes.c_longlong), ("completed", ctypes.c_longlong),
+                ("bcd_bytes", ctypes.c_double), ("bcd_gpu_ms", ctypes.c_double),
+                ("chunks", ctypes.c_longlong), ("graph_builds", ctypes.c_longlong)]
+
+
+CG_ALGO_BCD, CG_ALGO_SPLR = 0, 1
 CG_PRECOND_NONE, CG_PRECOND_DIAG, CG_PRECOND_SPLR = 0, 1, 2
 (CG_CTX_CSR_VALUES, CG_CTX_CSR_COLIND, CG_CTX_CSR_ROWPTR, CG_CTX_SECANT_S, CG_CTX_SECANT_Y,
  CG_CTX_INV_DIAG, CG_CTX_POINT, CG_CTX_INVA_Y) = range(8)
@@ -67,6 +95,8 @@ _SPLR_ARGS = [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_double,
 SIGNATURES = {
     "cg_last_error": [],
     "cg_version": [],
+    "cg_launch_count": [],
+    "cg_launch_count_reset": [],
     "cg_bcd_f64": [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_double, c_int,
                    c_int, c_int_p, c_void_p, c_void_p, c_void_p],
     "cg_bcd_mixed": [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_double, c_int,
@@ -92,8 +122,16 @@ SIGNATURES = {
                                c_void_p, c_void_p, c_void_p, c_void_p, c_ll_p, c_void_p],
     "cg_test_spd_solve_f64": [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p,
                               c_void_p],
+    "cg_engine_create": [c_size_t, c_int, c_int, c_int, c_void_pp],
+    "cg_engine_submit": [c_void_p, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)],
+    "cg_engine_poll": [c_void_p, ctypes.POINTER(Result), c_int, c_int, c_int_p],
+    "cg_engine_stats": [c_void_p, ctypes.POINTER(EngineStats)],
+    "cg_engine_clock": [],
+    "cg_engine_destroy": [c_void_p],
 }
-RESTYPES = {"cg_last_error": ctypes.c_char_p, "cg_version": ctypes.c_char_p}
+RESTYPES = {"cg_last_error": ctypes.c_char_p, "cg_version": ctypes.c_char_p,
+            "cg_engine_clock": ctypes.c_double, "cg_launch_count": ctypes.c_longlong,
+            "cg_launch_count_reset": None}
 
 
 class CuregotError(RuntimeError):

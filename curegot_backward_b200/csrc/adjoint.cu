@@ -443,16 +443,16 @@ int backward_solve(const double* T, const double* G, cg_ctx_s* ctx, double eta, 
   A.scal = ws.at<double>(o_sc);
   A.counters = ws.at<unsigned int>(o_cnt);
   CG_TRY_CUDA(cudaMemsetAsync(A.counters, 0, (splits + strips + 1) * sizeof(unsigned int), st));
-  pcg_state_init<<<1, 1, 0, st>>>(A.st, max_iter, precond, tol);
+  { pcg_state_init<<<1, 1, 0, st>>>(A.st, max_iter, precond, tol); cg::count_launch(); }
   const int grid = strips * splits;
   const bool splr = (precond == CG_PRECOND_SPLR);
   if (splr) {
     // RHS pass without preconditioner; then z = B^{-1} r, p = z, rz = r.z
     AdjArgs A0 = A;
     A0.inv_diag = nullptr;
-    adj_pass_kernel<0><<<grid, kThreads, 0, st>>>(A0, 0);
+    { adj_pass_kernel<0><<<grid, kThreads, 0, st>>>(A0, 0); cg::count_launch(); }
   } else {
-    adj_pass_kernel<0><<<grid, kThreads, 0, st>>>(A, 0);
+    { adj_pass_kernel<0><<<grid, kThreads, 0, st>>>(A, 0); cg::count_launch(); }
   }
   CG_TRY_CUDA(cudaGetLastError());
   PcgState hs{};
@@ -461,17 +461,17 @@ int backward_solve(const double* T, const double* G, cg_ctx_s* ctx, double eta, 
   if (!hs.allzero && splr) {
     // z = B^{-1} r, p = z, rz = r.z
     CG_TRY(ctx_apply_full(ctx, A.r, A.z, st));
-    pcg_splr_init_kernel<<<1, 1024, 0, st>>>(A.r, A.z, A.p, H, A.st);
+    { pcg_splr_init_kernel<<<1, 1024, 0, st>>>(A.r, A.z, A.p, H, A.st); cg::count_launch(); }
     CG_TRY_CUDA(cudaGetLastError());
   }
   if (!hs.allzero) {
     int chunk = 4;
     while (!hs.done) {
       for (int c = 0; c < chunk; ++c) {
-        adj_pass_kernel<1><<<grid, kThreads, 0, st>>>(A, splr ? 0 : 1);
+        { adj_pass_kernel<1><<<grid, kThreads, 0, st>>>(A, splr ? 0 : 1); cg::count_launch(); }
         if (splr) {
           CG_TRY(ctx_apply_full(ctx, A.r, A.z, st));
-          pcg_update2_kernel<<<1, 1024, 0, st>>>(A.r, A.z, A.p, H, A.st);
+          { pcg_update2_kernel<<<1, 1024, 0, st>>>(A.r, A.z, A.p, H, A.st); cg::count_launch(); }
         }
       }
       CG_TRY_CUDA(cudaGetLastError());
@@ -485,7 +485,7 @@ int backward_solve(const double* T, const double* G, cg_ctx_s* ctx, double eta, 
   if (grad) {
     const size_t total = (size_t)n * m;
     const int blocks = (int)std::max<size_t>(1, std::min<size_t>((total + 255) / 256, sms * 16));
-    assemble_grad_kernel<<<blocks, 256, 0, st>>>(T, G, lambda, n, m, 1.0 / eta, grad);
+    { assemble_grad_kernel<<<blocks, 256, 0, st>>>(T, G, lambda, n, m, 1.0 / eta, grad); cg::count_launch(); }
     CG_TRY_CUDA(cudaGetLastError());
   }
   ws.release();

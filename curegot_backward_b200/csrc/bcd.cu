@@ -624,23 +624,23 @@ __global__ void plan_kernel(const TM* __restrict__ M, const double* __restrict__
 void launch_bcd_row(bool f32, const BcdProb* d_probs, const int* d_cta_prob,
                     const int* d_cta_start, int total_ctas, cudaStream_t stream) {
   if (f32)
-    bcd_row_kernel<float><<<total_ctas, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start);
+    { bcd_row_kernel<float><<<total_ctas, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start); cg::count_launch(); }
   else
-    bcd_row_kernel<double><<<total_ctas, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start);
+    { bcd_row_kernel<double><<<total_ctas, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start); cg::count_launch(); }
 }
 void launch_bcd_col(bool f32, const BcdProb* d_probs, const int* d_cta_prob,
                     const int* d_cta_start, int total_ctas, cudaStream_t stream) {
   if (f32)
-    bcd_col_kernel<float><<<total_ctas, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start);
+    { bcd_col_kernel<float><<<total_ctas, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start); cg::count_launch(); }
   else
-    bcd_col_kernel<double><<<total_ctas, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start);
+    { bcd_col_kernel<double><<<total_ctas, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start); cg::count_launch(); }
 }
 template <typename TM>
 void launch_plan(const TM* M, const double* alpha, const double* beta, double* P,
                  double inv_eta, int n, int m, cudaStream_t stream) {
   const size_t total = (size_t)n * m;
   const int blocks = (int)std::min<size_t>((total + kThreads - 1) / kThreads, 148 * 16);
-  plan_kernel<TM><<<std::max(blocks, 1), kThreads, 0, stream>>>(M, alpha, beta, P, inv_eta, n, m);
+  { plan_kernel<TM><<<std::max(blocks, 1), kThreads, 0, stream>>>(M, alpha, beta, P, inv_eta, n, m); cg::count_launch(); }
 }
 template void launch_plan<double>(const double*, const double*, const double*, double*, double,
                                   int, int, cudaStream_t);

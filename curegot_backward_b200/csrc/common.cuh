@@ -41,6 +41,9 @@ void set_last_error(const char* msg, const char* file, int line);
 // Number of SMs of the current device.
 int sm_count_current();
 
+// Kernel launches issued by this library (graph replays count their kernels).
+void count_launch(long long k = 1);
+
 // Warp reductions: the result is valid in lane 0 (shfl_down tree, a fixed
 // association order, so results are bitwise reproducible).
 __device__ __forceinline__ double warp_sum_down(double v) {

@@ -102,7 +102,7 @@ int ctx_apply_full(cg_ctx_s* c, const double* r, double* z, cudaStream_t st) {
   CG_TRY(solver_handle(&h));
   CG_TRY(schur_solve(h, c->A, c->F, r, c->xtmp, 1, c->tmp, st));
   if (c->low_rank)
-    ctx_woodbury_kernel<<<1, 1024, 0, st>>>(c->xtmp, c->u, r, c->y, c->s, c->H, c->reg, c->ys);
+    { ctx_woodbury_kernel<<<1, 1024, 0, st>>>(c->xtmp, c->u, r, c->y, c->s, c->H, c->reg, c->ys); cg::count_launch(); }
   CG_TRY_CUDA(cudaMemcpyAsync(z, c->xtmp, c->H * sizeof(double), cudaMemcpyDeviceToDevice, st));
   CG_TRY_CUDA(cudaGetLastError());
   return CG_OK;
@@ -112,8 +112,8 @@ int ctx_setup_diag(cg_ctx_s* c, cudaStream_t st) {
   if (c->diag_ready) return CG_OK;
   const int init = INT_MAX;
   CG_TRY_CUDA(cudaMemcpyAsync(c->err, &init, sizeof(int), cudaMemcpyHostToDevice, st));
-  inv_diag_ctx_kernel<<<std::max(1, std::min((c->H + 255) / 256, 1024)), 256, 0, st>>>(
-      c->A.val, c->A.rowptr, c->n, c->H, c->inv_diag, c->err);
+  { inv_diag_ctx_kernel<<<std::max(1, std::min((c->H + 255) / 256, 1024)), 256, 0, st>>>(
+      c->A.val, c->A.rowptr, c->n, c->H, c->inv_diag, c->err); cg::count_launch(); }
   int bad = INT_MAX;
   CG_TRY_CUDA(cudaMemcpyAsync(&bad, c->err, sizeof(int), cudaMemcpyDeviceToHost, st));
   CG_TRY_CUDA(cudaStreamSynchronize(st));
@@ -202,8 +202,8 @@ int cg_ctx_apply(cg_ctx* ctx, const double* r, double* z, int mode, cudaStream_t
       cg::set_last_error("diagonal preconditioner not set up", __FILE__, __LINE__);
       return CG_ERR_INVALID_CONTEXT;
     }
-    cg::scale_kernel<<<std::max(1, std::min((c->H + 255) / 256, 1024)), 256, 0, stream>>>(
-        c->inv_diag, r, z, c->H);
+    { cg::scale_kernel<<<std::max(1, std::min((c->H + 255) / 256, 1024)), 256, 0, stream>>>(
+        c->inv_diag, r, z, c->H); cg::count_launch(); }
     CG_TRY_CUDA(cudaGetLastError());
     return CG_OK;
   }
@@ -254,8 +254,8 @@ int cg_t_values_f64(const double* alpha, const double* beta, const double* M, in
   if (m == 1) return CG_OK;
   const long long Te = (long long)n * (m - 1);
   const int blocks = (int)std::max<long long>(1, std::min<long long>((Te + 255) / 256, 148 * 16));
-  cg::t_values_kernel<<<blocks, 256, 0, stream>>>(alpha, beta, M, n, m, 1.0 / reg, Tvalues,
-                                                  Tflatind);
+  { cg::t_values_kernel<<<blocks, 256, 0, stream>>>(alpha, beta, M, n, m, 1.0 / reg, Tvalues,
+                                                  Tflatind); cg::count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
   return CG_OK;
 }
@@ -354,7 +354,7 @@ int cg_test_spd_solve_f64(const double* values, const int* colind, const int* ro
   CG_TRY(ws.allocate());
   double* S = ws.at<double>(o_S);
   CG_TRY_CUDA(cudaMemsetAsync(S, 0, (size_t)n * n * sizeof(double), stream));
-  densify_lower_kernel<<<std::min(n, 4096), 256, 0, stream>>>(values, colind, rowptr, n, S);
+  { densify_lower_kernel<<<std::min(n, 4096), 256, 0, stream>>>(values, colind, rowptr, n, S); cg::count_launch(); }
   CG_TRY_CUDA(cudaMemcpyAsync(x, rhs, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
   if (cusolverDnSetStream(h, stream) != CUSOLVER_STATUS_SUCCESS) return CG_ERR_SOLVER;
   int* info = ws.at<int>(o_info);

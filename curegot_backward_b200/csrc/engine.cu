@@ -1,0 +1,651 @@
+// Continuous-batching OT serving engine.
+//
+// No reference counterpart: the reference solves one problem per blocking
+// call and batches only by a Python loop (curegot/autograd.py:340-367).
+//
+//   * Sinkhorn (BCD) requests are packed into shared launches: every admitted
+//     problem contributes its CTAs to one row pass and one column pass per
+//     tick (bcd.cu kernels map CTAs to problems through cta_prob/cta_start).
+//     A chunk of ticks is captured once per batch composition as a CUDA graph
+//     and replayed; finished problems exit their CTAs immediately and are
+//     retired at the next chunk boundary, when queued requests are admitted
+//     into the freed slots.  Duals and solver state stay on the device.
+//   * SPLR requests run on worker threads, each with its own stream, so their
+//     device work overlaps the Sinkhorn batch.
+//   * Admission is by HBM footprint: a request enters only while the sum of
+//     the footprints of admitted requests stays within the budget.
+//   * Each request records submit / admit / finish times (host steady clock)
+//     and its iteration count; results are polled by the caller.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "bcd.cuh"
+#include "splr.cuh"
+
+namespace cg {
+namespace {
+
+double now_s() {
+  using namespace std::chrono;
+  return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+struct Req {
+  cg_request_t r;
+  uint64_t id = 0;
+  double t_submit = 0, t_admit = 0, t_done = 0;
+  size_t footprint = 0;
+  int status = CG_OK;
+  int niter = 0;
+  int converged = 0;
+  int fast_iters = 0;
+  double last_err = 0;
+  // device state
+  void* block = nullptr;
+  const void* dM = nullptr;
+  const double* da = nullptr;
+  const double* db = nullptr;
+  double* ddual = nullptr;
+  BcdProb prob{};
+  int slot = -1;
+};
+
+size_t bcd_footprint(const cg_request_t& r, BcdProb& geo, int sms) {
+  const int n = r.n, m = r.m;
+  const size_t es = r.m_f32 ? 4 : 8;
+  bcd_geometry(n, m, (int)es, sms, geo);
+  size_t b = 0;
+  if (r.host_inputs) b += align256((size_t)n * m * es) + align256(8 * (size_t)(n + m));
+  b += align256(8 * (size_t)(n + m));          // dual out (device)
+  b += 2 * align256(8 * (size_t)n) + 2 * align256(8 * (size_t)m);  // loga logb (+ spare)
+  b += 4 * align256(8 * (size_t)n) + 4 * align256(8 * (size_t)m);  // alpha/beta (scaled) x2
+  const size_t parts = geo.col_splits > 1 ? (size_t)geo.col_splits * m : 1;
+  b += 2 * align256(8 * parts);
+  b += align256(8 * (size_t)geo.row_ctas * 4) + align256(8 * (size_t)geo.col_strips * 3);
+  b += align256(4 * (size_t)(2 + geo.col_strips)) + align256(sizeof(BcdState));
+  return b;
+}
+
+size_t splr_footprint(const cg_request_t& r) {
+  const size_t n = r.n, m = r.m, H = n + m - 1;
+  const double dmax = std::min(10.0 / std::min(n, m), 1.0);
+  const size_t kmax = std::max<size_t>((size_t)(dmax * n * (m - 1)), 1);
+  const size_t k = std::min(n, m - 1);
+  size_t b = (size_t)n * m * (r.m_f32 ? 4 : 8) * (r.host_inputs ? 1 : 0);
+  b += kmax * 24 + k * k * 8 + 40 * H * 8 + (size_t)n * m / 64 * 8 + (64u << 20);
+  return b;
+}
+
+__global__ void engine_init_kernel(const double* a, const double* b, int n, int m, double s2,
+                                   double* loga, double* logb, double* al0, double* be0,
+                                   double* als0, double* bes0, unsigned int* counters, int nc,
+                                   BcdState* st, int max_iter, double tol, int fast) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  for (int i = tid; i < n; i += stride) {
+    loga[i] = log(a[i]);
+    al0[i] = 0.0;
+    als0[i] = 0.0;
+  }
+  for (int j = tid; j < m; j += stride) {
+    logb[j] = log(b[j]);
+    be0[j] = 0.0;
+    bes0[j] = 0.0;
+  }
+  for (int q = tid; q < nc; q += stride) counters[q] = 0u;
+  if (tid == 0) {
+    st->iter = 0;
+    st->phase = 1;
+    st->check_pending = 0;
+    st->done = (max_iter <= 0);
+    st->niter = 0;
+    st->max_iter = max_iter;
+    st->fast = fast;
+    st->stall = 0;
+    st->tol = tol;
+    st->last_err = 0.0;
+    st->best_est = INFINITY;
+    st->stat_a[0] = st->stat_a[1] = st->stat_a[2] = 0.0;
+    st->fast_iters = 0;
+  }
+}
+
+__global__ void gather_states_kernel(const BcdProb* probs, int P, BcdState* out) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < P; k += gridDim.x * blockDim.x)
+    out[k] = *probs[k].st;
+}
+
+__global__ void engine_dual_kernel(const BcdProb* p, double* dual) {
+  const int k = p->st->niter & 1;
+  const int n = p->n, m = p->m;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += gridDim.x * blockDim.x)
+    dual[i] = (i < n) ? p->alpha[k][i] : p->beta[k][i - n];
+}
+
+}  // namespace
+}  // namespace cg
+
+struct cg_engine_s {
+  int device = 0;
+  size_t budget = 0;
+  size_t in_use = 0;
+  int max_batch = 64;
+  int chunk = 8;
+  int sms = 148;
+  std::mutex mu;
+  std::condition_variable cv;
+  bool stop = false;
+  uint64_t next_id = 1;
+  std::deque<cg::Req*> bcd_q, splr_q;
+  std::vector<cg::Req*> done;
+  std::vector<std::thread> threads;
+  std::atomic<long long> active_bcd{0}, active_splr{0};
+  // statistics
+  std::atomic<long long> n_done{0};
+  double bytes_bcd = 0.0;     // algorithmic bytes streamed by Sinkhorn passes
+  double gpu_ms_bcd = 0.0;    // device time of the Sinkhorn chunks
+  long long chunks = 0, graph_builds = 0;
+};
+
+namespace cg {
+namespace {
+
+bool try_reserve(cg_engine_s* E, size_t bytes) {
+  if (E->in_use + bytes > E->budget) return false;
+  E->in_use += bytes;
+  return true;
+}
+
+void release(cg_engine_s* E, size_t bytes) {
+  std::lock_guard<std::mutex> lk(E->mu);
+  E->in_use -= std::min(bytes, E->in_use);
+}
+
+void finish(cg_engine_s* E, Req* q) {
+  q->t_done = now_s();
+  std::lock_guard<std::mutex> lk(E->mu);
+  E->done.push_back(q);
+  E->n_done++;
+  E->cv.notify_all();
+}
+
+// Allocate and initialise a Sinkhorn problem (engine stream).
+int bcd_admit(cg_engine_s* E, Req* q, cudaStream_t st) {
+  const cg_request_t& r = q->r;
+  const int n = r.n, m = r.m;
+  const size_t es = r.m_f32 ? 4 : 8;
+  BcdProb& P = q->prob;
+  CG_TRY_CUDA(cudaMallocAsync(&q->block, q->footprint, st));
+  char* p = static_cast<char*>(q->block);
+  auto take = [&](size_t bytes) {
+    char* x = p;
+    p += align256(bytes);
+    return x;
+  };
+  if (r.host_inputs) {
+    void* dM = take((size_t)n * m * es);
+    double* dab = reinterpret_cast<double*>(take(8 * (size_t)(n + m)));
+    CG_TRY_CUDA(cudaMemcpyAsync(dM, r.M, (size_t)n * m * es, cudaMemcpyHostToDevice, st));
+    CG_TRY_CUDA(cudaMemcpyAsync(dab, r.a, 8 * (size_t)n, cudaMemcpyHostToDevice, st));
+    CG_TRY_CUDA(cudaMemcpyAsync(dab + n, r.b, 8 * (size_t)m, cudaMemcpyHostToDevice, st));
+    q->dM = dM;
+    q->da = dab;
+    q->db = dab + n;
+  } else {
+    q->dM = r.M;
+    q->da = r.a;
+    q->db = r.b;
+  }
+  q->ddual = reinterpret_cast<double*>(take(8 * (size_t)(n + m)));
+  double* loga = reinterpret_cast<double*>(take(8 * (size_t)n));
+  take(8 * (size_t)n);
+  double* logb = reinterpret_cast<double*>(take(8 * (size_t)m));
+  take(8 * (size_t)m);
+  for (int k = 0; k < 2; ++k) {
+    P.alpha[k] = reinterpret_cast<double*>(take(8 * (size_t)n));
+    P.alphas[k] = reinterpret_cast<double*>(take(8 * (size_t)n));
+    P.beta[k] = reinterpret_cast<double*>(take(8 * (size_t)m));
+    P.betas[k] = reinterpret_cast<double*>(take(8 * (size_t)m));
+  }
+  const size_t parts = P.col_splits > 1 ? (size_t)P.col_splits * m : 1;
+  P.col_m = reinterpret_cast<double*>(take(8 * parts));
+  P.col_s = reinterpret_cast<double*>(take(8 * parts));
+  P.row_part = reinterpret_cast<double*>(take(8 * (size_t)P.row_ctas * 4));
+  P.col_part = reinterpret_cast<double*>(take(8 * (size_t)P.col_strips * 3));
+  P.counters = reinterpret_cast<unsigned int*>(take(4 * (size_t)(2 + P.col_strips)));
+  P.st = reinterpret_cast<BcdState*>(take(sizeof(BcdState)));
+  P.M = q->dM;
+  P.n = n;
+  P.m = m;
+  P.eta = r.eta;
+  P.s2 = kLog2e / r.eta;
+  P.a = q->da;
+  P.loga = loga;
+  P.logb = logb;
+  { engine_init_kernel<<<std::max(1, std::min((std::max(n, m) + 255) / 256, 64)), 256, 0, st>>>(
+      q->da, q->db, n, m, P.s2, loga, logb, P.alpha[0], P.beta[0], P.alphas[0], P.betas[0],
+      P.counters, 2 + P.col_strips, P.st, r.max_iter, r.tol, r.m_f32 ? 1 : 0); cg::count_launch(); }
+  CG_TRY_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
+// The Sinkhorn batch scheduler.
+void bcd_loop(cg_engine_s* E) {
+  cudaSetDevice(E->device);
+  cudaStream_t st;
+  cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  cudaEvent_t ev0, ev1;
+  cudaEventCreate(&ev0);
+  cudaEventCreate(&ev1);
+  std::vector<Req*> active;  // one precision class per batch (f32 or f64 kernels)
+  bool batch_f32 = true;
+  // device-side batch description
+  BcdProb* d_probs = nullptr;
+  int* d_map = nullptr;
+  size_t cap_probs = 0, cap_map = 0;
+  std::vector<BcdProb> h_probs;
+  std::vector<int> h_map;
+  BcdState* h_states = nullptr;  // pinned
+  BcdState* d_states = nullptr;
+  size_t cap_states = 0;
+  cudaGraphExec_t gexec = nullptr;
+  bool dirty = true;
+  int row_total = 0, col_total = 0;
+  double batch_bytes_per_tick = 0.0;
+
+  while (true) {
+    // ---- admission --------------------------------------------------------
+    {
+      std::unique_lock<std::mutex> lk(E->mu);
+      if (active.empty())
+        E->cv.wait(lk, [&] { return E->stop || !E->bcd_q.empty(); });
+      if (E->stop && active.empty()) break;
+      while (!E->stop && !E->bcd_q.empty() && (int)active.size() < E->max_batch) {
+        Req* q = E->bcd_q.front();
+        if (!active.empty() && (q->r.m_f32 != 0) != batch_f32) break;
+        if (!try_reserve(E, q->footprint)) {
+          if (!active.empty() || E->in_use > 0) break;
+          // larger than the whole budget: reject
+          E->bcd_q.pop_front();
+          q->status = CG_ERR_ADMISSION;
+          lk.unlock();
+          finish(E, q);
+          lk.lock();
+          continue;
+        }
+        E->bcd_q.pop_front();
+        lk.unlock();
+        q->t_admit = now_s();
+        if (active.empty()) batch_f32 = q->r.m_f32 != 0;
+        int rc = bcd_admit(E, q, st);
+        lk.lock();
+        if (rc != CG_OK) {
+          q->status = rc;
+          E->in_use -= q->footprint;
+          lk.unlock();
+          finish(E, q);
+          lk.lock();
+          continue;
+        }
+        active.push_back(q);
+        E->active_bcd = (long long)active.size();
+        dirty = true;
+      }
+    }
+    if (active.empty()) {
+      if (E->stop) break;
+      continue;
+    }
+    // ---- (re)build the batch description and its chunk graph ---------------
+    if (dirty) {
+      h_probs.clear();
+      h_map.clear();
+      row_total = col_total = 0;
+      batch_bytes_per_tick = 0.0;
+      for (size_t k = 0; k < active.size(); ++k) {
+        Req* q = active[k];
+        q->slot = (int)k;
+        h_probs.push_back(q->prob);
+        row_total += q->prob.row_ctas;
+        col_total += q->prob.col_strips * q->prob.col_splits;
+        batch_bytes_per_tick += 2.0 * q->r.n * (double)q->r.m * (q->r.m_f32 ? 4 : 8);
+      }
+      // map layout: [row cta->prob][row start][col cta->prob][col start]
+      const int P = (int)active.size();
+      h_map.resize((size_t)row_total + P + col_total + P);
+      int* rp = h_map.data();
+      int* rs = rp + row_total;
+      int* cp = rs + P;
+      int* cs = cp + col_total;
+      int ro = 0, co = 0;
+      for (int k = 0; k < P; ++k) {
+        rs[k] = ro;
+        for (int c = 0; c < active[k]->prob.row_ctas; ++c) rp[ro++] = k;
+        cs[k] = co;
+        const int nc = active[k]->prob.col_strips * active[k]->prob.col_splits;
+        for (int c = 0; c < nc; ++c) cp[co++] = k;
+      }
+      if ((size_t)P > cap_probs) {
+        if (d_probs) cudaFreeAsync(d_probs, st);
+        cap_probs = std::max<size_t>(P, 2 * cap_probs);
+        cudaMallocAsync(&d_probs, cap_probs * sizeof(BcdProb), st);
+      }
+      if (h_map.size() > cap_map) {
+        if (d_map) cudaFreeAsync(d_map, st);
+        cap_map = std::max<size_t>(h_map.size(), 2 * cap_map);
+        cudaMallocAsync(&d_map, cap_map * sizeof(int), st);
+      }
+      cudaMemcpyAsync(d_probs, h_probs.data(), P * sizeof(BcdProb), cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(d_map, h_map.data(), h_map.size() * sizeof(int), cudaMemcpyHostToDevice,
+                      st);
+      cudaStreamSynchronize(st);  // host vectors are reused below
+      if (gexec) cudaGraphExecDestroy(gexec);
+      gexec = nullptr;
+      cudaGraph_t g;
+      if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        const int* drp = d_map;
+        const int* drs = drp + row_total;
+        const int* dcp = drs + P;
+        const int* dcs = dcp + col_total;
+        for (int c = 0; c < E->chunk; ++c) {
+          launch_bcd_row(batch_f32, d_probs, drp, drs, row_total, st);
+          launch_bcd_col(batch_f32, d_probs, dcp, dcs, col_total, st);
+        }
+        count_launch(-2LL * E->chunk);  // captured, not executed
+        if (cudaStreamEndCapture(st, &g) == cudaSuccess) {
+          if (cudaGraphInstantiate(&gexec, g, 0) != cudaSuccess) gexec = nullptr;
+          cudaGraphDestroy(g);
+        }
+      }
+      E->graph_builds++;
+      if ((size_t)P > cap_states) {
+        if (h_states) cudaFreeHost(h_states);
+        if (d_states) cudaFreeAsync(d_states, st);
+        cap_states = std::max<size_t>(P, 2 * cap_states);
+        cudaHostAlloc(reinterpret_cast<void**>(&h_states), cap_states * sizeof(BcdState),
+                      cudaHostAllocDefault);
+        cudaMallocAsync(&d_states, cap_states * sizeof(BcdState), st);
+      }
+      dirty = false;
+    }
+    // ---- run one chunk ------------------------------------------------------
+    const int P = (int)active.size();
+    cudaEventRecord(ev0, st);
+    if (gexec) {
+      cudaGraphLaunch(gexec, st);
+      count_launch(2LL * E->chunk);
+    } else {
+      const int* drp = d_map;
+      const int* drs = drp + row_total;
+      const int* dcp = drs + P;
+      const int* dcs = dcp + col_total;
+      for (int c = 0; c < E->chunk; ++c) {
+        launch_bcd_row(batch_f32, d_probs, drp, drs, row_total, st);
+        launch_bcd_col(batch_f32, d_probs, dcp, dcs, col_total, st);
+      }
+    }
+    cudaEventRecord(ev1, st);
+    // states of all problems: one gather kernel, one copy
+    { gather_states_kernel<<<std::max(1, (P + 127) / 128), 128, 0, st>>>(d_probs, P, d_states); cg::count_launch(); }
+    cudaMemcpyAsync(h_states, d_states, P * sizeof(BcdState), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    E->gpu_ms_bcd += ms;
+    E->chunks++;
+    // algorithmic bytes: problems still running at the chunk start stream
+    // 2 n m elements per tick until they finish
+    for (int k = 0; k < P; ++k) {
+      const Req* q = active[k];
+      const int ran = std::min(E->chunk, std::max(0, h_states[k].iter - q->niter));
+      E->bytes_bcd += ran * 2.0 * q->r.n * (double)q->r.m * (q->r.m_f32 ? 4 : 8);
+      active[k]->niter = h_states[k].iter;
+    }
+    // ---- retire finished problems -----------------------------------------
+    std::vector<Req*> keep;
+    for (int k = 0; k < P; ++k) {
+      Req* q = active[k];
+      const BcdState& s = h_states[k];
+      if (!s.done) {
+        keep.push_back(q);
+        continue;
+      }
+      q->niter = s.niter;
+      q->converged = (s.niter < s.max_iter) || (s.phase == 2 && s.last_err < s.tol && !s.fast);
+      q->fast_iters = s.fast_iters;
+      q->last_err = s.last_err;
+      // duals -> output (device or host)
+      BcdProb* dp = d_probs + k;
+      { engine_dual_kernel<<<std::max(1, std::min((q->r.n + q->r.m + 255) / 256, 64)), 256, 0, st>>>(
+          dp, q->ddual); cg::count_launch(); }
+      if (q->r.dual_out) {
+        cudaMemcpyAsync(q->r.dual_out, q->ddual, 8 * (size_t)(q->r.n + q->r.m),
+                        q->r.host_inputs ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, st);
+      }
+      dirty = true;
+    }
+    if (dirty) {
+      cudaStreamSynchronize(st);
+      for (int k = 0; k < P; ++k) {
+        Req* q = active[k];
+        if (!h_states[k].done) continue;
+        cudaFreeAsync(q->block, st);
+        q->block = nullptr;
+        release(E, q->footprint);
+        finish(E, q);
+      }
+      active.swap(keep);
+      E->active_bcd = (long long)active.size();
+    }
+  }
+  if (gexec) cudaGraphExecDestroy(gexec);
+  if (d_states) cudaFreeAsync(d_states, st);
+  if (h_states) cudaFreeHost(h_states);
+  if (d_probs) cudaFreeAsync(d_probs, st);
+  if (d_map) cudaFreeAsync(d_map, st);
+  cudaStreamSynchronize(st);
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  cudaStreamDestroy(st);
+}
+
+void splr_loop(cg_engine_s* E) {
+  cudaSetDevice(E->device);
+  cudaStream_t st;
+  cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  while (true) {
+    Req* q = nullptr;
+    {
+      std::unique_lock<std::mutex> lk(E->mu);
+      E->cv.wait(lk, [&] {
+        if (E->stop) return true;
+        if (E->splr_q.empty()) return false;
+        Req* f = E->splr_q.front();
+        return f->footprint > E->budget || E->in_use + f->footprint <= E->budget;
+      });
+      if (E->stop) break;
+      if (E->splr_q.empty()) continue;
+      q = E->splr_q.front();
+      E->splr_q.pop_front();
+      if (q->footprint > E->budget) {
+        q->status = CG_ERR_ADMISSION;
+        lk.unlock();
+        finish(E, q);
+        continue;
+      }
+      E->in_use += q->footprint;
+      E->active_splr++;
+    }
+    q->t_admit = now_s();
+    const cg_request_t& r = q->r;
+    const int n = r.n, m = r.m;
+    const size_t es = r.m_f32 ? 4 : 8;
+    int rc = CG_OK;
+    void* blk = nullptr;
+    const void* dM = r.M;
+    const double *da = r.a, *db = r.b;
+    double* ddual = nullptr;
+    const size_t inb = r.host_inputs ? align256((size_t)n * m * es) + align256(8 * (size_t)(n + m)) : 0;
+    if (cudaMallocAsync(&blk, inb + align256(8 * (size_t)(n + m)), st) != cudaSuccess) {
+      rc = CG_ERR_OOM;
+    } else {
+      char* p = static_cast<char*>(blk);
+      if (r.host_inputs) {
+        cudaMemcpyAsync(p, r.M, (size_t)n * m * es, cudaMemcpyHostToDevice, st);
+        dM = p;
+        double* dab = reinterpret_cast<double*>(p + align256((size_t)n * m * es));
+        cudaMemcpyAsync(dab, r.a, 8 * (size_t)n, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(dab + n, r.b, 8 * (size_t)m, cudaMemcpyHostToDevice, st);
+        da = dab;
+        db = dab + n;
+      }
+      ddual = reinterpret_cast<double*>(p + inb);
+      SplrParams prm{r.eta, r.tol, r.max_iter, std::min(10.0 / std::min(n, m), 1.0), 1e-3, 30, 3,
+                     0};
+      int niter = 0, conv = 0;
+      if (r.m_f32)
+        rc = splr_solve<float>(static_cast<const float*>(dM), da, db, nullptr, n, m, prm, nullptr,
+                               ddual, &niter, &conv, nullptr, nullptr, st);
+      else
+        rc = splr_solve<double>(static_cast<const double*>(dM), da, db, nullptr, n, m, prm,
+                                nullptr, ddual, &niter, &conv, nullptr, nullptr, st);
+      q->niter = niter;
+      q->converged = conv;
+      if (rc == CG_OK && r.dual_out)
+        cudaMemcpyAsync(r.dual_out, ddual, 8 * (size_t)(n + m),
+                        r.host_inputs ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, st);
+      cudaFreeAsync(blk, st);
+      cudaStreamSynchronize(st);
+    }
+    q->status = rc;
+    {
+      std::lock_guard<std::mutex> lk(E->mu);
+      E->in_use -= std::min(q->footprint, E->in_use);
+      E->active_splr--;
+    }
+    E->cv.notify_all();
+    finish(E, q);
+  }
+  cudaStreamDestroy(st);
+}
+
+}  // namespace
+}  // namespace cg
+
+extern "C" {
+
+int cg_engine_create(size_t budget_bytes, int max_batch, int splr_workers, int chunk,
+                     cg_engine** out) {
+  if (!out || budget_bytes == 0 || max_batch <= 0 || splr_workers < 0) return CG_ERR_INVALID_ARG;
+  auto* E = new cg_engine_s();
+  cudaGetDevice(&E->device);
+  E->budget = budget_bytes;
+  E->max_batch = max_batch;
+  E->chunk = chunk > 0 ? chunk : 8;
+  E->sms = cg::sm_count_current();
+  E->threads.emplace_back(cg::bcd_loop, E);
+  for (int w = 0; w < splr_workers; ++w) E->threads.emplace_back(cg::splr_loop, E);
+  *out = reinterpret_cast<cg_engine*>(E);
+  return CG_OK;
+}
+
+int cg_engine_submit(cg_engine* eng, const cg_request_t* req, uint64_t* id) {
+  if (!eng || !req || req->n <= 0 || req->m <= 0 || !req->M || !req->a || !req->b ||
+      !(req->eta > 0.0) || (req->algo != CG_ALGO_BCD && req->algo != CG_ALGO_SPLR))
+    return CG_ERR_INVALID_ARG;
+  cg_engine_s* E = reinterpret_cast<cg_engine_s*>(eng);
+  auto* q = new cg::Req();
+  q->r = *req;
+  q->t_submit = cg::now_s();
+  if (req->algo == CG_ALGO_BCD) {
+    q->footprint = cg::bcd_footprint(q->r, q->prob, E->sms);
+  } else {
+    if (req->m < 2) {
+      delete q;
+      return CG_ERR_INVALID_ARG;
+    }
+    q->footprint = cg::splr_footprint(q->r);
+  }
+  {
+    std::lock_guard<std::mutex> lk(E->mu);
+    q->id = E->next_id++;
+    if (req->algo == CG_ALGO_BCD) E->bcd_q.push_back(q);
+    else E->splr_q.push_back(q);
+  }
+  E->cv.notify_all();
+  if (id) *id = q->id;
+  return CG_OK;
+}
+
+int cg_engine_poll(cg_engine* eng, cg_result_t* results, int capacity, int wait_ms, int* count) {
+  if (!eng || !count || (capacity > 0 && !results)) return CG_ERR_INVALID_ARG;
+  cg_engine_s* E = reinterpret_cast<cg_engine_s*>(eng);
+  std::unique_lock<std::mutex> lk(E->mu);
+  if (E->done.empty() && wait_ms > 0)
+    E->cv.wait_for(lk, std::chrono::milliseconds(wait_ms), [&] { return !E->done.empty(); });
+  const int k = std::min<int>(capacity, (int)E->done.size());
+  for (int i = 0; i < k; ++i) {
+    cg::Req* q = E->done[i];
+    cg_result_t& o = results[i];
+    o.id = q->id;
+    o.tag = q->r.tag;
+    o.status = q->status;
+    o.niter = q->niter;
+    o.converged = q->converged;
+    o.fast_iters = q->fast_iters;
+    o.last_err = q->last_err;
+    o.t_submit = q->t_submit;
+    o.t_admit = q->t_admit;
+    o.t_done = q->t_done;
+    delete q;
+  }
+  E->done.erase(E->done.begin(), E->done.begin() + k);
+  *count = k;
+  return CG_OK;
+}
+
+int cg_engine_stats(cg_engine* eng, cg_engine_stats_t* out) {
+  if (!eng || !out) return CG_ERR_INVALID_ARG;
+  cg_engine_s* E = reinterpret_cast<cg_engine_s*>(eng);
+  std::lock_guard<std::mutex> lk(E->mu);
+  out->in_use_bytes = E->in_use;
+  out->budget_bytes = E->budget;
+  out->queued = (long long)(E->bcd_q.size() + E->splr_q.size());
+  out->active_bcd = E->active_bcd;
+  out->active_splr = E->active_splr;
+  out->completed = E->n_done;
+  out->bcd_bytes = E->bytes_bcd;
+  out->bcd_gpu_ms = E->gpu_ms_bcd;
+  out->chunks = E->chunks;
+  out->graph_builds = E->graph_builds;
+  return CG_OK;
+}
+
+double cg_engine_clock(void) { return cg::now_s(); }
+
+int cg_engine_destroy(cg_engine* eng) {
+  if (!eng) return CG_OK;
+  cg_engine_s* E = reinterpret_cast<cg_engine_s*>(eng);
+  {
+    std::lock_guard<std::mutex> lk(E->mu);
+    E->stop = true;
+  }
+  E->cv.notify_all();
+  for (auto& t : E->threads) t.join();
+  for (auto* q : E->done) delete q;
+  for (auto* q : E->bcd_q) delete q;
+  for (auto* q : E->splr_q) delete q;
+  delete E;
+  return CG_OK;
+}
+
+}  // extern "C"

@@ -172,11 +172,11 @@ __global__ void back_kernel(int mode, const double* __restrict__ val, const int*
 int schur_factor(cusolverDnHandle_t h, const SpHess& A, SchurFactor& F, cudaStream_t st) {
   if (F.k <= 0) return CG_OK;
   if (F.big_alpha)
-    assemble_big_alpha<<<F.k, 256, 0, st>>>(A.val, A.col, A.rowptr, A.ipt, A.ij, A.iv, A.n, F.k,
-                                            F.S);
+    { assemble_big_alpha<<<F.k, 256, 0, st>>>(A.val, A.col, A.rowptr, A.ipt, A.ij, A.iv, A.n, F.k,
+                                            F.S); cg::count_launch(); }
   else
-    assemble_big_beta<<<F.k, 256, 0, st>>>(A.val, A.col, A.rowptr, A.ipt, A.ij, A.iv, A.n, F.k,
-                                           F.S);
+    { assemble_big_beta<<<F.k, 256, 0, st>>>(A.val, A.col, A.rowptr, A.ipt, A.ij, A.iv, A.n, F.k,
+                                           F.S); cg::count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
   if (cusolverDnSetStream(h, st) != CUSOLVER_STATUS_SUCCESS) return CG_ERR_SOLVER;
   if (cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, F.k, F.S, F.k, F.work, F.lwork, F.info) !=
@@ -192,8 +192,8 @@ int schur_solve(cusolverDnHandle_t h, const SpHess& A, const SchurFactor& F, con
   const int mode = F.big_alpha ? 0 : 1;
   const int k = F.k;
   if (k > 0) {
-    reduce_rhs_kernel<<<std::max(1, std::min((k + 7) / 8, 148 * 8)), 256, 0, st>>>(
-        mode, A.val, A.col, A.rowptr, A.ipt, A.ij, A.iv, A.n, A.H, k, rhs, nrhs, tmp);
+    { reduce_rhs_kernel<<<std::max(1, std::min((k + 7) / 8, 148 * 8)), 256, 0, st>>>(
+        mode, A.val, A.col, A.rowptr, A.ipt, A.ij, A.iv, A.n, A.H, k, rhs, nrhs, tmp); cg::count_launch(); }
     CG_TRY_CUDA(cudaGetLastError());
     if (cusolverDnSetStream(h, st) != CUSOLVER_STATUS_SUCCESS) return CG_ERR_SOLVER;
     if (cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, k, nrhs, F.S, k, tmp, k, F.info) !=
@@ -204,8 +204,8 @@ int schur_solve(cusolverDnHandle_t h, const SpHess& A, const SchurFactor& F, con
   }
   const int big = F.big_alpha ? A.n : (A.m - 1);
   const int work = std::max(big, k * nrhs);
-  back_kernel<<<std::max(1, std::min((work + 7) / 8, 148 * 8)), 256, 0, st>>>(
-      mode, A.val, A.col, A.rowptr, A.ipt, A.ij, A.iv, A.n, A.m, A.H, k, rhs, tmp, nrhs, x);
+  { back_kernel<<<std::max(1, std::min((work + 7) / 8, 148 * 8)), 256, 0, st>>>(
+      mode, A.val, A.col, A.rowptr, A.ipt, A.ij, A.iv, A.n, A.m, A.H, k, rhs, tmp, nrhs, x); cg::count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
   return CG_OK;
 }

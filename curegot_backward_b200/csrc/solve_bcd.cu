@@ -6,6 +6,7 @@
 // and reads the 48-byte state once per chunk; passes after convergence exit
 // immediately.  No host synchronisation happens inside an iteration.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <string>
 
@@ -17,6 +18,12 @@ namespace cg {
 namespace {
 thread_local std::string g_last_error;
 }
+
+namespace {
+std::atomic<long long> g_launches{0};
+}
+
+void count_launch(long long k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 
 void set_last_error(const char* msg, const char* file, int line) {
   g_last_error = std::string(msg) + " (" + file + ":" + std::to_string(line) + ")";
@@ -142,10 +149,10 @@ int bcd_solve(const TM* M, const double* a, const double* b, double* Pout, doubl
   BcdProb* dprob = ws.at<BcdProb>(o_prob);
 
   const bool f32 = sizeof(TM) == 4;
-  bcd_init_kernel<<<64, 256, 0, stream>>>(a, b, x0, n, m, hp.s2, const_cast<double*>(hp.loga),
+  { bcd_init_kernel<<<64, 256, 0, stream>>>(a, b, x0, n, m, hp.s2, const_cast<double*>(hp.loga),
                                           const_cast<double*>(hp.logb), hp.alpha[0], hp.beta[0],
                                           hp.alphas[0], hp.betas[0], hp.counters, ncount, hp.st,
-                                          max_iter, tol, f32 ? 1 : 0);
+                                          max_iter, tol, f32 ? 1 : 0); cg::count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
   CG_TRY_CUDA(cudaMemcpyAsync(dprob, &hp, sizeof(BcdProb), cudaMemcpyHostToDevice, stream));
 
@@ -170,9 +177,9 @@ int bcd_solve(const TM* M, const double* a, const double* b, double* Pout, doubl
   if (Pout) {
     const size_t total = (size_t)n * m;
     const int blocks = (int)std::max<size_t>(1, std::min<size_t>((total + 255) / 256, sms * 16));
-    plan_from_state_kernel<TM><<<blocks, 256, 0, stream>>>(M, hp.st, dprob, Pout);
+    { plan_from_state_kernel<TM><<<blocks, 256, 0, stream>>>(M, hp.st, dprob, Pout); cg::count_launch(); }
   }
-  if (dual) dual_from_state_kernel<<<std::max(1, (n + m + 255) / 256), 256, 0, stream>>>(hp.st, dprob, dual);
+  { if (dual) dual_from_state_kernel<<<std::max(1, (n + m + 255) / 256), 256, 0, stream>>>(hp.st, dprob, dual); cg::count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
   ws.release();
   return CG_OK;
@@ -193,6 +200,10 @@ extern "C" {
 const char* cg_last_error(void) { return cg::g_last_error.c_str(); }
 
 const char* cg_version(void) { return "curegot_b200 0.1.0 (sm_100a)"; }
+
+long long cg_launch_count(void) { return cg::g_launches.load(); }
+
+void cg_launch_count_reset(void) { cg::g_launches.store(0); }
 
 int cg_bcd_f64(const double* M, const double* a, const double* b, double* P, double reg,
                int max_iter, double tol, int n, int m, int* niter, const double* x0,
@@ -225,7 +236,7 @@ int cg_transport_plan_mixed(const float* M, const double* alpha, const double* b
 int cg_diag_exp2(const double* x, double* y, int n, int mode, cudaStream_t stream) {
   if (!x || !y || n < 0 || mode < 0 || mode > 1) return CG_ERR_INVALID_ARG;
   if (n == 0) return CG_OK;
-  cg::diag_exp2_kernel<<<(n + 255) / 256, 256, 0, stream>>>(x, y, n, mode);
+  { cg::diag_exp2_kernel<<<(n + 255) / 256, 256, 0, stream>>>(x, y, n, mode); cg::count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
   return CG_OK;
 }

@@ -482,27 +482,27 @@ static int select_and_build_t(const TM* M, const double* gamma, const double* ro
   int* scr_c = w.scr_c;
   int* scr_r = w.scr_r;
 
-  sel_init_kernel<<<1, 256, 0, st>>>(w.sel, w.hist, Ks, Te);
+  { sel_init_kernel<<<1, 256, 0, st>>>(w.sel, w.hist, Ks, Te); cg::count_launch(); }
   if (Te > 0) {
     const int hgrid = grid_for(n, kWarps, sms * 8);
     for (int level = 0; level < 9; ++level) {
-      hist_kernel<TM><<<hgrid, kThreads, 0, st>>>(M, gamma, n, m, s2, w.sel, w.hist);
-      select_kernel<<<1, 1024, 0, st>>>(w.sel, w.hist);
+      { hist_kernel<TM><<<hgrid, kThreads, 0, st>>>(M, gamma, n, m, s2, w.sel, w.hist); cg::count_launch(); }
+      { select_kernel<<<1, 1024, 0, st>>>(w.sel, w.hist); cg::count_launch(); }
     }
-    count_kernel<TM><<<rowtiles * coltiles, kThreads, 0, st>>>(M, gamma, n, m, s2, w.sel,
-                                                               w.colcnt, w.rowcnt, coltiles);
-    prefix_cols_kernel<<<grid_for(m - 1, 256, sms * 4), 256, 0, st>>>(w.colcnt, w.coltot, m - 1,
-                                                                       rowtiles);
+    { count_kernel<TM><<<rowtiles * coltiles, kThreads, 0, st>>>(M, gamma, n, m, s2, w.sel,
+                                                               w.colcnt, w.rowcnt, coltiles); cg::count_launch(); }
+    { prefix_cols_kernel<<<grid_for(m - 1, 256, sms * 4), 256, 0, st>>>(w.colcnt, w.coltot, m - 1,
+                                                                       rowtiles); cg::count_launch(); }
   }
-  prefix_rows_kernel<<<grid_for(n, 256, sms * 4), 256, 0, st>>>(w.rowcnt, w.rowtot, n,
-                                                                 Te > 0 ? coltiles : 0);
-  scan_kernel<<<1, 1024, 0, st>>>(w.coltot, w.rowtot, n, m, scr_c, scr_r, h.rowptr, h.ipt, w.kout);
+  { prefix_rows_kernel<<<grid_for(n, 256, sms * 4), 256, 0, st>>>(w.rowcnt, w.rowtot, n,
+                                                                 Te > 0 ? coltiles : 0); cg::count_launch(); }
+  { scan_kernel<<<1, 1024, 0, st>>>(w.coltot, w.rowtot, n, m, scr_c, scr_r, h.rowptr, h.ipt, w.kout); cg::count_launch(); }
   if (Te > 0)
-    emit_kernel<TM><<<rowtiles * coltiles, kThreads, 0, st>>>(
+    { emit_kernel<TM><<<rowtiles * coltiles, kThreads, 0, st>>>(
         M, gamma, n, m, s2, w.sel, w.colcnt, w.rowcnt, coltiles, h.rowptr, h.ipt, h.val, h.col,
-        h.ij, h.iv);
-  diag_kernel<<<grid_for(h.H, 256, sms * 4), 256, 0, st>>>(rows, cols, n, m, shift, h.rowptr,
-                                                            h.val, h.col);
+        h.ij, h.iv); cg::count_launch(); }
+  { diag_kernel<<<grid_for(h.H, 256, sms * 4), 256, 0, st>>>(rows, cols, n, m, shift, h.rowptr,
+                                                            h.val, h.col); cg::count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
   return CG_OK;
 }
@@ -525,19 +525,19 @@ int sparsify_refresh(bool f32, const void* M, const double* gamma, const double*
   if (m > 1) {
     const int gj = grid_for(m - 1, kWarps, sms * 8), gi = grid_for(n, kWarps, sms * 8);
     if (f32) {
-      refresh_byj_kernel<float><<<gj, kThreads, 0, st>>>(static_cast<const float*>(M), gamma, n, m,
-                                                         s2, h.rowptr, h.col, h.val);
-      refresh_byi_kernel<float><<<gi, kThreads, 0, st>>>(static_cast<const float*>(M), gamma, n, m,
-                                                         s2, h.ipt, h.ij, h.iv);
+      { refresh_byj_kernel<float><<<gj, kThreads, 0, st>>>(static_cast<const float*>(M), gamma, n, m,
+                                                         s2, h.rowptr, h.col, h.val); cg::count_launch(); }
+      { refresh_byi_kernel<float><<<gi, kThreads, 0, st>>>(static_cast<const float*>(M), gamma, n, m,
+                                                         s2, h.ipt, h.ij, h.iv); cg::count_launch(); }
     } else {
-      refresh_byj_kernel<double><<<gj, kThreads, 0, st>>>(static_cast<const double*>(M), gamma, n,
-                                                          m, s2, h.rowptr, h.col, h.val);
-      refresh_byi_kernel<double><<<gi, kThreads, 0, st>>>(static_cast<const double*>(M), gamma, n,
-                                                          m, s2, h.ipt, h.ij, h.iv);
+      { refresh_byj_kernel<double><<<gj, kThreads, 0, st>>>(static_cast<const double*>(M), gamma, n,
+                                                          m, s2, h.rowptr, h.col, h.val); cg::count_launch(); }
+      { refresh_byi_kernel<double><<<gi, kThreads, 0, st>>>(static_cast<const double*>(M), gamma, n,
+                                                          m, s2, h.ipt, h.ij, h.iv); cg::count_launch(); }
     }
   }
-  diag_kernel<<<grid_for(h.H, 256, sms * 4), 256, 0, st>>>(rows, cols, n, m, shift, h.rowptr,
-                                                            h.val, h.col);
+  { diag_kernel<<<grid_for(h.H, 256, sms * 4), 256, 0, st>>>(rows, cols, n, m, shift, h.rowptr,
+                                                            h.val, h.col); cg::count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
   return CG_OK;
 }

@@ -373,18 +373,28 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
   int lwork = 0;
   CG_TRY(schur_lwork(sol, k, lwork));
 
-  // context-capable block (plain cudaMalloc: it may outlive the stream)
+  // context-capable block: plain cudaMalloc when a context will own it (it
+  // may outlive the stream), stream-ordered otherwise (no device-wide sync)
   const size_t hbytes = hblock_bytes(n, m, Kmax, k, lwork);
   void* hbase = nullptr;
-  CG_TRY_CUDA(cudaMalloc(&hbase, hbytes));
+  const bool owned_by_ctx = (ctx_out != nullptr);
+  if (owned_by_ctx) {
+    CG_TRY_CUDA(cudaMalloc(&hbase, hbytes));
+  } else {
+    CG_TRY_CUDA(cudaMallocAsync(&hbase, hbytes, st));
+  }
   HBlock hb;
   hblock_carve(hbase, n, m, Kmax, k, big_alpha, lwork, hb);
   struct Guard {
     void*& p;
+    bool sync_free;
+    cudaStream_t s;
     ~Guard() {
-      if (p) cudaFree(p);
+      if (!p) return;
+      if (sync_free) cudaFree(p);
+      else cudaFreeAsync(p, s);
     }
-  } hguard{hbase};
+  } hguard{hbase, owned_by_ctx, st};
 
   // per-solve workspace
   int tstrips = 1, tsplits = 1;
@@ -463,7 +473,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
 
   CG_TRY_CUDA(cudaMemcpyAsync(ab, a, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
   CG_TRY_CUDA(cudaMemcpyAsync(ab + n, b, m * sizeof(double), cudaMemcpyDeviceToDevice, st));
-  log_kernel<<<grid_for(n + m, 256, 1024), 256, 0, st>>>(ab, logab, n + m);
+  { log_kernel<<<grid_for(n + m, 256, 1024), 256, 0, st>>>(ab, logab, n + m); cg::count_launch(); }
   CG_TRY_CUDA(cudaMemcpyAsync(dcp, &cp, sizeof(BcdProb), cudaMemcpyHostToDevice, st));
   CG_TRY_CUDA(cudaMemsetAsync(tcnt, 0, (tsplits + tstrips + 1) * sizeof(unsigned int), st));
   CG_TRY_CUDA(cudaMemsetAsync(gamma_prev, 0, (n + m) * sizeof(double), st));
@@ -516,8 +526,8 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
   const int bgrid = grid_for(m, 256, 1024);
   // alpha_bcd = A(beta) then `sweeps` x (beta, alpha): BCD passes, phase 0.
   auto bcd_sweeps = [&](const double* beta_src, bool zero_beta, int sweeps) {
-    bcd_seed_kernel<<<bgrid, 256, 0, st>>>(beta_src, zero_beta ? 1 : 0, cp.beta[0], cp.betas[0],
-                                           m, s2, cp.st, cp.counters, bcount);
+    { bcd_seed_kernel<<<bgrid, 256, 0, st>>>(beta_src, zero_beta ? 1 : 0, cp.beta[0], cp.betas[0],
+                                           m, s2, cp.st, cp.counters, bcount); cg::count_launch(); }
     launch_bcd_row(f32, dcp, nullptr, nullptr, cp.row_ctas, st);
     for (int q = 0; q < sweeps; ++q) {
       launch_bcd_col(f32, dcp, nullptr, nullptr, cp.col_strips * cp.col_splits, st);
@@ -528,7 +538,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
   // init_dual (sinkhorn_splr.cu:330-359)
   if (x0) {
     CG_TRY_CUDA(cudaMemcpyAsync(gamma, x0, (n + m) * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    shift_inplace_kernel<<<1, 1024, 0, st>>>(gamma, n, m);
+    { shift_inplace_kernel<<<1, 1024, 0, st>>>(gamma, n, m); cg::count_launch(); }
   } else {
     bcd_sweeps(nullptr, true, 0);
     // alpha in buffer 1, beta = 0
@@ -569,8 +579,8 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     }
     if (!std::isfinite(objfn)) break;
 
-    lowrank_kernel<<<1, 1024, 0, st>>>(grad, grad_prev, gamma, gamma_prev, hb.rhs2 + H, hb.s, H,
-                                       iter, hb.dres);
+    { lowrank_kernel<<<1, 1024, 0, st>>>(grad, grad_prev, gamma, gamma_prev, hb.rhs2 + H, hb.s, H,
+                                       iter, hb.dres); cg::count_launch(); }
     const bool analyze = (iter % prm.cycle == 0);
     const bool update = (iter % prm.cycle == (prm.cycle - 1));
 
@@ -579,8 +589,8 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     const bool use_cand = analyze && (cand != 0);
     if (use_cand) {
       bcd_sweeps(gamma + n, false, cand);
-      shift_assemble_kernel<<<grid_for(n + m, 256, 1024), 256, 0, st>>>(
-          gamma_bcd, cp.alpha[(cand + 1) & 1], cp.beta[cand & 1], n, m);
+      { shift_assemble_kernel<<<grid_for(n + m, 256, 1024), 256, 0, st>>>(
+          gamma_bcd, cp.alpha[(cand + 1) & 1], cp.beta[cand & 1], n, m); cg::count_launch(); }
       CG_TRY(eval_at(gamma_bcd, grad_c, rows_c, cols_c, res_c, trc, nullptr));
     }
 
@@ -589,8 +599,8 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     CG_TRY(schur_factor(sol, hb.A, hb.F, st));
     const int nrhs = (iter > 0) ? 2 : 1;
     CG_TRY(schur_solve(sol, hb.A, hb.F, hb.rhs2, hb.sol2, nrhs, hb.tmp, st));
-    woodbury_kernel<<<1, 1024, 0, st>>>(hb.sol2, hb.sol2 + H, grad, hb.rhs2 + H, hb.s, H, reg, 1,
-                                        hb.dres);
+    { woodbury_kernel<<<1, 1024, 0, st>>>(hb.sol2, hb.sol2 + H, grad, hb.rhs2 + H, hb.s, H, reg, 1,
+                                        hb.dres); cg::count_launch(); }
     CG_TRY_CUDA(cudaGetLastError());
     DirRes dr{};
     int info = 0;

@@ -220,9 +220,9 @@ size_t tpass_workspace_doubles(int n, int m, int strips, int splits) {
 int launch_tpass(bool f32, const TPassArgs& a, cudaStream_t stream) {
   const int grid = a.strips * a.splits;
   if (f32)
-    tpass_kernel<float><<<grid, kThreads, 0, stream>>>(a);
+    { tpass_kernel<float><<<grid, kThreads, 0, stream>>>(a); cg::count_launch(); }
   else
-    tpass_kernel<double><<<grid, kThreads, 0, stream>>>(a);
+    { tpass_kernel<double><<<grid, kThreads, 0, stream>>>(a); cg::count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
   return CG_OK;
 }

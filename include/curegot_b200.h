@@ -42,6 +42,10 @@ enum {
 const char* cg_last_error(void);
 /* Library version string. */
 const char* cg_version(void);
+/* Kernel launches issued by the library since load / last reset (graph
+ * replays count the kernels they run). */
+long long cg_launch_count(void);
+void cg_launch_count_reset(void);
 
 /* ------------------------------------------------------------------------ */
 /* Sinkhorn block-coordinate descent (log-domain Sinkhorn).                  */
@@ -157,6 +161,63 @@ int cg_ctx_destroy(cg_ctx* ctx);
 int cg_backward_f64(const double* T, const double* G, cg_ctx* ctx, double eta, int precond,
                     double tol, int max_iter, int n, int m, double* lambda, double* grad,
                     int* iterations, int* converged, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Continuous-batching serving engine (no reference counterpart: the         */
+/* reference solves one problem per blocking call and batches only with a    */
+/* Python loop, curegot/autograd.py:340-367).                                */
+/* ------------------------------------------------------------------------ */
+
+typedef struct cg_engine_s cg_engine;
+
+enum { CG_ALGO_BCD = 0, CG_ALGO_SPLR = 1 };
+
+typedef struct {
+  int algo;            /* CG_ALGO_BCD | CG_ALGO_SPLR                                  */
+  int n, m;
+  int m_f32;           /* 1: M is float (mixed precision), 0: double                 */
+  int host_inputs;     /* 1: M, a, b, dual_out are host pointers (copied by the engine) */
+  int max_iter;
+  double eta, tol;
+  const void* M;       /* row-major n x m                                             */
+  const double* a;     /* [n] */
+  const double* b;     /* [m] */
+  double* dual_out;    /* [n + m] (nullable)                                          */
+  uint64_t tag;        /* caller's tag, returned with the result                      */
+} cg_request_t;
+
+typedef struct {
+  uint64_t id, tag;
+  int status, niter, converged, fast_iters;
+  double last_err;                 /* last stop-test value (Sinkhorn)             */
+  double t_submit, t_admit, t_done; /* cg_engine_clock() seconds                  */
+} cg_result_t;
+
+typedef struct {
+  size_t in_use_bytes, budget_bytes;
+  long long queued, active_bcd, active_splr, completed;
+  double bcd_bytes;      /* algorithmic bytes streamed by the Sinkhorn passes   */
+  double bcd_gpu_ms;     /* device time of the Sinkhorn chunks                  */
+  long long chunks, graph_builds;
+} cg_engine_stats_t;
+
+/* Starts the engine on the current device: a Sinkhorn batch scheduler and
+ * splr_workers SPLR worker threads.  budget_bytes bounds the device memory
+ * of admitted requests; max_batch bounds the Sinkhorn batch; chunk = ticks
+ * (row + column pass) per captured graph launch. */
+int cg_engine_create(size_t budget_bytes, int max_batch, int splr_workers, int chunk,
+                     cg_engine** out);
+/* Enqueues a request (non-blocking).  Input buffers must stay valid until its
+ * result is polled. */
+int cg_engine_submit(cg_engine* eng, const cg_request_t* req, uint64_t* id);
+/* Moves up to capacity finished results into results (waits up to wait_ms
+ * for the first one). */
+int cg_engine_poll(cg_engine* eng, cg_result_t* results, int capacity, int wait_ms, int* count);
+int cg_engine_stats(cg_engine* eng, cg_engine_stats_t* out);
+/* The engine's clock (seconds, monotonic), for latency accounting. */
+double cg_engine_clock(void);
+/* Stops the engine (admitted work finishes; queued requests are dropped). */
+int cg_engine_destroy(cg_engine* eng);
 
 /* ------------------------------------------------------------------------ */
 /* Test hooks of the reference (curegot.tests, src/tests.cpp:36-200).        */
