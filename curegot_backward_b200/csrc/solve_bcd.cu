@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "bcd.cuh"
@@ -185,6 +186,161 @@ int bcd_solve(const TM* M, const double* a, const double* b, double* Pout, doubl
   return CG_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free FP64 BCD (cg_bcd_f64_noalloc).
+//
+// Same kernels, geometry and loop as bcd_solve<double>; the scratch (log
+// marginals, the double-buffered duals, column-pass partials, counters, the
+// control state and the problem descriptor) lives in one file-scope device
+// array instead of a stream-ordered allocation.  Nothing in the array has to
+// start at zero: bcd_init_kernel writes the counters, the state and the
+// initial duals at the start of every call.  One array per device, so calls
+// on the same device must not overlap (the plan/dual kernels of a call still
+// read the array after it returns): issue them on one stream, or synchronize
+// between them.
+constexpr int kNoAllocMaxDim = 16384;
+constexpr size_t kNoAllocBytes = size_t(4) << 20;  // 4 MiB; n = m = 16384 needs ~2.5 MiB
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+namespace {
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+}  // namespace
+
+// Device address of this device's scratch array; resolved on the first call
+// per device (which may load the module, so it belongs before any capture).
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  CG_TRY_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) {
+    set_last_error("cg_bcd_f64_noalloc: device ordinal above 63", __FILE__, __LINE__);
+    return CG_ERR_INVALID_ARG;
+  }
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      set_last_error("cg_bcd_f64_noalloc: cudaGetSymbolAddress of the scratch array failed",
+                     __FILE__, __LINE__);
+      return CG_ERR_CUDA;
+    }
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return CG_OK;
+}
+
+int bcd_solve_noalloc(const double* M, const double* a, const double* b, double* Pout,
+                      double reg, int max_iter, double tol, int n, int m, int* niter,
+                      const double* x0, double* dual, cudaStream_t stream) {
+  if (!M || !a || !b || !niter || n <= 0 || m <= 0 || !(reg > 0.0) || !std::isfinite(reg)) {
+    set_last_error("cg_bcd_f64_noalloc: invalid argument", __FILE__, __LINE__);
+    return CG_ERR_INVALID_ARG;
+  }
+  if (n > kNoAllocMaxDim || m > kNoAllocMaxDim) {
+    set_last_error("cg_bcd_f64_noalloc: n and m must be <= 16384 (fixed scratch array)",
+                   __FILE__, __LINE__);
+    return CG_ERR_INVALID_ARG;
+  }
+  const int sms = sm_count_current();
+  BcdProb hp{};
+  bcd_geometry(n, m, (int)sizeof(double), sms, hp);
+  const int ncount = 2 + hp.col_strips;
+
+  // Carve the scratch exactly as bcd_solve sizes its workspace.
+  size_t top = 0;
+  auto take = [&top](size_t bytes) {
+    const size_t off = (top + 255) & ~size_t(255);
+    top = off + bytes;
+    return off;
+  };
+  const size_t o_loga = take(n * 8), o_logb = take(m * 8);
+  size_t o_al[2], o_be[2], o_als[2], o_bes[2];
+  for (int k = 0; k < 2; ++k) {
+    o_al[k] = take(n * 8);
+    o_be[k] = take(m * 8);
+    o_als[k] = take(n * 8);
+    o_bes[k] = take(m * 8);
+  }
+  const size_t parts = (hp.col_splits > 1) ? (size_t)hp.col_splits * m : 1;
+  const size_t o_cm = take(parts * 8), o_cs = take(parts * 8);
+  const size_t o_rp = take((size_t)hp.row_ctas * 4 * 8);
+  const size_t o_cp = take((size_t)hp.col_strips * 3 * 8);
+  const size_t o_cnt = take((size_t)ncount * sizeof(unsigned int));
+  const size_t o_st = take(sizeof(BcdState));
+  const size_t o_prob = take(sizeof(BcdProb));
+  if (top > kNoAllocBytes) {
+    set_last_error("cg_bcd_f64_noalloc: problem needs more than the 4 MiB scratch array",
+                   __FILE__, __LINE__);
+    return CG_ERR_INVALID_ARG;
+  }
+  void* base = nullptr;
+  CG_TRY(noalloc_scratch(&base));
+  char* s = static_cast<char*>(base);
+
+  hp.M = M;
+  hp.n = n;
+  hp.m = m;
+  hp.eta = reg;
+  hp.s2 = kLog2e / reg;
+  hp.a = a;
+  hp.loga = reinterpret_cast<double*>(s + o_loga);
+  hp.logb = reinterpret_cast<double*>(s + o_logb);
+  for (int k = 0; k < 2; ++k) {
+    hp.alpha[k] = reinterpret_cast<double*>(s + o_al[k]);
+    hp.beta[k] = reinterpret_cast<double*>(s + o_be[k]);
+    hp.alphas[k] = reinterpret_cast<double*>(s + o_als[k]);
+    hp.betas[k] = reinterpret_cast<double*>(s + o_bes[k]);
+  }
+  hp.col_m = reinterpret_cast<double*>(s + o_cm);
+  hp.col_s = reinterpret_cast<double*>(s + o_cs);
+  hp.row_part = reinterpret_cast<double*>(s + o_rp);
+  hp.col_part = reinterpret_cast<double*>(s + o_cp);
+  hp.counters = reinterpret_cast<unsigned int*>(s + o_cnt);
+  hp.st = reinterpret_cast<BcdState*>(s + o_st);
+  BcdProb* dprob = reinterpret_cast<BcdProb*>(s + o_prob);
+
+  { bcd_init_kernel<<<64, 256, 0, stream>>>(a, b, x0, n, m, hp.s2, const_cast<double*>(hp.loga),
+                                          const_cast<double*>(hp.logb), hp.alpha[0], hp.beta[0],
+                                          hp.alphas[0], hp.betas[0], hp.counters, ncount, hp.st,
+                                          max_iter, tol, 0); cg::count_launch(); }
+  CG_TRY_CUDA(cudaGetLastError());
+  CG_TRY_CUDA(cudaMemcpyAsync(dprob, &hp, sizeof(BcdProb), cudaMemcpyHostToDevice, stream));
+
+  BcdState hs{};
+  int chunk = 4;
+  int queued = 0;
+  while (true) {
+    const int todo = std::min(chunk, std::max(max_iter - queued, 0));
+    for (int c = 0; c < todo; ++c) {
+      launch_bcd_row(false, dprob, nullptr, nullptr, hp.row_ctas, stream);
+      launch_bcd_col(false, dprob, nullptr, nullptr, hp.col_strips * hp.col_splits, stream);
+    }
+    queued += todo;
+    CG_TRY_CUDA(cudaGetLastError());
+    CG_TRY_CUDA(cudaMemcpyAsync(&hs, hp.st, sizeof(BcdState), cudaMemcpyDeviceToHost, stream));
+    CG_TRY_CUDA(cudaStreamSynchronize(stream));
+    if (hs.done || queued >= max_iter) break;
+    chunk = std::min(chunk * 2, 64);
+  }
+  *niter = hs.niter;
+
+  if (Pout) {
+    const size_t total = (size_t)n * m;
+    const int blocks = (int)std::max<size_t>(1, std::min<size_t>((total + 255) / 256, sms * 16));
+    { plan_from_state_kernel<double><<<blocks, 256, 0, stream>>>(M, hp.st, dprob, Pout); cg::count_launch(); }
+  }
+  if (dual) {
+    dual_from_state_kernel<<<std::max(1, (n + m + 255) / 256), 256, 0, stream>>>(hp.st, dprob, dual);
+    cg::count_launch();
+  }
+  CG_TRY_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
 __global__ void diag_exp2_kernel(const double* x, double* y, int n, int mode) {
   __shared__ double tab[16];
   load_exp2_table(tab);
@@ -209,6 +365,12 @@ int cg_bcd_f64(const double* M, const double* a, const double* b, double* P, dou
                int max_iter, double tol, int n, int m, int* niter, const double* x0,
                double* dual, cudaStream_t stream) {
   return cg::bcd_solve<double>(M, a, b, P, reg, max_iter, tol, n, m, niter, x0, dual, stream);
+}
+
+int cg_bcd_f64_noalloc(const double* M, const double* a, const double* b, double* P, double reg,
+                       int max_iter, double tol, int n, int m, int* niter, const double* x0,
+                       double* dual, cudaStream_t stream) {
+  return cg::bcd_solve_noalloc(M, a, b, P, reg, max_iter, tol, n, m, niter, x0, dual, stream);
 }
 
 int cg_bcd_mixed(const float* M, const double* a, const double* b, double* P, double reg,

@@ -65,6 +65,32 @@ int cg_bcd_f64(const double* M, const double* a, const double* b, double* P, dou
                double* dual, cudaStream_t stream);
 
 /*
+ * Allocation-free FP64 BCD.  No counterpart in the reference: an addition
+ * for callers that must not allocate device memory at call time -- a host
+ * framework that owns HBM (a preallocating allocator, or a caching allocator
+ * that has reserved nearly all of it), where a stream-ordered allocation
+ * inside the call can fail with out-of-memory or grow a second pool beside
+ * the framework's.  Same arguments, kernels and results as cg_bcd_f64; the
+ * scratch is a 4 MiB file-scope device array inside this library instead of
+ * a cudaMallocAsync block, and nothing else is allocated.
+ *   - n and m must each be <= 16384, otherwise CG_ERR_INVALID_ARG (before any
+ *     launch; cg_last_error() says why).
+ *   - Nothing has to start at zero: every call initialises the state, the
+ *     counters and the duals it uses.
+ *   - The first call on each device resolves the array's address
+ *     (cudaGetSymbolAddress, which may load the module): make it before any
+ *     stream capture.  The call reads its state back with a stream
+ *     synchronize, like cg_bcd_f64.
+ *   - One array per device: calls on the same device must not overlap.  The
+ *     plan/dual kernels of a call still read the array after it returns, so
+ *     issue calls on one stream or synchronize between them; overlapping
+ *     calls race on the scratch.
+ */
+int cg_bcd_f64_noalloc(const double* M, const double* a, const double* b, double* P,
+                       double reg, int max_iter, double tol, int n, int m, int* niter,
+                       const double* x0, double* dual, cudaStream_t stream);
+
+/*
  * Mixed-precision BCD: M stored in FP32, duals and all reductions in FP64.
  * Same contract as cg_bcd_f64; P (nullable) is written in FP64.  The
  * FP32-M form of cuda_sinkhorn_bcd; the stopping rule is evaluated with the
