@@ -60,3 +60,23 @@ tests = _namespace("tests", "Test functions.", {
 })
 
 CuregotError = _native.CuregotError
+
+_DIRSOLVE = {"auto": 0, "dense": 1, "sparse": 2, "peel": 3}
+
+
+def set_direction_solver(mode: str = "auto") -> None:
+    """Choose the SPLR direction-solve path for this process: "dense" (Schur
+    complement + dense FP64 Cholesky), "sparse" (cuSOLVER sparse Cholesky of
+    the full sparsified Hessian in an AMD order), "peel" (fill-free
+    elimination of the nodes outside the graph's 2-core, then the dense Schur
+    path on the core) or "auto" (per sparsity pattern: "peel" when the core's
+    Schur complement is at most half the dense one, else "dense")."""
+    if mode not in _DIRSOLVE:
+        raise ValueError(f"direction solver must be one of {sorted(_DIRSOLVE)}, got {mode!r}")
+    _native.call("cg_splr_set_direction_solver", _DIRSOLVE[mode])
+
+
+def last_direction_solver() -> str | None:
+    """Path of the last SPLR direction solve on this thread."""
+    v = _native.lib().cg_splr_last_direction_solver()
+    return {0: "dense", 1: "sparse", 2: "peel"}.get(v)

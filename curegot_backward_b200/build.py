@@ -75,7 +75,7 @@ def build(verbose: bool = False, jobs: int | None = None, extra=()) -> str:
         return LIB
     tmp = LIB + ".tmp"
     cmd = [_nvcc(), *ARCH, "-shared", "-o", tmp, *objs,
-           "-L", os.path.join(CUDA_HOME, "lib64"), "-lcusolver", "-lcublas",
+           "-L", os.path.join(CUDA_HOME, "lib64"), "-lcusolver", "-lcusparse", "-lcublas",
            "-Xlinker", "-rpath=" + os.path.join(CUDA_HOME, "lib64")]
     if verbose:
         print(" ".join(cmd), flush=True)

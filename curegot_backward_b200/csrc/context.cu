@@ -98,9 +98,14 @@ __global__ void densify_lower_kernel(const double* val, const int* col, const in
 }  // namespace
 
 int ctx_apply_full(cg_ctx_s* c, const double* r, double* z, cudaStream_t st) {
-  cusolverDnHandle_t h = nullptr;
-  CG_TRY(solver_handle(&h));
-  CG_TRY(schur_solve(h, c->A, c->F, r, c->xtmp, 1, c->tmp, st));
+  if (c->path == 1) {
+    CG_TRY(spchol_solve(*c->sc, r, c->xtmp, 1, st));
+  } else {
+    cusolverDnHandle_t h = nullptr;
+    CG_TRY(solver_handle(&h));
+    if (c->path == 2) CG_TRY(peel_solve(*c->pf, c->A, h, r, c->xtmp, 1, st));
+    else CG_TRY(schur_solve(h, c->A, c->F, r, c->xtmp, 1, c->tmp, st));
+  }
   if (c->low_rank)
     { ctx_woodbury_kernel<<<1, 1024, 0, st>>>(c->xtmp, c->u, r, c->y, c->s, c->H, c->reg, c->ys); cg::count_launch(); }
   CG_TRY_CUDA(cudaMemcpyAsync(z, c->xtmp, c->H * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -243,6 +248,14 @@ int cg_ctx_destroy(cg_ctx* ctx) {
   cudaSetDevice(c->device);
   cudaDeviceSynchronize();
   if (c->block) cudaFree(c->block);
+  if (c->sc) {
+    cg::spchol_release(*c->sc);
+    delete c->sc;
+  }
+  if (c->pf) {
+    cg::peel_release(*c->pf);
+    delete c->pf;
+  }
   cudaSetDevice(prev);
   delete c;
   return CG_OK;
@@ -350,7 +363,7 @@ int cg_test_spd_solve_f64(const double* values, const int* colind, const int* ro
   CG_TRY(schur_lwork(h, n, lwork));
   Workspace ws(stream);
   const size_t o_S = ws.reserve<double>((size_t)n * n), o_w = ws.reserve<double>(std::max(lwork, 1));
-  const size_t o_info = ws.reserve<int>(1);
+  const size_t o_info = ws.reserve<int>(2);  // potrf, potrs
   CG_TRY(ws.allocate());
   double* S = ws.at<double>(o_S);
   CG_TRY_CUDA(cudaMemsetAsync(S, 0, (size_t)n * n * sizeof(double), stream));
@@ -361,7 +374,7 @@ int cg_test_spd_solve_f64(const double* values, const int* colind, const int* ro
   if (cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, n, S, n, ws.at<double>(o_w), lwork, info) !=
       CUSOLVER_STATUS_SUCCESS)
     return CG_ERR_SOLVER;
-  if (cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, n, 1, S, n, x, n, info) !=
+  if (cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, n, 1, S, n, x, n, info + 1) !=
       CUSOLVER_STATUS_SUCCESS)
     return CG_ERR_SOLVER;
   int hinfo = 0;

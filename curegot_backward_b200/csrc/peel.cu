@@ -1,0 +1,455 @@
+// Leaf-peeling LDL^T + 2-core Schur complement direction solve.
+//
+// Host (on every sparsity-pattern update, every `cycle` SPLR iterations):
+//   the pattern of A's lower CSR (the reference Hsl layout: row i < n holds
+//   only its diagonal; row n + j holds the alpha columns of beta node j in
+//   ascending order, then its diagonal) is copied to the host and peeled:
+//   round after round, every alive node of degree <= 1 whose single
+//   neighbour is not itself eliminated in the same round is eliminated.
+//   Each eliminated node remembers its parent (the neighbour still alive)
+//   and each node the list of its eliminated children.  The nodes never
+//   eliminated form the 2-core; its larger side is eliminated exactly and
+//   the smaller side carries the dense Schur complement.
+// Device (every iteration): one CTA computes the pivots round by round (a
+//   node's pivot pulls its children's contributions in a fixed order, so
+//   the result is deterministic), one CTA per Schur row assembles the core
+//   Schur complement, cuSOLVER potrf factors it.  The solve is a forward
+//   sweep over the rounds, potrs on the core, and a backward sweep.
+#include <algorithm>
+#include <cmath>
+
+#include "peel.cuh"
+
+namespace cg {
+
+namespace {
+
+constexpr int kMaxPeelRounds = 512;
+constexpr int kPeelThreads = 1024;
+
+struct PeelPtrs {
+  const int *order, *rptr, *diagq, *cptr, *child, *childq, *par, *parq;
+  const int *snodes, *enodes, *sptr, *sadj, *sq, *eptr, *eadj, *eq;
+};
+
+PeelPtrs ptrs_of(const PeelFactor& P) {
+  const int* b = P.ints;
+  PeelPtrs p;
+  p.order = b + P.off_order;
+  p.rptr = b + P.off_rptr;
+  p.diagq = b + P.off_diagq;
+  p.cptr = b + P.off_cptr;
+  p.child = b + P.off_child;
+  p.childq = b + P.off_childq;
+  p.par = b + P.off_par;
+  p.parq = b + P.off_parq;
+  p.snodes = b + P.off_snodes;
+  p.enodes = b + P.off_enodes;
+  p.sptr = b + P.off_sptr;
+  p.sadj = b + P.off_sadj;
+  p.sq = b + P.off_sq;
+  p.eptr = b + P.off_eptr;
+  p.eadj = b + P.off_eadj;
+  p.eq = b + P.off_eq;
+  return p;
+}
+
+// Pivots of every node, round by round; the core nodes come last (one round)
+// and receive their diagonal updated by their peeled children.
+__global__ void __launch_bounds__(kPeelThreads) peel_factor_kernel(
+    const double* __restrict__ val, PeelPtrs p, int rounds, double* __restrict__ d,
+    int* __restrict__ info) {
+  for (int r = 0; r <= rounds; ++r) {
+    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
+      const int v = p.order[idx];
+      double dv = val[p.diagq[v]];
+      for (int q = p.cptr[v]; q < p.cptr[v + 1]; ++q) {
+        const double a = val[p.childq[q]];
+        dv -= (a / d[p.child[q]]) * a;
+      }
+      d[v] = dv;
+      if (!(dv > 0.0) || !isfinite(dv)) info[1] = 1;
+    }
+    __syncthreads();
+  }
+}
+
+// Row t of the core Schur complement:
+//   S_t,: = d_{s_t} e_t - sum_{(e, q) in S-list t} (a_q / d_e) * (a_q' over E-list e)
+__global__ void peel_assemble_kernel(const double* __restrict__ val, PeelPtrs p,
+                                     const double* __restrict__ d, int kc,
+                                     double* __restrict__ S) {
+  const int t = blockIdx.x;
+  double* __restrict__ Sr = S + (size_t)t * kc;
+  for (int c = threadIdx.x; c < kc; c += blockDim.x) Sr[c] = 0.0;
+  __syncthreads();
+  if (threadIdx.x == 0) Sr[t] = d[p.snodes[t]];
+  __syncthreads();
+  for (int q = p.sptr[t]; q < p.sptr[t + 1]; ++q) {
+    const int e = p.sadj[q];
+    const double w = val[p.sq[q]] / d[p.enodes[e]];
+    for (int q2 = p.eptr[e] + threadIdx.x; q2 < p.eptr[e + 1]; q2 += blockDim.x)
+      Sr[p.eadj[q2]] -= w * val[p.eq[q2]];
+    __syncthreads();
+  }
+}
+
+// Forward sweep (y = L^{-1} b over the peeled rounds and the core's own
+// children), then the reduction of the core right-hand side to the Schur side.
+__global__ void __launch_bounds__(kPeelThreads) peel_forward_kernel(
+    const double* __restrict__ val, PeelPtrs p, int rounds, const double* __restrict__ d,
+    const double* __restrict__ rhs, int nrhs, int H, int kc, double* __restrict__ y,
+    double* __restrict__ rs) {
+  for (int r = 0; r <= rounds; ++r) {
+    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
+      const int v = p.order[idx];
+      for (int c = 0; c < nrhs; ++c) {
+        const double* yc = y + (size_t)c * H;
+        double yv = rhs[(size_t)c * H + v];
+        for (int q = p.cptr[v]; q < p.cptr[v + 1]; ++q) {
+          const int ch = p.child[q];
+          yv -= (val[p.childq[q]] / d[ch]) * yc[ch];
+        }
+        y[(size_t)c * H + v] = yv;
+      }
+    }
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < kc; t += blockDim.x) {
+    const int s = p.snodes[t];
+    for (int c = 0; c < nrhs; ++c) {
+      const double* yc = y + (size_t)c * H;
+      double acc = yc[s];
+      for (int q = p.sptr[t]; q < p.sptr[t + 1]; ++q) {
+        const int ev = p.enodes[p.sadj[q]];
+        acc -= (val[p.sq[q]] / d[ev]) * yc[ev];
+      }
+      rs[(size_t)c * kc + t] = acc;
+    }
+  }
+}
+
+// Core back-substitution, then the backward sweep over the peeled rounds.
+__global__ void __launch_bounds__(kPeelThreads) peel_backward_kernel(
+    const double* __restrict__ val, PeelPtrs p, int rounds, const double* __restrict__ d,
+    const double* __restrict__ y, const double* __restrict__ rs, int nrhs, int H, int kc,
+    int ke, double* __restrict__ x) {
+  for (int t = threadIdx.x; t < kc; t += blockDim.x)
+    for (int c = 0; c < nrhs; ++c) x[(size_t)c * H + p.snodes[t]] = rs[(size_t)c * kc + t];
+  for (int e = threadIdx.x; e < ke; e += blockDim.x) {
+    const int ev = p.enodes[e];
+    for (int c = 0; c < nrhs; ++c) {
+      double acc = y[(size_t)c * H + ev];
+      for (int q = p.eptr[e]; q < p.eptr[e + 1]; ++q)
+        acc -= val[p.eq[q]] * rs[(size_t)c * kc + p.eadj[q]];
+      x[(size_t)c * H + ev] = acc / d[ev];
+    }
+  }
+  __syncthreads();
+  for (int r = rounds - 1; r >= 0; --r) {
+    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
+      const int v = p.order[idx];
+      const int u = p.par[v];
+      for (int c = 0; c < nrhs; ++c) {
+        double xv = y[(size_t)c * H + v];
+        if (u >= 0) xv -= val[p.parq[v]] * x[(size_t)c * H + u];
+        x[(size_t)c * H + v] = xv / d[v];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+int alloc_dev(PeelFactor& P, void** ptr, size_t bytes) {
+  if (P.stream_ordered) CG_TRY_CUDA(cudaMallocAsync(ptr, bytes, P.alloc_stream));
+  else CG_TRY_CUDA(cudaMalloc(ptr, bytes));
+  return CG_OK;
+}
+
+void free_dev(PeelFactor& P, void* ptr) {
+  if (!ptr) return;
+  if (P.stream_ordered) cudaFreeAsync(ptr, P.alloc_stream);
+  else cudaFree(ptr);
+}
+
+}  // namespace
+
+void peel_release(PeelFactor& P) {
+  free_dev(P, P.block);
+  P.block = nullptr;
+  P.block_bytes = 0;
+  P.ready = false;
+}
+
+int peel_plan(PeelFactor& P, const SpHess& A, cudaStream_t st) {
+  const int n = A.n, m = A.m, H = A.H;
+  P.ready = false;
+  P.n = n;
+  P.m = m;
+  P.H = H;
+  std::vector<int> rp(H + 1);
+  CG_TRY_CUDA(cudaMemcpyAsync(rp.data(), A.rowptr, (H + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
+  CG_TRY_CUDA(cudaStreamSynchronize(st));
+  const int nl = rp[H];
+  std::vector<int> cl(std::max(nl, 1));
+  CG_TRY_CUDA(cudaMemcpyAsync(cl.data(), A.col, (size_t)nl * sizeof(int), cudaMemcpyDeviceToHost, st));
+  CG_TRY_CUDA(cudaStreamSynchronize(st));
+
+  // diagonal positions and the bipartite adjacency (neighbour, value index)
+  std::vector<int> diagq(H);
+  std::vector<int> deg(H, 0);
+  for (int i = 0; i < n; ++i) diagq[i] = rp[i];
+  for (int j = 0; j < m - 1; ++j) {
+    const int r = n + j;
+    diagq[r] = rp[r + 1] - 1;
+    for (int q = rp[r]; q < rp[r + 1] - 1; ++q) {
+      deg[r]++;
+      deg[cl[q]]++;
+    }
+  }
+  std::vector<int> aptr(H + 1, 0);
+  for (int v = 0; v < H; ++v) aptr[v + 1] = aptr[v] + deg[v];
+  std::vector<int> adj(std::max(aptr[H], 1)), adjq(std::max(aptr[H], 1));
+  {
+    std::vector<int> fill(aptr.begin(), aptr.end() - 1);
+    for (int j = 0; j < m - 1; ++j) {
+      const int r = n + j;
+      for (int q = rp[r]; q < rp[r + 1] - 1; ++q) {
+        const int i = cl[q];
+        adj[fill[r]] = i;
+        adjq[fill[r]++] = q;
+        adj[fill[i]] = r;
+        adjq[fill[i]++] = q;
+      }
+    }
+  }
+
+  // synchronous peeling
+  std::vector<char> alive(H, 1), taken(H, 0);
+  std::vector<int> par(H, -1), parq(H, -1);
+  std::vector<int> order;
+  order.reserve(H);
+  std::vector<int> rptr(1, 0);
+  std::vector<int> cur, next;
+  for (int v = 0; v < H; ++v)
+    if (deg[v] <= 1) cur.push_back(v);
+  int rounds = 0;
+  while (!cur.empty()) {
+    if (rounds >= kMaxPeelRounds) {
+      P.rounds = rounds + 1;  // over the limit: the caller keeps the dense path
+      P.kc = H;
+      P.ke = 0;
+      return CG_OK;
+    }
+    next.clear();
+    std::vector<int> sel;
+    for (int v : cur) {
+      if (!alive[v] || deg[v] > 1) continue;
+      int u = -1, uq = -1;
+      if (deg[v] == 1)
+        for (int q = aptr[v]; q < aptr[v + 1]; ++q)
+          if (alive[adj[q]]) {
+            u = adj[q];
+            uq = adjq[q];
+            break;
+          }
+      if (u >= 0 && taken[u]) {  // its neighbour goes this round: v waits
+        next.push_back(v);
+        continue;
+      }
+      taken[v] = 1;
+      par[v] = u;
+      parq[v] = uq;
+      sel.push_back(v);
+    }
+    for (int v : sel) {
+      alive[v] = 0;
+      order.push_back(v);
+    }
+    for (int v : sel) {
+      const int u = par[v];
+      if (u >= 0) {
+        deg[u]--;
+        if (deg[u] <= 1) next.push_back(u);
+      }
+    }
+    for (int v : sel) taken[v] = 0;
+    std::sort(next.begin(), next.end());
+    next.erase(std::unique(next.begin(), next.end()), next.end());
+    cur.swap(next);
+    rptr.push_back((int)order.size());
+    ++rounds;
+  }
+  const int npeel = (int)order.size();
+  // core nodes (one final round) and the sides of the core
+  std::vector<int> core_a, core_b;
+  for (int v = 0; v < H; ++v)
+    if (alive[v]) {
+      order.push_back(v);
+      (v < n ? core_a : core_b).push_back(v);
+    }
+  rptr.push_back((int)order.size());
+  const bool elim_a = core_a.size() >= core_b.size();
+  const std::vector<int>& snodes = elim_a ? core_b : core_a;
+  const std::vector<int>& enodes = elim_a ? core_a : core_b;
+  const int kc = (int)snodes.size(), ke = (int)enodes.size();
+  std::vector<int> loc(H, -1);
+  for (int t = 0; t < kc; ++t) loc[snodes[t]] = t;
+  for (int e = 0; e < ke; ++e) loc[enodes[e]] = e;
+  // children lists (eliminated neighbours of every node), in round order
+  std::vector<int> ccount(H, 0);
+  for (int k = 0; k < npeel; ++k)
+    if (par[order[k]] >= 0) ccount[par[order[k]]]++;
+  std::vector<int> cptr(H + 1, 0);
+  for (int v = 0; v < H; ++v) cptr[v + 1] = cptr[v] + ccount[v];
+  std::vector<int> child(std::max(cptr[H], 1)), childq(std::max(cptr[H], 1));
+  {
+    std::vector<int> fill(cptr.begin(), cptr.end() - 1);
+    for (int k = 0; k < npeel; ++k) {
+      const int v = order[k], u = par[v];
+      if (u < 0) continue;
+      child[fill[u]] = v;
+      childq[fill[u]++] = parq[v];
+    }
+  }
+  // core adjacency restricted to alive neighbours, as local indices
+  auto core_lists = [&](const std::vector<int>& nodes, std::vector<int>& ptr, std::vector<int>& ladj,
+                        std::vector<int>& lq) {
+    ptr.assign(nodes.size() + 1, 0);
+    ladj.clear();
+    lq.clear();
+    for (size_t t = 0; t < nodes.size(); ++t) {
+      const int v = nodes[t];
+      for (int q = aptr[v]; q < aptr[v + 1]; ++q)
+        if (alive[adj[q]]) {
+          ladj.push_back(loc[adj[q]]);
+          lq.push_back(adjq[q]);
+        }
+      ptr[t + 1] = (int)ladj.size();
+    }
+  };
+  std::vector<int> sptr, sadj, sq, eptr, eadj, eq;
+  core_lists(snodes, sptr, sadj, sq);
+  core_lists(enodes, eptr, eadj, eq);
+
+  // pack
+  std::vector<int>& I = P.h_ints;
+  I.clear();
+  auto put = [&I](const std::vector<int>& v, size_t count) {
+    const size_t off = I.size();
+    I.insert(I.end(), v.begin(), v.begin() + count);
+    while (I.size() % 64) I.push_back(0);  // 256-byte alignment of every array
+    return off;
+  };
+  P.off_order = put(order, order.size());
+  P.off_rptr = put(rptr, rptr.size());
+  P.off_diagq = put(diagq, H);
+  P.off_cptr = put(cptr, H + 1);
+  P.off_child = put(child, cptr[H]);
+  P.off_childq = put(childq, cptr[H]);
+  P.off_par = put(par, H);
+  P.off_parq = put(parq, H);
+  P.off_snodes = put(snodes, kc);
+  P.off_enodes = put(enodes, ke);
+  P.off_sptr = put(sptr, kc + 1);
+  P.off_sadj = put(sadj, sadj.size());
+  P.off_sq = put(sq, sq.size());
+  P.off_eptr = put(eptr, ke + 1);
+  P.off_eadj = put(eadj, eadj.size());
+  P.off_eq = put(eq, eq.size());
+  P.rounds = rounds;
+  P.npeel = npeel;
+  P.kc = kc;
+  P.ke = ke;
+  P.nchild = cptr[H];
+  P.ns_adj = (long long)sadj.size();
+  P.ne_adj = (long long)eadj.size();
+  return CG_OK;
+}
+
+int peel_upload(PeelFactor& P, cusolverDnHandle_t h, cudaStream_t st) {
+  const int H = P.H, kc = P.kc;
+  int lwork = 0;
+  if (kc > 0 &&
+      cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, kc, nullptr, kc, &lwork) !=
+          CUSOLVER_STATUS_SUCCESS) {
+    set_last_error("cusolverDnDpotrf_bufferSize failed", __FILE__, __LINE__);
+    return CG_ERR_SOLVER;
+  }
+  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t ib = al(P.h_ints.size() * sizeof(int));
+  const size_t bytes = ib + al((size_t)H * 8) + al((size_t)kc * kc * 8) +
+                       al((size_t)std::max(lwork, 1) * 8) + al(3 * sizeof(int)) +
+                       al((size_t)2 * H * 8) + al((size_t)2 * std::max(kc, 1) * 8);
+  if (bytes > P.block_bytes) {
+    free_dev(P, P.block);
+    P.block = nullptr;
+    P.block_bytes = 0;
+    CG_TRY(alloc_dev(P, &P.block, bytes));
+    P.block_bytes = bytes;
+  }
+  char* p = static_cast<char*>(P.block);
+  P.ints = reinterpret_cast<int*>(p); p += ib;
+  P.d = reinterpret_cast<double*>(p); p += al((size_t)H * 8);
+  P.S = reinterpret_cast<double*>(p); p += al((size_t)kc * kc * 8);
+  P.work = reinterpret_cast<double*>(p); p += al((size_t)std::max(lwork, 1) * 8);
+  P.info = reinterpret_cast<int*>(p); p += al(3 * sizeof(int));
+  P.y = reinterpret_cast<double*>(p); p += al((size_t)2 * H * 8);
+  P.rs = reinterpret_cast<double*>(p);
+  P.lwork = lwork;
+  CG_TRY_CUDA(cudaMemcpyAsync(P.ints, P.h_ints.data(), P.h_ints.size() * sizeof(int),
+                              cudaMemcpyHostToDevice, st));
+  // the pageable source is staged before cudaMemcpyAsync returns
+  P.ready = true;
+  return CG_OK;
+}
+
+int peel_factor(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, cudaStream_t st) {
+  if (!P.ready) {
+    set_last_error("peel factor: no plan for the current pattern", __FILE__, __LINE__);
+    return CG_ERR_INVALID_ARG;
+  }
+  const PeelPtrs pp = ptrs_of(P);
+  CG_TRY_CUDA(cudaMemsetAsync(P.info, 0, 3 * sizeof(int), st));
+  { peel_factor_kernel<<<1, kPeelThreads, 0, st>>>(A.val, pp, P.rounds, P.d, P.info); count_launch(); }
+  CG_TRY_CUDA(cudaGetLastError());
+  if (P.kc > 0) {
+    { peel_assemble_kernel<<<P.kc, 256, 0, st>>>(A.val, pp, P.d, P.kc, P.S); count_launch(); }
+    CG_TRY_CUDA(cudaGetLastError());
+    if (cusolverDnSetStream(h, st) != CUSOLVER_STATUS_SUCCESS) return CG_ERR_SOLVER;
+    if (cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, P.kc, P.S, P.kc, P.work, P.lwork, P.info) !=
+        CUSOLVER_STATUS_SUCCESS) {
+      set_last_error("cusolverDnDpotrf failed to launch", __FILE__, __LINE__);
+      return CG_ERR_SOLVER;
+    }
+  }
+  return CG_OK;
+}
+
+int peel_info_async(const PeelFactor& P, int* host2, cudaStream_t st) {
+  CG_TRY_CUDA(cudaMemcpyAsync(host2, P.info, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  return CG_OK;
+}
+
+int peel_solve(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, const double* rhs,
+               double* x, int nrhs, cudaStream_t st) {
+  if (nrhs < 1 || nrhs > 2) return CG_ERR_INVALID_ARG;
+  const PeelPtrs pp = ptrs_of(P);
+  { peel_forward_kernel<<<1, kPeelThreads, 0, st>>>(A.val, pp, P.rounds, P.d, rhs, nrhs, P.H,
+                                                    P.kc, P.y, P.rs); count_launch(); }
+  CG_TRY_CUDA(cudaGetLastError());
+  if (P.kc > 0) {
+    if (cusolverDnSetStream(h, st) != CUSOLVER_STATUS_SUCCESS) return CG_ERR_SOLVER;
+    if (cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, P.kc, nrhs, P.S, P.kc, P.rs, P.kc,
+                         P.info + 2) != CUSOLVER_STATUS_SUCCESS) {
+      set_last_error("cusolverDnDpotrs failed to launch", __FILE__, __LINE__);
+      return CG_ERR_SOLVER;
+    }
+  }
+  { peel_backward_kernel<<<1, kPeelThreads, 0, st>>>(A.val, pp, P.rounds, P.d, P.y, P.rs, nrhs,
+                                                     P.H, P.kc, P.ke, x); count_launch(); }
+  CG_TRY_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
+}  // namespace cg

@@ -1,0 +1,68 @@
+// Direction solve by leaf peeling + dense Schur complement on the 2-core.
+//
+// The SPLR sparsified Hessian A (H = n + m - 1) is a diagonal plus a
+// bipartite graph between the alpha nodes (rows i < n) and the beta nodes
+// (rows n + j).  At the default density the graph is close to a forest.
+// Eliminating a node of degree <= 1 creates no fill (it only changes the
+// pivot of its single neighbour), so the nodes outside the graph's 2-core
+// are eliminated first, in rounds of independent leaves, as an LDL^T
+// factorization with 1x1 pivots.  What remains (the 2-core, with updated
+// diagonals) is factored like the dense Schur path: its larger side is
+// eliminated exactly and the Schur complement of the smaller side is
+// factored with cuSOLVER potrf in FP64.  The result is A^{-1} b to rounding,
+// computed with a different elimination order than the reference's cuDSS
+// call (src/linsolve.cu:159-268).
+#pragma once
+
+#include <cusolverDn.h>
+
+#include <vector>
+
+#include "sparsify.cuh"
+
+namespace cg {
+
+struct PeelFactor {
+  int H = 0, n = 0, m = 0;
+  int rounds = 0;       // peel rounds (the core is processed as one extra round)
+  int npeel = 0;        // peeled nodes
+  int kc = 0, ke = 0;   // core nodes on the Schur side / on the eliminated side
+  long long nchild = 0, ns_adj = 0, ne_adj = 0;
+  // host plan
+  std::vector<int> h_ints;  // every int array below, packed in device order
+  size_t off_order = 0, off_rptr = 0, off_diagq = 0, off_cptr = 0, off_child = 0, off_childq = 0,
+         off_par = 0, off_parq = 0, off_snodes = 0, off_enodes = 0, off_sptr = 0, off_sadj = 0,
+         off_sq = 0, off_eptr = 0, off_eadj = 0, off_eq = 0;
+  // device
+  void* block = nullptr;
+  size_t block_bytes = 0;
+  int* ints = nullptr;
+  double* d = nullptr;      // [H] pivots (core nodes: updated diagonal)
+  double* S = nullptr;      // [kc * kc] Schur complement / factor
+  double* work = nullptr;   // potrf workspace
+  int lwork = 0;
+  int* info = nullptr;      // [3] potrf info, pivot check, potrs info
+  double* y = nullptr;      // [2H] forward-substitution values
+  double* rs = nullptr;     // [2 kc] reduced right-hand sides / Schur solution
+  bool ready = false;
+  bool stream_ordered = false;
+  cudaStream_t alloc_stream = nullptr;
+};
+
+// Host plan of the current pattern of A (copies the pattern to the host and
+// synchronizes the stream).  Sets rounds, kc, ke; ready stays false.
+int peel_plan(PeelFactor& P, const SpHess& A, cudaStream_t st);
+// Device buffers + upload of the plan.
+int peel_upload(PeelFactor& P, cusolverDnHandle_t h, cudaStream_t st);
+// Numeric factorization of A's current values (async; a non-positive pivot
+// or a potrf failure lands in info[0] / info[1]).
+int peel_factor(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, cudaStream_t st);
+// Device-side status of the last factorization: copy of info[0..1] (async;
+// non-zero = not positive definite).
+int peel_info_async(const PeelFactor& P, int* host2, cudaStream_t st);
+// x = A^{-1} rhs for nrhs <= 2 column-major right-hand sides (leading dim H).
+int peel_solve(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, const double* rhs,
+               double* x, int nrhs, cudaStream_t st);
+void peel_release(PeelFactor& P);
+
+}  // namespace cg

@@ -196,7 +196,7 @@ int schur_solve(cusolverDnHandle_t h, const SpHess& A, const SchurFactor& F, con
         mode, A.val, A.col, A.rowptr, A.ipt, A.ij, A.iv, A.n, A.H, k, rhs, nrhs, tmp); cg::count_launch(); }
     CG_TRY_CUDA(cudaGetLastError());
     if (cusolverDnSetStream(h, st) != CUSOLVER_STATUS_SUCCESS) return CG_ERR_SOLVER;
-    if (cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, k, nrhs, F.S, k, tmp, k, F.info) !=
+    if (cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, k, nrhs, F.S, k, tmp, k, F.solve_info) !=
         CUSOLVER_STATUS_SUCCESS) {
       set_last_error("cusolverDnDpotrs failed to launch", __FILE__, __LINE__);
       return CG_ERR_SOLVER;

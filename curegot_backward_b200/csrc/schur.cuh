@@ -14,6 +14,7 @@ struct SchurFactor {
   bool big_alpha = true;   // eliminate the alpha block (n >= m-1)
   double* S = nullptr;     // [k*k] factor (in place)
   int* info = nullptr;     // [1] potrf info (device)
+  int* solve_info = nullptr;  // [1] potrs info (kept apart so potrf's survives)
   double* work = nullptr;  // potrf workspace
   int lwork = 0;
 };

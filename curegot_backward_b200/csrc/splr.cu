@@ -9,15 +9,19 @@
 // flow; every vector and matrix operation runs on the device:
 //   plan pass + objective/gradient       tpass.cu
 //   sparsification into CSR              sparsify.cu
-//   direction solve                      schur.cu (cuSOLVER FP64 Cholesky)
+//   direction solve                      schur.cu (dense Schur complement, cuSOLVER
+//                                        potrf) or spchol.cu (sparse Cholesky),
+//                                        chosen per sparsity pattern
 //   secant pair, BFGS/Woodbury, scaling  kernels below (one CTA, device scalars)
 //   candidate Sinkhorn iterate           bcd.cu passes
 // The host reads 32-64 bytes per line-search trial and per direction step.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <memory>
 #include <vector>
 
 #include "bcd.cuh"
@@ -30,6 +34,17 @@ namespace cg {
 namespace {
 
 constexpr double kInf = std::numeric_limits<double>::infinity();
+
+// Direction-solve selection (process-wide mode, see DirSolveMode).  Auto mode
+// plans the leaf peeling of every new sparsity pattern on the host and takes
+// it when the core Schur complement is at most half the dense one; the sparse
+// Cholesky (cuSOLVER) is only used when asked for: on B200 it was slower than
+// the dense Schur path at every measured size.
+constexpr int kMaxPeelRoundsUsed = 512;
+enum { kPathDense = 0, kPathSparse = 1, kPathPeel = 2 };
+
+std::atomic<int> g_dir_mode{kDirAuto};
+thread_local int g_last_dir = -1;
 
 // ---------------------------------------------------------------------------
 // Small single-CTA vector kernels (H <= a few 10^4): fixed-order reductions.
@@ -278,6 +293,7 @@ static size_t hblock_bytes(int n, int m, long long kcap, int k, int lwork) {
   add(std::max<long long>(kcap, 1) * sizeof(double));
   add((size_t)k * k * sizeof(double));
   add(sizeof(int));
+  add(sizeof(int));
   add((size_t)std::max(lwork, 1) * sizeof(double));
   add(2 * (size_t)H * sizeof(double));  // rhs2 = [g, y]
   add(2 * (size_t)H * sizeof(double));  // sol2 = [x, u]
@@ -325,6 +341,7 @@ static void hblock_carve(void* base, int n, int m, long long kcap, int k, bool b
   hb.F.big_alpha = big_alpha;
   hb.F.S = reinterpret_cast<double*>(take((size_t)k * k * sizeof(double)));
   hb.F.info = reinterpret_cast<int*>(take(sizeof(int)));
+  hb.F.solve_info = reinterpret_cast<int*>(take(sizeof(int)));
   hb.F.work = reinterpret_cast<double*>(take((size_t)std::max(lwork, 1) * sizeof(double)));
   hb.F.lwork = lwork;
   hb.rhs2 = reinterpret_cast<double*>(take(2 * (size_t)H * sizeof(double)));
@@ -395,6 +412,24 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
       else cudaFreeAsync(p, s);
     }
   } hguard{hbase, owned_by_ctx, st};
+  struct ScDelete {
+    void operator()(SparseChol* p) const {
+      spchol_release(*p);
+      delete p;
+    }
+  };
+  std::unique_ptr<SparseChol, ScDelete> sc(new SparseChol());
+  sc->stream_ordered = !owned_by_ctx;
+  sc->alloc_stream = st;
+  struct PfDelete {
+    void operator()(PeelFactor* p) const {
+      peel_release(*p);
+      delete p;
+    }
+  };
+  std::unique_ptr<PeelFactor, PfDelete> pf(new PeelFactor());
+  pf->stream_ordered = !owned_by_ctx;
+  pf->alloc_stream = st;
 
   // per-solve workspace
   int tstrips = 1, tsplits = 1;
@@ -554,6 +589,60 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
   double shift = std::min(gnorm, prm.shift_max);
   long long Kcur = 0;
 
+  // direction-solve path for the current sparsity pattern
+  bool pattern_new = true;
+  int path = kPathDense;
+  const int dir_mode = g_dir_mode.load();
+  auto prepare_direction = [&]() -> int {
+    if (!pattern_new) return CG_OK;
+    pattern_new = false;
+    path = kPathDense;
+    if (dir_mode == kDirDense) return CG_OK;
+    if (dir_mode == kDirSparse) {
+      CG_TRY(spchol_order(*sc, hb.A, kInf, st));
+      CG_TRY(spchol_analyze(*sc, st));
+      path = kPathSparse;
+      return CG_OK;
+    }
+    // auto / peel: leaf peeling when its core Schur complement is at most
+    // half the dense one (1/8 of the potrf work), else the dense Schur path
+    CG_TRY(peel_plan(*pf, hb.A, st));
+    const bool fits = pf->rounds <= kMaxPeelRoundsUsed;
+    if (fits && (dir_mode == kDirPeel || 2 * pf->kc <= k)) {
+      CG_TRY(peel_upload(*pf, sol, st));
+      path = kPathPeel;
+    }
+    return CG_OK;
+  };
+  // factor A (current values); *bad (host) = 1 when the sparse Cholesky met a
+  // non-positive pivot.  The dense and peel paths report on the device
+  // (read_factor_info after the next synchronization).
+  auto factor_direction = [&](int* sp_bad) -> int {
+    CG_TRY(prepare_direction());
+    *sp_bad = 0;
+    if (path == kPathSparse) {
+      int zp = -1;
+      CG_TRY(spchol_factor(*sc, hb.A, st, &zp));
+      *sp_bad = (zp >= 0) ? 1 : 0;
+      return CG_OK;
+    }
+    if (path == kPathPeel) return peel_factor(*pf, hb.A, sol, st);
+    return schur_factor(sol, hb.A, hb.F, st);
+  };
+  auto solve_direction = [&](const double* rhs, double* x, int nrhs) -> int {
+    if (path == kPathSparse) return spchol_solve(*sc, rhs, x, nrhs, st);
+    if (path == kPathPeel) return peel_solve(*pf, hb.A, sol, rhs, x, nrhs, st);
+    return schur_solve(sol, hb.A, hb.F, rhs, x, nrhs, hb.tmp, st);
+  };
+  // queue the device status of the last factorization into info2[0..1]
+  auto queue_factor_info = [&](int* info2) -> int {
+    info2[0] = info2[1] = 0;
+    if (path == kPathPeel) return peel_info_async(*pf, info2, st);
+    if (path == kPathDense)
+      CG_TRY_CUDA(cudaMemcpyAsync(info2, hb.F.info, sizeof(int), cudaMemcpyDeviceToHost, st));
+    return CG_OK;
+  };
+
   auto dual_sphess = [&](double dens, double sh, bool fixed) -> int {
     dens = std::min(std::max(dens, 0.0), 1.0);
     long long K = (long long)(dens * (double)Te);
@@ -562,6 +651,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     long long Ks = std::min(std::max(K, 1LL), Te);
     Kcur = Ks;
     if (fixed) return sparsify_refresh(f32, M, gamma, rows, cols, n, m, s2, sh, hb.A, st);
+    pattern_new = true;
     return sparsify_select_and_build(f32, M, gamma, rows, cols, n, m, s2, sh, Ks, hb.A, sw, st);
   };
   CG_TRY(dual_sphess(density, shift * reg, false));
@@ -596,18 +686,20 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
 
     // search direction (sinkhorn_splr.cu:538-649)
     CG_TRY_CUDA(cudaMemcpyAsync(hb.rhs2, grad, H * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    CG_TRY(schur_factor(sol, hb.A, hb.F, st));
+    int sp_bad = 0;
+    CG_TRY(factor_direction(&sp_bad));
     const int nrhs = (iter > 0) ? 2 : 1;
-    CG_TRY(schur_solve(sol, hb.A, hb.F, hb.rhs2, hb.sol2, nrhs, hb.tmp, st));
+    CG_TRY(solve_direction(hb.rhs2, hb.sol2, nrhs));
+    g_last_dir = path;
     { woodbury_kernel<<<1, 1024, 0, st>>>(hb.sol2, hb.sol2 + H, grad, hb.rhs2 + H, hb.s, H, reg, 1,
                                         hb.dres); cg::count_launch(); }
     CG_TRY_CUDA(cudaGetLastError());
     DirRes dr{};
-    int info = 0;
-    CG_TRY_CUDA(cudaMemcpyAsync(&info, hb.F.info, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int info2[2];
+    CG_TRY(queue_factor_info(info2));
     CG_TRY(read_dev(&dr, hb.dres, st));
-    if (info != 0) {
-      set_last_error("direction solve: Schur complement not positive definite", __FILE__,
+    if (sp_bad || info2[0] != 0 || info2[1] != 0) {
+      set_last_error("direction solve: sparsified Hessian not positive definite", __FILE__,
                      __LINE__);
       return CG_ERR_NOT_SPD;
     }
@@ -783,6 +875,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
 
   if (ctx_out) {
     *ctx_out = nullptr;
+    int ctx_sp_bad = 0;
     cg_ctx_s* c = new cg_ctx_s();
     CG_TRY_CUDA(cudaGetDevice(&c->device));
     c->n = n;
@@ -797,7 +890,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
       c->ys = 0.0;
       c->low_rank = false;
       if (c->valid) {
-        int rc = schur_factor(sol, hb.A, hb.F, st);
+        int rc = factor_direction(&ctx_sp_bad);
         if (rc != CG_OK) {
           delete c;
           return rc;
@@ -809,6 +902,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     }
     c->A = hb.A;
     c->F = hb.F;
+    c->path = path;
     c->s = hb.s;
     c->y = hb.rhs2 + H;
     c->u = hb.sol2 + H;
@@ -822,14 +916,17 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     CG_TRY_CUDA(cudaMemcpyAsync(&rp, hb.A.rowptr + H, sizeof(int), cudaMemcpyDeviceToHost, st));
     CG_TRY_CUDA(cudaMemcpyAsync(c->point, c->fallback ? gamma : gamma_prev, H * sizeof(double),
                                 cudaMemcpyDeviceToDevice, st));
-    int info = 0;
-    CG_TRY_CUDA(cudaMemcpyAsync(&info, hb.F.info, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int info2[2];
+    CG_TRY(queue_factor_info(info2));
     CG_TRY_CUDA(cudaStreamSynchronize(st));
+    const int info = ctx_sp_bad | info2[0] | info2[1];
     c->nnz = rp;
     c->has_point = true;
     if (info != 0) c->valid = false;
     c->block = hbase;
     hbase = nullptr;  // ownership moves to the context
+    if (path == kPathSparse) c->sc = sc.release();
+    if (path == kPathPeel) c->pf = pf.release();
     *ctx_out = c;
   }
   ws.release();
@@ -844,3 +941,19 @@ template int splr_solve<float>(const float*, const double*, const double*, doubl
                                cg_ctx_s**, double*, cudaStream_t);
 
 }  // namespace cg
+
+extern "C" {
+
+int cg_splr_set_direction_solver(int mode) {
+  if (mode < cg::kDirAuto || mode > cg::kDirPeel) {
+    cg::set_last_error("cg_splr_set_direction_solver: mode must be 0, 1, 2 or 3", __FILE__,
+                       __LINE__);
+    return CG_ERR_INVALID_ARG;
+  }
+  cg::g_dir_mode.store(mode);
+  return CG_OK;
+}
+
+int cg_splr_last_direction_solver(void) { return cg::g_last_dir; }
+
+}  // extern "C"

@@ -3,6 +3,8 @@
 #pragma once
 
 #include "schur.cuh"
+#include "peel.cuh"
+#include "spchol.cuh"
 
 struct cg_ctx_s;
 
@@ -14,6 +16,13 @@ struct DirRes {
   int low_rank;
   int pad;
 };
+
+// Direction-solve choice (process-wide): 0 auto -- per sparsity pattern, leaf
+// peeling + core Schur complement when the core Schur complement is at most
+// half the dense one, else the dense Schur path; 1 always dense Schur;
+// 2 always cuSOLVER sparse Cholesky; 3 always leaf peeling (unless the
+// pattern needs more peel rounds than the solver allows).
+enum DirSolveMode { kDirAuto = 0, kDirDense = 1, kDirSparse = 2, kDirPeel = 3 };
 
 struct SplrParams {
   double reg, tol;
@@ -45,6 +54,9 @@ struct cg_ctx_s {
   void* block = nullptr;  // single allocation owning every device buffer below
   cg::SpHess A;
   cg::SchurFactor F;
+  cg::SparseChol* sc = nullptr;  // sparse Cholesky factor (owned) when path == 1
+  cg::PeelFactor* pf = nullptr;  // leaf-peeling factor (owned) when path == 2
+  int path = 0;                  // factor of the last direction solve: 0 F, 1 sc, 2 pf
   double* s = nullptr;
   double* y = nullptr;
   double* u = nullptr;  // A^{-1} y

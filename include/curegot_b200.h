@@ -158,6 +158,28 @@ int cg_splr_mixed(const float* M, const double* a, const double* b, double* P, d
                   int verbose, const double* x0, double* dual, cg_ctx** ctx_out,
                   int* converged, double* trace, cudaStream_t stream);
 
+/*
+ * Direction-solve path of the SPLR Newton step (process-wide setting).  The
+ * reference always calls cuDSS sparse Cholesky (src/linsolve.cu:159-268);
+ * here the same A^{-1}[g, y] is computed either by
+ *   CG_DIRSOLVE_DENSE : exact elimination of the larger diagonal block and a
+ *                       dense FP64 Cholesky (cuSOLVER potrf) of the Schur
+ *                       complement, or
+ *   CG_DIRSOLVE_SPARSE: cuSOLVER sparse Cholesky of the full A in an AMD order
+ *                       computed on the host on every pattern update;
+ *   CG_DIRSOLVE_PEEL  : LDL^T elimination of the nodes outside the graph's
+ *                       2-core (degree <= 1, no fill), planned on the host on
+ *                       every pattern update, then the dense Schur path on
+ *                       the 2-core only;
+ *   CG_DIRSOLVE_AUTO  : (default) per pattern, PEEL when the 2-core's Schur
+ *                       complement is at most half the dense one, else DENSE.
+ * cg_splr_last_direction_solver() returns the path of the last direction
+ * solve issued by the calling thread (0 dense, 1 sparse, 2 peel, -1 none).
+ */
+enum { CG_DIRSOLVE_AUTO = 0, CG_DIRSOLVE_DENSE = 1, CG_DIRSOLVE_SPARSE = 2, CG_DIRSOLVE_PEEL = 3 };
+int cg_splr_set_direction_solver(int mode);
+int cg_splr_last_direction_solver(void);
+
 /* Context properties (reg, dim, low_rank_enabled, is_fallback, ...;
  * src/solvers_torch.cpp:691-696). */
 int cg_ctx_info(const cg_ctx* ctx, cg_ctx_info_t* out);

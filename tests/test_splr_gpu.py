@@ -99,7 +99,53 @@ def test_splr_matches_oracle(cuda_dev, n, m, reg, kind):
     assert np.abs(got["plan"] - ref["plan"]).max() <= 1e-12
 
 
-def test_splr_bwd_context_matches_oracle(cuda_dev):
+@pytest.fixture
+def dirsolver():
+    """Sets the process-wide direction-solve path; restores "auto" afterwards."""
+    yield cg.set_direction_solver
+    cg.set_direction_solver("auto")
+
+
+@pytest.mark.parametrize("mode", ["dense", "peel", "sparse"])
+@pytest.mark.parametrize("n,m,reg,kind,dens", [(120, 90, 0.05, "gauss", None),
+                                               (90, 150, 0.01, "gauss", None),
+                                               (64, 64, 0.01, "gauss", 0.1),
+                                               (45, 2, 0.05, "uniform", None)])
+def test_direction_solvers_match_oracle(cuda_dev, dirsolver, mode, n, m, reg, kind, dens):
+    # every direction-solve path is an exact A^{-1}[g, y]: same bar as the
+    # default path against the oracle's dense Schur elimination
+    dirsolver(mode)
+    M, a, b = problem(n, m, n + 3 * m, kind)
+    kw = {} if dens is None else {"density": dens}
+    got = cg.numpy.sinkhorn_splr(M, a, b, reg, tol=1e-8, max_iter=300, return_trace=True, **kw)
+    assert cg.last_direction_solver() == mode
+    ref = oracle.splr(M, a, b, reg, tol=1e-8, max_iter=300, density=dens)
+    assert got["niter"] == ref["niter"]
+    np.testing.assert_array_equal(got["trace"][:, [3, 4, 5, 6, 7]], ref["trace"][:, [3, 4, 5, 6, 7]])
+    assert np.abs(got["dual"] - ref["dual"]).max() <= 1e-10 * np.abs(ref["dual"]).max()
+    assert np.abs(got["plan"] - ref["plan"]).max() <= 1e-12
+
+
+def test_auto_direction_solver_peels_forest_like_patterns(cuda_dev, dirsolver):
+    # at the default density the Hessian graph of a point-cloud problem is
+    # close to a forest: auto mode takes the peel path
+    dirsolver("auto")
+    M, a, b = problem(600, 500, 3, "gauss")
+    got = cg.numpy.sinkhorn_splr(M, a, b, 0.01, tol=1e-8, max_iter=300)
+    assert cg.last_direction_solver() == "peel"
+    ref = oracle.splr(M, a, b, 0.01, tol=1e-8, max_iter=300)
+    assert got["niter"] == ref["niter"]
+    assert np.abs(got["dual"] - ref["dual"]).max() <= 1e-10 * np.abs(ref["dual"]).max()
+
+
+def test_direction_solver_rejects_unknown_mode():
+    with pytest.raises(ValueError):
+        cg.set_direction_solver("lu")
+
+
+@pytest.mark.parametrize("mode", ["dense", "peel", "sparse"])
+def test_splr_bwd_context_matches_oracle(cuda_dev, dirsolver, mode):
+    dirsolver(mode)
     n, m, reg = 70, 50, 0.02
     M, a, b = problem(n, m, 11, "gauss")
     Mt = torch.tensor(M, device=cuda_dev)
