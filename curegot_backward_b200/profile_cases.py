@@ -1,0 +1,129 @@
+"""Fixed single-GPU cases of the hot kernels, for timing and for profilers.
+
+    python -m curegot_backward_b200.profile_cases bcd --n 8192 --m 8192 --precision mixed
+    python -m curegot_backward_b200.profile_cases splr --n 4096 --m 4096 --density 0.1
+    python -m curegot_backward_b200.profile_cases backward --n 2048 --m 2560
+
+Each case builds a seeded synthetic problem on cuda:0, runs it once to warm
+up, then times `--reps` runs with CUDA events on the launching stream and
+prints one JSON line.  Achieved bandwidth uses algorithmic bytes:
+  bcd       2 * n * m * sizeof(M) per iteration (one row pass + one column
+            pass, each reading M once), iterations fixed by --iters (tol 0);
+  backward  n * m * 8 per PCG iteration (one fused pass over T), plus the
+            right-hand-side and gradient-assembly passes (2 * n * m * 8 reads
+            of T and G, n * m * 8 written).
+The SPLR case reports wall time, iterations and the direction-solve path.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+
+import torch
+
+from . import _solvers, synthetic
+from .backward import solve_backward
+
+
+def _peak():
+    p = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                     "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _gauss(n, m, d, seed, dev, dtype):
+    spec = synthetic.StreamSpec(0, n, m, d, 0.0, "bcd", seed, 0.0)
+    return synthetic.stream_problem(spec, dev, dtype)
+
+
+def _time(fn, reps):
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    out = None
+    for _ in range(reps):
+        out = fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps, out
+
+
+def case_bcd(a):
+    dev = torch.device("cuda", 0)
+    dtype = torch.float32 if a.precision == "mixed" else torch.float64
+    M, am, bm = _gauss(a.n, a.m, a.d, a.seed, dev, dtype)
+    run = lambda: _solvers._bcd_device(M, am, bm, a.eta, 0.0, a.iters, None, a.precision,
+                                       want_plan=False)
+    ms, out = _time(run, a.reps)
+    niter = out[0]
+    bytes_ = 2.0 * a.n * a.m * M.element_size() * niter
+    gbs = bytes_ / (ms / 1e3) / 1e9
+    peak, kind = _peak()
+    return {"case": "bcd", "n": a.n, "m": a.m, "precision": a.precision, "eta": a.eta,
+            "iterations": niter, "ms_per_solve": ms, "us_per_iteration": 1e3 * ms / niter,
+            "algorithmic_GBps": gbs, "peak_GBps": peak, "peak_kind": kind, "frac": gbs / peak}
+
+
+def case_splr(a):
+    import curegot_backward_b200 as cg
+    dev = torch.device("cuda", 0)
+    dtype = torch.float32 if a.precision == "mixed" else torch.float64
+    M, am, bm = _gauss(a.n, a.m, a.d, a.seed, dev, dtype)
+    if a.solver:
+        cg.set_direction_solver(a.solver)
+    kw = {} if a.density is None else {"density": a.density}
+    run = lambda: cg.torch.sinkhorn_splr(M, am, bm, a.eta, tol=a.tol, max_iter=1000,
+                                         precision=a.precision, **kw)
+    ms, out = _time(run, a.reps)
+    return {"case": "splr", "n": a.n, "m": a.m, "precision": a.precision, "eta": a.eta,
+            "density": a.density, "iterations": out["niter"], "ms_per_solve": ms,
+            "direction_solver": cg.last_direction_solver()}
+
+
+def case_backward(a):
+    import curegot_backward_b200 as cg
+    dev = torch.device("cuda", 0)
+    M, am, bm = _gauss(a.n, a.m, a.d, a.seed, dev, torch.float64)
+    out = cg.torch.sinkhorn_splr_bwd(M, am, bm, a.eta, 1e-8, 1000, 0)
+    dual, ctx = out["dual"], out["context"]
+    T = torch.exp((dual[: a.n, None] + dual[None, a.n:] - M) / a.eta)
+    G = 2.0 * T
+    run = lambda: solve_backward(T, G, ctx, a.eta, preconditioner=a.precond, tol=1e-12)
+    ms, res = _time(run, a.reps)
+    it = res["iterations"]
+    bytes_ = a.n * a.m * 8.0 * (it + 3)
+    gbs = bytes_ / (ms / 1e3) / 1e9
+    peak, kind = _peak()
+    return {"case": "backward", "n": a.n, "m": a.m, "eta": a.eta, "preconditioner": a.precond,
+            "pcg_iterations": it, "ms_per_solve": ms, "algorithmic_GBps": gbs,
+            "peak_GBps": peak, "peak_kind": kind, "frac": gbs / peak}
+
+
+def main(argv=None):
+    p = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    p.add_argument("case", choices=["bcd", "splr", "backward"])
+    p.add_argument("--n", type=int, default=8192)
+    p.add_argument("--m", type=int, default=8192)
+    p.add_argument("--d", type=int, default=16)
+    p.add_argument("--eta", type=float, default=0.01)
+    p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    p.add_argument("--iters", type=int, default=100, help="bcd: fixed iteration count")
+    p.add_argument("--density", type=float, default=None, help="splr: density_max kwarg")
+    p.add_argument("--solver", default=None, choices=[None, "auto", "dense", "peel", "sparse"])
+    p.add_argument("--tol", type=float, default=1e-8)
+    p.add_argument("--precond", default="diag", choices=["none", "diag", "splr"])
+    p.add_argument("--reps", type=int, default=3)
+    p.add_argument("--seed", type=int, default=7)
+    a = p.parse_args(argv)
+    res = {"bcd": case_bcd, "splr": case_splr, "backward": case_backward}[a.case](a)
+    print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()
