@@ -97,6 +97,8 @@ SIGNATURES = {
     "cg_version": [],
     "cg_launch_count": [],
     "cg_launch_count_reset": [],
+    "cg_memory_pool": [c_int, c_void_pp],
+    "cg_memory_pool_trim": [c_int, c_size_t],
     "cg_bcd_f64": [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_double, c_int,
                    c_int, c_int_p, c_void_p, c_void_p, c_void_p],
     "cg_bcd_f64_noalloc": [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_double,

@@ -44,6 +44,13 @@ int sm_count_current();
 // Kernel launches issued by this library (graph replays count their kernels).
 void count_launch(long long k = 1);
 
+// Stream-ordered allocation from the library's own memory pool on the current
+// device (created on first use; it keeps freed memory mapped for reuse instead
+// of returning it to the driver at every synchronization).  Free with
+// cudaFreeAsync.
+int pool_alloc_async(void** ptr, size_t bytes, cudaStream_t stream);
+int library_pool(int device, cudaMemPool_t* out);
+
 // Warp reductions: the result is valid in lane 0 (shfl_down tree, a fixed
 // association order, so results are bitwise reproducible).
 __device__ __forceinline__ double warp_sum_down(double v) {

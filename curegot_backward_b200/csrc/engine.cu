@@ -184,7 +184,7 @@ int bcd_admit(cg_engine_s* E, Req* q, cudaStream_t st) {
   const int n = r.n, m = r.m;
   const size_t es = r.m_f32 ? 4 : 8;
   BcdProb& P = q->prob;
-  CG_TRY_CUDA(cudaMallocAsync(&q->block, q->footprint, st));
+  CG_TRY(pool_alloc_async(&q->block, q->footprint, st));
   char* p = static_cast<char*>(q->block);
   auto take = [&](size_t bytes) {
     char* x = p;
@@ -242,7 +242,11 @@ int bcd_admit(cg_engine_s* E, Req* q, cudaStream_t st) {
 void bcd_loop(cg_engine_s* E) {
   cudaSetDevice(E->device);
   cudaStream_t st;
-  cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  // lowest priority: the batch passes are throughput work that fills every
+  // SM; the latency-bound SPLR kernels of the workers go first
+  int prio_lo = 0, prio_hi = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+  cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio_lo);
   cudaEvent_t ev0, ev1;
   cudaEventCreate(&ev0);
   cudaEventCreate(&ev1);
@@ -337,12 +341,12 @@ void bcd_loop(cg_engine_s* E) {
       if ((size_t)P > cap_probs) {
         if (d_probs) cudaFreeAsync(d_probs, st);
         cap_probs = std::max<size_t>(P, 2 * cap_probs);
-        cudaMallocAsync(&d_probs, cap_probs * sizeof(BcdProb), st);
+        pool_alloc_async(reinterpret_cast<void**>(&d_probs), cap_probs * sizeof(BcdProb), st);
       }
       if (h_map.size() > cap_map) {
         if (d_map) cudaFreeAsync(d_map, st);
         cap_map = std::max<size_t>(h_map.size(), 2 * cap_map);
-        cudaMallocAsync(&d_map, cap_map * sizeof(int), st);
+        pool_alloc_async(reinterpret_cast<void**>(&d_map), cap_map * sizeof(int), st);
       }
       cudaMemcpyAsync(d_probs, h_probs.data(), P * sizeof(BcdProb), cudaMemcpyHostToDevice, st);
       cudaMemcpyAsync(d_map, h_map.data(), h_map.size() * sizeof(int), cudaMemcpyHostToDevice,
@@ -373,7 +377,7 @@ void bcd_loop(cg_engine_s* E) {
         cap_states = std::max<size_t>(P, 2 * cap_states);
         cudaHostAlloc(reinterpret_cast<void**>(&h_states), cap_states * sizeof(BcdState),
                       cudaHostAllocDefault);
-        cudaMallocAsync(&d_states, cap_states * sizeof(BcdState), st);
+        pool_alloc_async(reinterpret_cast<void**>(&d_states), cap_states * sizeof(BcdState), st);
       }
       dirty = false;
     }
@@ -461,7 +465,9 @@ void bcd_loop(cg_engine_s* E) {
 void splr_loop(cg_engine_s* E) {
   cudaSetDevice(E->device);
   cudaStream_t st;
-  cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  int prio_lo = 0, prio_hi = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+  cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio_hi);
   while (true) {
     Req* q = nullptr;
     {
@@ -495,7 +501,7 @@ void splr_loop(cg_engine_s* E) {
     const double *da = r.a, *db = r.b;
     double* ddual = nullptr;
     const size_t inb = r.host_inputs ? align256((size_t)n * m * es) + align256(8 * (size_t)(n + m)) : 0;
-    if (cudaMallocAsync(&blk, inb + align256(8 * (size_t)(n + m)), st) != cudaSuccess) {
+    if (pool_alloc_async(&blk, inb + align256(8 * (size_t)(n + m)), st) != CG_OK) {
       rc = CG_ERR_OOM;
     } else {
       char* p = static_cast<char*>(blk);

@@ -15,6 +15,13 @@
 //   the result is deterministic), one CTA per Schur row assembles the core
 //   Schur complement, cuSOLVER potrf factors it.  The solve is a forward
 //   sweep over the rounds, potrs on the core, and a backward sweep.
+// Small cores (kc <= kSmallCore): the whole factorization and solve run in
+//   ONE single-CTA kernel -- pivots and forward values in the same rounds,
+//   the core Schur complement assembled and Cholesky-factored in shared
+//   memory, the triangular solves and the backward sweep -- instead of ~6
+//   launches with cuSOLVER calls that cost tens of microseconds each at
+//   these sizes.  The factor L is also written out for later solves
+//   (backward-context applies).
 #include <algorithm>
 #include <cmath>
 
@@ -26,6 +33,7 @@ namespace {
 
 constexpr int kMaxPeelRounds = 512;
 constexpr int kPeelThreads = 1024;
+constexpr int kSmallCore = 128;  // in-shared-memory Cholesky up to 128 x 128
 
 struct PeelPtrs {
   const int *order, *rptr, *diagq, *cptr, *child, *childq, *par, *parq;
@@ -160,8 +168,219 @@ __global__ void __launch_bounds__(kPeelThreads) peel_backward_kernel(
   }
 }
 
+// ---- small-core path: everything in one CTA --------------------------------
+// Forward values of the peeled rounds and the core (pivots d already known).
+__device__ void dev_forward(const double* __restrict__ val, const PeelPtrs& p, int rounds,
+                            const double* __restrict__ d, const double* __restrict__ rhs,
+                            int nrhs, int H, double* __restrict__ y) {
+  for (int r = 0; r <= rounds; ++r) {
+    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
+      const int v = p.order[idx];
+      for (int c = 0; c < nrhs; ++c) {
+        const double* yc = y + (size_t)c * H;
+        double yv = rhs[(size_t)c * H + v];
+        for (int q = p.cptr[v]; q < p.cptr[v + 1]; ++q) {
+          const int ch = p.child[q];
+          yv -= (val[p.childq[q]] / d[ch]) * yc[ch];
+        }
+        y[(size_t)c * H + v] = yv;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Core right-hand side reduced to the Schur side, into z[c * kc + t].
+__device__ void dev_core_rhs(const double* __restrict__ val, const PeelPtrs& p,
+                             const double* __restrict__ d, const double* __restrict__ y,
+                             int nrhs, int H, int kc, double* __restrict__ z) {
+  for (int t = threadIdx.x; t < kc; t += blockDim.x) {
+    const int s = p.snodes[t];
+    for (int c = 0; c < nrhs; ++c) {
+      const double* yc = y + (size_t)c * H;
+      double acc = yc[s];
+      for (int q = p.sptr[t]; q < p.sptr[t + 1]; ++q) {
+        const int ev = p.enodes[p.sadj[q]];
+        acc -= (val[p.sq[q]] / d[ev]) * yc[ev];
+      }
+      z[(size_t)c * kc + t] = acc;
+    }
+  }
+  __syncthreads();
+}
+
+// z <- (L L^T)^{-1} z for nrhs columns; L lower, row-major kc x kc (shared).
+__device__ void dev_trisolve(const double* __restrict__ L, int kc, double* __restrict__ z,
+                             int nrhs) {
+  for (int j = 0; j < kc; ++j) {
+    if ((int)threadIdx.x < nrhs) z[threadIdx.x * kc + j] /= L[j * kc + j];
+    __syncthreads();
+    const int w = kc - j - 1;
+    for (int e = threadIdx.x; e < nrhs * w; e += blockDim.x) {
+      const int c = e / w, i = j + 1 + (e - c * w);
+      z[c * kc + i] -= L[i * kc + j] * z[c * kc + j];
+    }
+    __syncthreads();
+  }
+  for (int j = kc - 1; j >= 0; --j) {
+    if ((int)threadIdx.x < nrhs) z[threadIdx.x * kc + j] /= L[j * kc + j];
+    __syncthreads();
+    for (int e = threadIdx.x; e < nrhs * j; e += blockDim.x) {
+      const int c = e / j, i = e - c * j;
+      z[c * kc + i] -= L[j * kc + i] * z[c * kc + j];
+    }
+    __syncthreads();
+  }
+}
+
+// Core back-substitution from the Schur-side solution zc, then the backward
+// sweep over the peeled rounds.
+__device__ void dev_backward(const double* __restrict__ val, const PeelPtrs& p, int rounds,
+                             const double* __restrict__ d, const double* __restrict__ y,
+                             const double* __restrict__ zc, int nrhs, int H, int kc, int ke,
+                             double* __restrict__ x) {
+  for (int t = threadIdx.x; t < kc; t += blockDim.x)
+    for (int c = 0; c < nrhs; ++c) x[(size_t)c * H + p.snodes[t]] = zc[(size_t)c * kc + t];
+  for (int e = threadIdx.x; e < ke; e += blockDim.x) {
+    const int ev = p.enodes[e];
+    for (int c = 0; c < nrhs; ++c) {
+      double acc = y[(size_t)c * H + ev];
+      for (int q = p.eptr[e]; q < p.eptr[e + 1]; ++q)
+        acc -= val[p.eq[q]] * zc[(size_t)c * kc + p.eadj[q]];
+      x[(size_t)c * H + ev] = acc / d[ev];
+    }
+  }
+  __syncthreads();
+  for (int r = rounds - 1; r >= 0; --r) {
+    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
+      const int v = p.order[idx];
+      const int u = p.par[v];
+      for (int c = 0; c < nrhs; ++c) {
+        double xv = y[(size_t)c * H + v];
+        if (u >= 0) xv -= val[p.parq[v]] * x[(size_t)c * H + u];
+        x[(size_t)c * H + v] = xv / d[v];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Factorization (pivots d, core factor L -> Lout) and, for nrhs > 0, the
+// solve x = A^{-1} rhs.  Dynamic shared memory: kc*kc + 2*kc doubles.
+__global__ void __launch_bounds__(kPeelThreads) peel_fused_kernel(
+    const double* __restrict__ val, PeelPtrs p, int rounds, int kc, int ke, int H,
+    const double* __restrict__ rhs, int nrhs, double* __restrict__ x, double* __restrict__ d,
+    double* __restrict__ y, double* __restrict__ Lout, int* __restrict__ info) {
+  extern __shared__ double sm[];
+  double* S = sm;
+  double* z = sm + (size_t)kc * kc;
+  // pivots and forward values, round by round (core last)
+  for (int r = 0; r <= rounds; ++r) {
+    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
+      const int v = p.order[idx];
+      double dv = val[p.diagq[v]];
+      double y0 = nrhs > 0 ? rhs[v] : 0.0, y1 = nrhs > 1 ? rhs[(size_t)H + v] : 0.0;
+      for (int q = p.cptr[v]; q < p.cptr[v + 1]; ++q) {
+        const int ch = p.child[q];
+        const double a = val[p.childq[q]];
+        const double w = a / d[ch];
+        dv -= w * a;
+        if (nrhs > 0) y0 -= w * y[ch];
+        if (nrhs > 1) y1 -= w * y[(size_t)H + ch];
+      }
+      d[v] = dv;
+      if (nrhs > 0) y[v] = y0;
+      if (nrhs > 1) y[(size_t)H + v] = y1;
+      if (!(dv > 0.0) || !isfinite(dv)) info[1] = 1;
+    }
+    __syncthreads();
+  }
+  if (kc > 0) {
+    // core Schur complement, one warp per row (same order as the multi-CTA path)
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int t = warp; t < kc; t += nw) {
+      double* Sr = S + (size_t)t * kc;
+      for (int c = lane; c < kc; c += 32) Sr[c] = 0.0;
+      __syncwarp();
+      if (lane == 0) Sr[t] = d[p.snodes[t]];
+      __syncwarp();
+      for (int q = p.sptr[t]; q < p.sptr[t + 1]; ++q) {
+        const int e = p.sadj[q];
+        const double w = val[p.sq[q]] / d[p.enodes[e]];
+        for (int q2 = p.eptr[e] + lane; q2 < p.eptr[e + 1]; q2 += 32)
+          Sr[p.eadj[q2]] -= w * val[p.eq[q2]];
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    // right-looking Cholesky of the lower triangle
+    for (int j = 0; j < kc; ++j) {
+      if (threadIdx.x == 0) {
+        double dj = S[j * kc + j];
+        if (!(dj > 0.0) || !isfinite(dj)) {
+          info[0] = j + 1;
+          dj = 1.0;
+        }
+        S[j * kc + j] = sqrt(dj);
+      }
+      __syncthreads();
+      const double ljj = S[j * kc + j];
+      for (int i = j + 1 + threadIdx.x; i < kc; i += blockDim.x) S[i * kc + j] = S[i * kc + j] / ljj;
+      __syncthreads();
+      const int w = kc - j - 1;
+      for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+        const int ii = e / w, kk = e - ii * w;
+        if (kk <= ii) {
+          const int i = j + 1 + ii, k = j + 1 + kk;
+          S[i * kc + k] -= S[i * kc + j] * S[k * kc + j];
+        }
+      }
+      __syncthreads();
+    }
+    for (int e = threadIdx.x; e < kc * kc; e += blockDim.x) Lout[e] = S[e];
+  }
+  if (nrhs == 0) return;
+  if (kc > 0) {
+    dev_core_rhs(val, p, d, y, nrhs, H, kc, z);
+    dev_trisolve(S, kc, z, nrhs);
+  }
+  dev_backward(val, p, rounds, d, y, z, nrhs, H, kc, ke, x);
+}
+
+// Solve with a stored small-core factor (pivots d, L in global memory).
+__global__ void __launch_bounds__(kPeelThreads) peel_small_solve_kernel(
+    const double* __restrict__ val, PeelPtrs p, int rounds, int kc, int ke, int H,
+    const double* __restrict__ rhs, int nrhs, double* __restrict__ x,
+    const double* __restrict__ d, double* __restrict__ y, const double* __restrict__ Lin) {
+  extern __shared__ double sm[];
+  double* S = sm;
+  double* z = sm + (size_t)kc * kc;
+  for (int e = threadIdx.x; e < kc * kc; e += blockDim.x) S[e] = Lin[e];
+  dev_forward(val, p, rounds, d, rhs, nrhs, H, y);  // its round barriers also publish S
+  if (kc > 0) {
+    dev_core_rhs(val, p, d, y, nrhs, H, kc, z);
+    dev_trisolve(S, kc, z, nrhs);
+  }
+  dev_backward(val, p, rounds, d, y, z, nrhs, H, kc, ke, x);
+}
+
+size_t small_smem(int kc) { return ((size_t)kc * kc + 2 * (size_t)std::max(kc, 1)) * sizeof(double); }
+
+int ensure_small_smem() {
+  static thread_local int done_dev = -1;
+  int dev = 0;
+  CG_TRY_CUDA(cudaGetDevice(&dev));
+  if (done_dev == dev) return CG_OK;
+  const int bytes = (int)small_smem(kSmallCore);
+  CG_TRY_CUDA(cudaFuncSetAttribute(peel_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  CG_TRY_CUDA(cudaFuncSetAttribute(peel_small_solve_kernel,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  done_dev = dev;
+  return CG_OK;
+}
+
 int alloc_dev(PeelFactor& P, void** ptr, size_t bytes) {
-  if (P.stream_ordered) CG_TRY_CUDA(cudaMallocAsync(ptr, bytes, P.alloc_stream));
+  if (P.stream_ordered) CG_TRY(pool_alloc_async(ptr, bytes, P.alloc_stream));
   else CG_TRY_CUDA(cudaMalloc(ptr, bytes));
   return CG_OK;
 }
@@ -370,7 +589,7 @@ int peel_plan(PeelFactor& P, const SpHess& A, cudaStream_t st) {
 int peel_upload(PeelFactor& P, cusolverDnHandle_t h, cudaStream_t st) {
   const int H = P.H, kc = P.kc;
   int lwork = 0;
-  if (kc > 0 &&
+  if (kc > kSmallCore &&
       cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, kc, nullptr, kc, &lwork) !=
           CUSOLVER_STATUS_SUCCESS) {
     set_last_error("cusolverDnDpotrf_bufferSize failed", __FILE__, __LINE__);
@@ -411,6 +630,7 @@ int peel_factor(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, cudaStream
   }
   const PeelPtrs pp = ptrs_of(P);
   CG_TRY_CUDA(cudaMemsetAsync(P.info, 0, 3 * sizeof(int), st));
+  if (P.kc <= kSmallCore) return peel_factor_solve(P, A, h, nullptr, nullptr, 0, st);
   { peel_factor_kernel<<<1, kPeelThreads, 0, st>>>(A.val, pp, P.rounds, P.d, P.info); count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
   if (P.kc > 0) {
@@ -435,6 +655,13 @@ int peel_solve(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, const doubl
                double* x, int nrhs, cudaStream_t st) {
   if (nrhs < 1 || nrhs > 2) return CG_ERR_INVALID_ARG;
   const PeelPtrs pp = ptrs_of(P);
+  if (P.kc <= kSmallCore) {
+    CG_TRY(ensure_small_smem());
+    { peel_small_solve_kernel<<<1, kPeelThreads, small_smem(P.kc), st>>>(
+        A.val, pp, P.rounds, P.kc, P.ke, P.H, rhs, nrhs, x, P.d, P.y, P.S); count_launch(); }
+    CG_TRY_CUDA(cudaGetLastError());
+    return CG_OK;
+  }
   { peel_forward_kernel<<<1, kPeelThreads, 0, st>>>(A.val, pp, P.rounds, P.d, rhs, nrhs, P.H,
                                                     P.kc, P.y, P.rs); count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
@@ -448,6 +675,26 @@ int peel_solve(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, const doubl
   }
   { peel_backward_kernel<<<1, kPeelThreads, 0, st>>>(A.val, pp, P.rounds, P.d, P.y, P.rs, nrhs,
                                                      P.H, P.kc, P.ke, x); count_launch(); }
+  CG_TRY_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
+int peel_factor_solve(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, const double* rhs,
+                      double* x, int nrhs, cudaStream_t st) {
+  if (!P.ready) {
+    set_last_error("peel factor: no plan for the current pattern", __FILE__, __LINE__);
+    return CG_ERR_INVALID_ARG;
+  }
+  if (nrhs < 0 || nrhs > 2) return CG_ERR_INVALID_ARG;
+  if (P.kc > kSmallCore) {
+    CG_TRY(peel_factor(P, A, h, st));
+    return nrhs > 0 ? peel_solve(P, A, h, rhs, x, nrhs, st) : CG_OK;
+  }
+  CG_TRY(ensure_small_smem());
+  const PeelPtrs pp = ptrs_of(P);
+  CG_TRY_CUDA(cudaMemsetAsync(P.info, 0, 3 * sizeof(int), st));
+  { peel_fused_kernel<<<1, kPeelThreads, small_smem(P.kc), st>>>(
+      A.val, pp, P.rounds, P.kc, P.ke, P.H, rhs, nrhs, x, P.d, P.y, P.S, P.info); count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
   return CG_OK;
 }

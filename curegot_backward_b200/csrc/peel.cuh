@@ -60,6 +60,10 @@ int peel_factor(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, cudaStream
 // Device-side status of the last factorization: copy of info[0..1] (async;
 // non-zero = not positive definite).
 int peel_info_async(const PeelFactor& P, int* host2, cudaStream_t st);
+// Factorization followed by x = A^{-1} rhs (nrhs 0..2; 0 = factor only).  For
+// small cores this is a single kernel launch.
+int peel_factor_solve(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, const double* rhs,
+                      double* x, int nrhs, cudaStream_t st);
 // x = A^{-1} rhs for nrhs <= 2 column-major right-hand sides (leading dim H).
 int peel_solve(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, const double* rhs,
                double* x, int nrhs, cudaStream_t st);

@@ -26,6 +26,49 @@ std::atomic<long long> g_launches{0};
 
 void count_launch(long long k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 
+namespace {
+constexpr int kMaxPoolDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[kMaxPoolDevices] = {};
+}  // namespace
+
+int library_pool(int device, cudaMemPool_t* out) {
+  if (device < 0 || device >= kMaxPoolDevices) {
+    set_last_error("memory pool: device ordinal above 63", __FILE__, __LINE__);
+    return CG_ERR_INVALID_ARG;
+  }
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pools[device]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    CG_TRY_CUDA(cudaMemPoolCreate(&pool, &props));
+    // keep freed blocks mapped: serving reuses the same sizes over and over
+    unsigned long long keep = ~0ull;
+    CG_TRY_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    g_pools[device] = pool;
+  }
+  *out = g_pools[device];
+  return CG_OK;
+}
+
+int pool_alloc_async(void** ptr, size_t bytes, cudaStream_t stream) {
+  int dev = 0;
+  CG_TRY_CUDA(cudaGetDevice(&dev));
+  cudaMemPool_t pool = nullptr;
+  CG_TRY(library_pool(dev, &pool));
+  const cudaError_t e = cudaMallocFromPoolAsync(ptr, bytes, pool, stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
+    return (e == cudaErrorMemoryAllocation) ? CG_ERR_OOM : CG_ERR_CUDA;
+  }
+  return CG_OK;
+}
+
 void set_last_error(const char* msg, const char* file, int line) {
   g_last_error = std::string(msg) + " (" + file + ":" + std::to_string(line) + ")";
 }
@@ -358,6 +401,21 @@ const char* cg_last_error(void) { return cg::g_last_error.c_str(); }
 const char* cg_version(void) { return "curegot_b200 0.1.0 (sm_100a)"; }
 
 long long cg_launch_count(void) { return cg::g_launches.load(); }
+
+int cg_memory_pool(int device, void** pool) {
+  if (!pool) return CG_ERR_INVALID_ARG;
+  cudaMemPool_t p = nullptr;
+  CG_TRY(cg::library_pool(device, &p));
+  *pool = reinterpret_cast<void*>(p);
+  return CG_OK;
+}
+
+int cg_memory_pool_trim(int device, size_t keep_bytes) {
+  cudaMemPool_t p = nullptr;
+  CG_TRY(cg::library_pool(device, &p));
+  CG_TRY_CUDA(cudaMemPoolTrimTo(p, keep_bytes));
+  return CG_OK;
+}
 
 void cg_launch_count_reset(void) { cg::g_launches.store(0); }
 

@@ -135,7 +135,7 @@ void count_factor(int H, const std::vector<int>& rp, const std::vector<int>& col
 
 namespace {
 int dev_alloc(SparseChol& C, void** p, size_t bytes) {
-  if (C.stream_ordered) CG_TRY_CUDA(cudaMallocAsync(p, bytes, C.alloc_stream));
+  if (C.stream_ordered) CG_TRY(pool_alloc_async(p, bytes, C.alloc_stream));
   else CG_TRY_CUDA(cudaMalloc(p, bytes));
   return CG_OK;
 }

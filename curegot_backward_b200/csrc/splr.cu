@@ -398,7 +398,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
   if (owned_by_ctx) {
     CG_TRY_CUDA(cudaMalloc(&hbase, hbytes));
   } else {
-    CG_TRY_CUDA(cudaMallocAsync(&hbase, hbytes, st));
+    CG_TRY(pool_alloc_async(&hbase, hbytes, st));
   }
   HBlock hb;
   hblock_carve(hbase, n, m, Kmax, k, big_alpha, lwork, hb);
@@ -629,9 +629,16 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     if (path == kPathPeel) return peel_factor(*pf, hb.A, sol, st);
     return schur_factor(sol, hb.A, hb.F, st);
   };
-  auto solve_direction = [&](const double* rhs, double* x, int nrhs) -> int {
+  // factorization and solve together (one kernel on the small-core peel path)
+  auto factor_solve_direction = [&](int* sp_bad, const double* rhs, double* x,
+                                    int nrhs) -> int {
+    CG_TRY(prepare_direction());
+    if (path == kPathPeel) {
+      *sp_bad = 0;
+      return peel_factor_solve(*pf, hb.A, sol, rhs, x, nrhs, st);
+    }
+    CG_TRY(factor_direction(sp_bad));
     if (path == kPathSparse) return spchol_solve(*sc, rhs, x, nrhs, st);
-    if (path == kPathPeel) return peel_solve(*pf, hb.A, sol, rhs, x, nrhs, st);
     return schur_solve(sol, hb.A, hb.F, rhs, x, nrhs, hb.tmp, st);
   };
   // queue the device status of the last factorization into info2[0..1]
@@ -687,9 +694,8 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     // search direction (sinkhorn_splr.cu:538-649)
     CG_TRY_CUDA(cudaMemcpyAsync(hb.rhs2, grad, H * sizeof(double), cudaMemcpyDeviceToDevice, st));
     int sp_bad = 0;
-    CG_TRY(factor_direction(&sp_bad));
     const int nrhs = (iter > 0) ? 2 : 1;
-    CG_TRY(solve_direction(hb.rhs2, hb.sol2, nrhs));
+    CG_TRY(factor_solve_direction(&sp_bad, hb.rhs2, hb.sol2, nrhs));
     g_last_dir = path;
     { woodbury_kernel<<<1, 1024, 0, st>>>(hb.sol2, hb.sol2 + H, grad, hb.rhs2 + H, hb.s, H, reg, 1,
                                         hb.dres); cg::count_launch(); }

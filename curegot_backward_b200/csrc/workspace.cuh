@@ -1,4 +1,4 @@
-// Stream-ordered workspace: one cudaMallocAsync block carved into
+// Stream-ordered workspace: one block from the library pool carved into
 // 256-byte-aligned pieces, released with cudaFreeAsync on the same stream.
 #pragma once
 
@@ -28,7 +28,7 @@ class Workspace {
   }
   int allocate() {
     if (size_ == 0) return CG_OK;
-    CG_TRY_CUDA(cudaMallocAsync(&base_, size_, stream_));
+    CG_TRY(pool_alloc_async(&base_, size_, stream_));
     return CG_OK;
   }
   template <typename T>

@@ -47,6 +47,15 @@ const char* cg_version(void);
 long long cg_launch_count(void);
 void cg_launch_count_reset(void);
 
+/* The library's stream-ordered memory pool on `device` (a cudaMemPool_t),
+ * created on first use.  Solver workspaces come from it; it keeps freed
+ * blocks mapped (release threshold = max) so repeated solves of similar sizes
+ * reuse memory without remapping.  cg_memory_pool_trim releases unused memory
+ * above keep_bytes back to the driver.  No reference counterpart (the
+ * reference calls cudaMalloc/cudaFree inside its loops). */
+int cg_memory_pool(int device, void** pool);
+int cg_memory_pool_trim(int device, size_t keep_bytes);
+
 /* ------------------------------------------------------------------------ */
 /* Sinkhorn block-coordinate descent (log-domain Sinkhorn).                  */
 /* ------------------------------------------------------------------------ */

@@ -110,6 +110,7 @@ def dirsolver():
 @pytest.mark.parametrize("n,m,reg,kind,dens", [(120, 90, 0.05, "gauss", None),
                                                (90, 150, 0.01, "gauss", None),
                                                (64, 64, 0.01, "gauss", 0.1),
+                                               (300, 260, 0.02, "gauss", 0.1),
                                                (45, 2, 0.05, "uniform", None)])
 def test_direction_solvers_match_oracle(cuda_dev, dirsolver, mode, n, m, reg, kind, dens):
     # every direction-solve path is an exact A^{-1}[g, y]: same bar as the

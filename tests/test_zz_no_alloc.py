@@ -63,14 +63,26 @@ def test_two_calls_in_a_row_match_allocating_entry(cuda_dev):
 
 
 class _PoolProbe:
-    """High-water mark of the device's default stream-ordered memory pool."""
+    """High-water mark of a stream-ordered memory pool (driver API)."""
 
-    def __init__(self, ordinal):
+    def __init__(self, pool):
         self.cu = ctypes.CDLL("libcuda.so.1")
+        self.pool = pool
+
+    @classmethod
+    def default_pool(cls, ordinal):
+        cu = ctypes.CDLL("libcuda.so.1")
         dev = ctypes.c_int()
-        assert self.cu.cuDeviceGet(ctypes.byref(dev), ordinal) == 0
-        self.pool = ctypes.c_void_p()
-        assert self.cu.cuDeviceGetDefaultMemPool(ctypes.byref(self.pool), dev) == 0
+        assert cu.cuDeviceGet(ctypes.byref(dev), ordinal) == 0
+        pool = ctypes.c_void_p()
+        assert cu.cuDeviceGetDefaultMemPool(ctypes.byref(pool), dev) == 0
+        return cls(pool)
+
+    @classmethod
+    def library_pool(cls, ordinal):
+        pool = ctypes.c_void_p()
+        _native.call("cg_memory_pool", ordinal, ctypes.byref(pool))
+        return cls(pool)
 
     def reset(self):
         zero = ctypes.c_uint64(0)
@@ -86,19 +98,23 @@ class _PoolProbe:
 
 def test_no_pool_allocation(cuda_dev):
     M, a, b = _problem(700, 900, 13)
-    probe = _PoolProbe(cuda_dev.index or 0)
-    # the probe sees the allocating entry point's workspace ...
-    torch.cuda.synchronize(cuda_dev)
-    probe.reset()
-    base = probe.high()
-    _solve("cg_bcd_f64", M, a, b, 0.05, 1e-8, 2000, cuda_dev)
-    assert probe.high() > base
-    # ... and nothing from the allocation-free one
-    torch.cuda.synchronize(cuda_dev)
-    probe.reset()
-    base = probe.high()
-    _solve("cg_bcd_f64_noalloc", M, a, b, 0.05, 1e-8, 2000, cuda_dev)
-    assert probe.high() == base
+    ordinal = cuda_dev.index or 0
+    probes = [_PoolProbe.library_pool(ordinal), _PoolProbe.default_pool(ordinal)]
+
+    def highs_after(fn):
+        torch.cuda.synchronize(cuda_dev)
+        for p in probes:
+            p.reset()
+        base = [p.high() for p in probes]
+        _solve(fn, M, a, b, 0.05, 1e-8, 2000, cuda_dev)
+        return base, [p.high() for p in probes]
+
+    # the probe sees the allocating entry point's workspace (library pool) ...
+    base, after = highs_after("cg_bcd_f64")
+    assert after[0] > base[0]
+    # ... and nothing from the allocation-free one, in either pool
+    base, after = highs_after("cg_bcd_f64_noalloc")
+    assert after == base
 
 
 def test_rejects_sizes_above_the_scratch_limit(cuda_dev):
