@@ -61,6 +61,13 @@ tests = _namespace("tests", "Test functions.", {
 
 CuregotError = _native.CuregotError
 
+def set_bcd_cluster_path(enabled: bool = True) -> None:
+    """Enable (default) or disable the cluster-resident Sinkhorn solver for
+    problems whose cost matrix fits one thread-block cluster's shared memory;
+    disabled, every problem uses the multi-CTA row/column passes."""
+    _native.call("cg_bcd_set_cluster_path", 1 if enabled else 0)
+
+
 _DIRSOLVE = {"auto": 0, "dense": 1, "sparse": 2, "peel": 3}
 
 

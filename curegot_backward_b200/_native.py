@@ -103,6 +103,7 @@ SIGNATURES = {
                    c_int, c_int_p, c_void_p, c_void_p, c_void_p],
     "cg_bcd_f64_noalloc": [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_double,
                            c_int, c_int, c_int_p, c_void_p, c_void_p, c_void_p],
+    "cg_bcd_set_cluster_path": [c_int],
     "cg_bcd_mixed": [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_double, c_int,
                      c_int, c_int_p, c_void_p, c_void_p, c_void_p],
     "cg_transport_plan_f64": [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_int,

@@ -456,8 +456,7 @@ int backward_solve(const double* T, const double* G, cg_ctx_s* ctx, double eta, 
   }
   CG_TRY_CUDA(cudaGetLastError());
   PcgState hs{};
-  CG_TRY_CUDA(cudaMemcpyAsync(&hs, A.st, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
-  CG_TRY_CUDA(cudaStreamSynchronize(st));
+  CG_TRY(read_device(&hs, A.st, sizeof(PcgState), st));
   if (!hs.allzero && splr) {
     // z = B^{-1} r, p = z, rz = r.z
     CG_TRY(ctx_apply_full(ctx, A.r, A.z, st));
@@ -475,8 +474,7 @@ int backward_solve(const double* T, const double* G, cg_ctx_s* ctx, double eta, 
         }
       }
       CG_TRY_CUDA(cudaGetLastError());
-      CG_TRY_CUDA(cudaMemcpyAsync(&hs, A.st, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
-      CG_TRY_CUDA(cudaStreamSynchronize(st));
+      CG_TRY(read_device(&hs, A.st, sizeof(PcgState), st));
       chunk = std::min(chunk * 2, 64);
     }
   }

@@ -30,99 +30,11 @@
 #include <algorithm>
 
 #include "bcd.cuh"
+#include "lse.cuh"
 
 namespace cg {
 
 namespace {
-constexpr int kUnroll = 4;
-
-// (max, sum) merge in base 2
-__device__ __forceinline__ void lse2_merge(double& mx, double& s, double mx2, double s2,
-                                           const double* tab) {
-  if (s2 == 0.0) return;
-  if (s == 0.0) {
-    mx = mx2;
-    s = s2;
-    return;
-  }
-  if (mx2 > mx) {
-    s = s * exp2_f64(mx - mx2, tab) + s2;
-    mx = mx2;
-  } else {
-    s += s2 * exp2_f64(mx2 - mx, tab);
-  }
-}
-
-// Accumulate K exponents (valid ones only) into the running (mx, s).
-template <bool FAST, int K>
-__device__ __forceinline__ void lse_chunk(const double (&d)[K], const bool (&ok)[K], double& mx,
-                                          double& s, const double* tab) {
-  double cmax = kNegInf;
-#pragma unroll
-  for (int q = 0; q < K; ++q)
-    if (ok[q]) cmax = fmax(cmax, d[q]);
-  if (cmax > mx) {
-    if (s != 0.0) s *= exp2_f64(mx - cmax, tab);
-    mx = cmax;
-  }
-  if (FAST) {
-    float acc = 0.0f;
-#pragma unroll
-    for (int q = 0; q < K; ++q)
-      if (ok[q]) acc += exp2_neg_mixed(d[q] - mx);
-    s += static_cast<double>(acc);
-  } else {
-#pragma unroll
-    for (int q = 0; q < K; ++q)
-      if (ok[q]) s += exp2_neg_f64(d[q] - mx, tab);
-  }
-}
-
-// Same, for a chunk known to be fully in range (no predicates).
-template <bool FAST, int K>
-__device__ __forceinline__ void lse_chunk_full(const double (&d)[K], double& mx, double& s,
-                                               const double* tab) {
-  double cmax = d[0];
-#pragma unroll
-  for (int q = 1; q < K; ++q) cmax = fmax(cmax, d[q]);
-  if (cmax > mx) {
-    if (s != 0.0) s *= exp2_f64(mx - cmax, tab);
-    mx = cmax;
-  }
-  if (FAST) {
-    float acc = 0.0f;
-#pragma unroll
-    for (int q = 0; q < K; ++q) acc += exp2_neg_mixed(d[q] - mx);
-    s += static_cast<double>(acc);
-  } else {
-    double acc = 0.0;
-#pragma unroll
-    for (int q = 0; q < K; ++q) acc += exp2_neg_f64(d[q] - mx, tab);
-    s += acc;
-  }
-}
-
-template <typename TM>
-struct Raw;  // raw 16-byte vector of M
-template <>
-struct Raw<double> {
-  using T = double2;
-  __device__ __forceinline__ static T load(const double* p) {
-    return __ldg(reinterpret_cast<const double2*>(p));
-  }
-  __device__ __forceinline__ static double get(const T& v, int k) { return k == 0 ? v.x : v.y; }
-};
-template <>
-struct Raw<float> {
-  using T = float4;
-  __device__ __forceinline__ static T load(const float* p) {
-    return __ldg(reinterpret_cast<const float4*>(p));
-  }
-  __device__ __forceinline__ static double get(const T& v, int k) {
-    return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
-  }
-};
-
 // Elements per lane per step: 8 (two float4 or four double2 vectors).
 template <typename TM>
 struct RowU {
@@ -238,10 +150,11 @@ __device__ __forceinline__ void cta_stats(double v, bool valid, double* red, dou
 // ---------------------------------------------------------------------------
 // Row pass: alpha^{t+1}_i = eta * (log a_i - LSE_j((beta^t_j - M_ij) / eta))
 // ---------------------------------------------------------------------------
+// One virtual CTA (index vb) of the row pass.
 template <typename TM>
-__global__ void __launch_bounds__(kThreads, 3) bcd_row_kernel(const BcdProb* __restrict__ probs,
-                                                            const int* __restrict__ cta_prob,
-                                                            const int* __restrict__ cta_start) {
+__device__ __forceinline__ void row_block(const BcdProb* __restrict__ probs,
+                                          const int* __restrict__ cta_prob,
+                                          const int* __restrict__ cta_start, int vb) {
   __shared__ double tab[16];
   __shared__ double sm_mx[kWarps], sm_s[kWarps];
   __shared__ double sm_v[kWarps][2];
@@ -249,8 +162,8 @@ __global__ void __launch_bounds__(kThreads, 3) bcd_row_kernel(const BcdProb* __r
   __shared__ double shc[3 * kThreads];
   load_exp2_table(tab);
 
-  const int pidx = cta_prob ? cta_prob[blockIdx.x] : 0;
-  const int cta = cta_prob ? (int)blockIdx.x - cta_start[pidx] : (int)blockIdx.x;
+  const int pidx = cta_prob ? cta_prob[vb] : 0;
+  const int cta = cta_prob ? vb - cta_start[pidx] : vb;
   const BcdProb& P = probs[pidx];
   BcdState* st = P.st;
   if (ldcg(&st->done)) return;
@@ -462,10 +375,11 @@ __device__ __forceinline__ void col_rows(const TM* __restrict__ M, const double*
   }
 }
 
+// One virtual CTA (index vb) of the column pass.
 template <typename TM>
-__global__ void __launch_bounds__(kThreads, 3) bcd_col_kernel(const BcdProb* __restrict__ probs,
-                                                            const int* __restrict__ cta_prob,
-                                                            const int* __restrict__ cta_start) {
+__device__ __forceinline__ void col_block(const BcdProb* __restrict__ probs,
+                                          const int* __restrict__ cta_prob,
+                                          const int* __restrict__ cta_start, int vb) {
   constexpr int VN = Vec<TM>::N;
   constexpr int W = 32 * VN;
   constexpr int G = kThreads / W;  // merge groups per column
@@ -476,8 +390,8 @@ __global__ void __launch_bounds__(kThreads, 3) bcd_col_kernel(const BcdProb* __r
   __shared__ double shc[3 * kThreads];
   load_exp2_table(tab);
 
-  const int pidx = cta_prob ? cta_prob[blockIdx.x] : 0;
-  const int cta = cta_prob ? (int)blockIdx.x - cta_start[pidx] : (int)blockIdx.x;
+  const int pidx = cta_prob ? cta_prob[vb] : 0;
+  const int cta = cta_prob ? vb - cta_start[pidx] : vb;
   const BcdProb& P = probs[pidx];
   BcdState* st = P.st;
   if (ldcg(&st->done)) return;
@@ -607,6 +521,41 @@ __global__ void __launch_bounds__(kThreads, 3) bcd_col_kernel(const BcdProb* __r
   }
 }
 
+// The passes run as grid-stride loops over virtual CTAs: a launch with fewer
+// CTAs than virtual blocks (the serving engine caps its batch launches) does
+// the same work, in the same per-block order, leaving SM slots free for
+// latency-bound kernels on other streams.
+// LOOP = false: one virtual CTA per CTA (uncapped launches).
+template <typename TM, bool LOOP>
+__global__ void __launch_bounds__(kThreads, 3) bcd_row_kernel(const BcdProb* __restrict__ probs,
+                                                            const int* __restrict__ cta_prob,
+                                                            const int* __restrict__ cta_start,
+                                                            int total) {
+  if (!LOOP) {
+    row_block<TM>(probs, cta_prob, cta_start, (int)blockIdx.x);
+    return;
+  }
+  for (int vb = blockIdx.x; vb < total; vb += gridDim.x) {
+    row_block<TM>(probs, cta_prob, cta_start, vb);
+    __syncthreads();
+  }
+}
+
+template <typename TM, bool LOOP>
+__global__ void __launch_bounds__(kThreads, 3) bcd_col_kernel(const BcdProb* __restrict__ probs,
+                                                            const int* __restrict__ cta_prob,
+                                                            const int* __restrict__ cta_start,
+                                                            int total) {
+  if (!LOOP) {
+    col_block<TM>(probs, cta_prob, cta_start, (int)blockIdx.x);
+    return;
+  }
+  for (int vb = blockIdx.x; vb < total; vb += gridDim.x) {
+    col_block<TM>(probs, cta_prob, cta_start, vb);
+    __syncthreads();
+  }
+}
+
 // P = exp((alpha_i + beta_j - M_ij) / eta)
 template <typename TM>
 __global__ void plan_kernel(const TM* __restrict__ M, const double* __restrict__ alpha,
@@ -622,18 +571,30 @@ __global__ void plan_kernel(const TM* __restrict__ M, const double* __restrict__
 }
 
 void launch_bcd_row(bool f32, const BcdProb* d_probs, const int* d_cta_prob,
-                    const int* d_cta_start, int total_ctas, cudaStream_t stream) {
-  if (f32)
-    { bcd_row_kernel<float><<<total_ctas, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start); cg::count_launch(); }
+                    const int* d_cta_start, int total_ctas, cudaStream_t stream, int grid_cap) {
+  const bool loop = grid_cap > 0 && grid_cap < total_ctas;
+  const int grid = loop ? grid_cap : total_ctas;
+  if (f32 && loop)
+    { bcd_row_kernel<float, true><<<grid, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas); cg::count_launch(); }
+  else if (f32)
+    { bcd_row_kernel<float, false><<<grid, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas); cg::count_launch(); }
+  else if (loop)
+    { bcd_row_kernel<double, true><<<grid, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas); cg::count_launch(); }
   else
-    { bcd_row_kernel<double><<<total_ctas, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start); cg::count_launch(); }
+    { bcd_row_kernel<double, false><<<grid, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas); cg::count_launch(); }
 }
 void launch_bcd_col(bool f32, const BcdProb* d_probs, const int* d_cta_prob,
-                    const int* d_cta_start, int total_ctas, cudaStream_t stream) {
-  if (f32)
-    { bcd_col_kernel<float><<<total_ctas, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start); cg::count_launch(); }
+                    const int* d_cta_start, int total_ctas, cudaStream_t stream, int grid_cap) {
+  const bool loop = grid_cap > 0 && grid_cap < total_ctas;
+  const int grid = loop ? grid_cap : total_ctas;
+  if (f32 && loop)
+    { bcd_col_kernel<float, true><<<grid, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas); cg::count_launch(); }
+  else if (f32)
+    { bcd_col_kernel<float, false><<<grid, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas); cg::count_launch(); }
+  else if (loop)
+    { bcd_col_kernel<double, true><<<grid, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas); cg::count_launch(); }
   else
-    { bcd_col_kernel<double><<<total_ctas, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start); cg::count_launch(); }
+    { bcd_col_kernel<double, false><<<grid, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas); cg::count_launch(); }
 }
 template <typename TM>
 void launch_plan(const TM* M, const double* alpha, const double* beta, double* P,

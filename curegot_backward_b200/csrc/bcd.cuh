@@ -53,16 +53,45 @@ struct BcdProb {
   BcdState* st;
 };
 
+// total_ctas virtual CTAs; grid_cap > 0 limits the launched grid (the
+// kernels loop over the virtual CTAs), 0 launches one CTA per virtual CTA.
 void launch_bcd_row(bool f32, const BcdProb* d_probs, const int* d_cta_prob,
-                    const int* d_cta_start, int total_ctas, cudaStream_t stream);
+                    const int* d_cta_start, int total_ctas, cudaStream_t stream,
+                    int grid_cap = 0);
 void launch_bcd_col(bool f32, const BcdProb* d_probs, const int* d_cta_prob,
-                    const int* d_cta_start, int total_ctas, cudaStream_t stream);
+                    const int* d_cta_start, int total_ctas, cudaStream_t stream,
+                    int grid_cap = 0);
 template <typename TM>
 void launch_plan(const TM* M, const double* alpha, const double* beta, double* P,
                  double inv_eta, int n, int m, cudaStream_t stream);
 
 // Launch geometry for one problem.
 void bcd_geometry(int n, int m, int elem_bytes, int sm_count, BcdProb& p);
+
+// One problem of the cluster-resident solver (bcd_cluster.cu): a whole
+// solve in one launch for cost matrices that fit one cluster's shared memory.
+struct ClusterProb {
+  const void* M;        // row-major n x m, float or double (fixed per launch)
+  const double* a;
+  const double* b;
+  const double* x0;     // nullable [alpha; beta]
+  double* dual;         // nullable output [alpha; beta] of iterate niter
+  BcdState* st;         // output: niter, last_err, fast_iters, ...
+  int n, m, max_iter;
+  double eta, s2, tol;
+};
+
+// Cluster size (1..16) for an n x m problem when the cluster path is enabled
+// and the problem fits, else 0.
+template <typename TM>
+int bcd_cluster_eligible(int n, int m);
+int bcd_cluster_plan(int n, int m, int elem_bytes, int max_c);
+bool bcd_cluster_enabled();
+// Largest cluster size the current device runs this solver with (0: none).
+int bcd_cluster_max(bool f32);
+// Launch `nprob` problems (cluster size C each) on one stream.
+template <typename TM>
+int launch_bcd_cluster(const ClusterProb* d_probs, int nprob, int C, cudaStream_t st);
 
 
 }  // namespace cg

@@ -51,6 +51,13 @@ void count_launch(long long k = 1);
 int pool_alloc_async(void** ptr, size_t bytes, cudaStream_t stream);
 int library_pool(int device, cudaMemPool_t* out);
 
+// Device-to-host reads of small solver state through a thread-local pinned
+// buffer (a pageable destination would take the driver's staged-copy path,
+// which serializes concurrent solver threads).  Both copies are queued on
+// `st`, then the stream is synchronized once.  bytes1 + bytes2 <= 4096.
+int read_device(void* host1, const void* dev1, size_t bytes1, cudaStream_t st,
+                void* host2 = nullptr, const void* dev2 = nullptr, size_t bytes2 = 0);
+
 // Warp reductions: the result is valid in lane 0 (shfl_down tree, a fixed
 // association order, so results are bitwise reproducible).
 __device__ __forceinline__ double warp_sum_down(double v) {

@@ -10,6 +10,10 @@
 //     and replayed; finished problems exit their CTAs immediately and are
 //     retired at the next chunk boundary, when queued requests are admitted
 //     into the freed slots.  Duals and solver state stay on the device.
+//   * Two batches run side by side on their own streams: requests with at
+//     most 8 MB of M, and the larger ones.  A tick of the small batch takes
+//     tens of microseconds, so small requests are not held back by the tick
+//     length of the large problems.
 //   * SPLR requests run on worker threads, each with its own stream, so their
 //     device work overlaps the Sinkhorn batch.
 //   * Admission is by HBM footprint: a request enters only while the sum of
@@ -40,6 +44,9 @@ double now_s() {
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// Sinkhorn requests with at most this many bytes of M share the small batch.
+constexpr size_t kSmallBatchBytes = size_t(8) << 20;
+
 struct Req {
   cg_request_t r;
   uint64_t id = 0;
@@ -58,6 +65,7 @@ struct Req {
   double* ddual = nullptr;
   BcdProb prob{};
   int slot = -1;
+  int cls = 0;  // Sinkhorn batch: 0 small, 1 large
 };
 
 size_t bcd_footprint(const cg_request_t& r, BcdProb& geo, int sms) {
@@ -145,7 +153,9 @@ struct cg_engine_s {
   std::condition_variable cv;
   bool stop = false;
   uint64_t next_id = 1;
-  std::deque<cg::Req*> bcd_q, splr_q;
+  std::deque<cg::Req*> bcd_qs[2], splr_q;  // Sinkhorn batches: small, large
+  int n_workers = 0;
+  std::mutex stat_mu;  // guards the statistics below (two batch threads)
   std::vector<cg::Req*> done;
   std::vector<std::thread> threads;
   std::atomic<long long> active_bcd{0}, active_splr{0};
@@ -239,7 +249,9 @@ int bcd_admit(cg_engine_s* E, Req* q, cudaStream_t st) {
 }
 
 // The Sinkhorn batch scheduler.
-void bcd_loop(cg_engine_s* E) {
+void bcd_loop(cg_engine_s* E, int cls) {
+  std::deque<Req*>& bq = E->bcd_qs[cls];
+  long long my_active = 0;
   cudaSetDevice(E->device);
   cudaStream_t st;
   // lowest priority: the batch passes are throughput work that fills every
@@ -271,22 +283,22 @@ void bcd_loop(cg_engine_s* E) {
     {
       std::unique_lock<std::mutex> lk(E->mu);
       if (active.empty())
-        E->cv.wait(lk, [&] { return E->stop || !E->bcd_q.empty(); });
+        E->cv.wait(lk, [&] { return E->stop || !bq.empty(); });
       if (E->stop && active.empty()) break;
-      while (!E->stop && !E->bcd_q.empty() && (int)active.size() < E->max_batch) {
-        Req* q = E->bcd_q.front();
+      while (!E->stop && !bq.empty() && (int)active.size() < E->max_batch) {
+        Req* q = bq.front();
         if (!active.empty() && (q->r.m_f32 != 0) != batch_f32) break;
         if (!try_reserve(E, q->footprint)) {
           if (!active.empty() || E->in_use > 0) break;
           // larger than the whole budget: reject
-          E->bcd_q.pop_front();
+          bq.pop_front();
           q->status = CG_ERR_ADMISSION;
           lk.unlock();
           finish(E, q);
           lk.lock();
           continue;
         }
-        E->bcd_q.pop_front();
+        bq.pop_front();
         lk.unlock();
         q->t_admit = now_s();
         if (active.empty()) batch_f32 = q->r.m_f32 != 0;
@@ -301,7 +313,8 @@ void bcd_loop(cg_engine_s* E) {
           continue;
         }
         active.push_back(q);
-        E->active_bcd = (long long)active.size();
+        E->active_bcd += (long long)active.size() - my_active;
+        my_active = (long long)active.size();
         dirty = true;
       }
     }
@@ -361,8 +374,10 @@ void bcd_loop(cg_engine_s* E) {
         const int* dcp = drs + P;
         const int* dcs = dcp + col_total;
         for (int c = 0; c < E->chunk; ++c) {
-          launch_bcd_row(batch_f32, d_probs, drp, drs, row_total, st);
-          launch_bcd_col(batch_f32, d_probs, dcp, dcs, col_total, st);
+          // at most 2 of the 3 resident CTA slots per SM: the third stays
+          // free for the latency-bound SPLR kernels of the worker streams
+          launch_bcd_row(batch_f32, d_probs, drp, drs, row_total, st, 2 * E->sms);
+          launch_bcd_col(batch_f32, d_probs, dcp, dcs, col_total, st, 2 * E->sms);
         }
         count_launch(-2LL * E->chunk);  // captured, not executed
         if (cudaStreamEndCapture(st, &g) == cudaSuccess) {
@@ -370,7 +385,10 @@ void bcd_loop(cg_engine_s* E) {
           cudaGraphDestroy(g);
         }
       }
-      E->graph_builds++;
+      {
+        std::lock_guard<std::mutex> sl(E->stat_mu);
+        E->graph_builds++;
+      }
       if ((size_t)P > cap_states) {
         if (h_states) cudaFreeHost(h_states);
         if (d_states) cudaFreeAsync(d_states, st);
@@ -404,6 +422,7 @@ void bcd_loop(cg_engine_s* E) {
     cudaStreamSynchronize(st);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ev0, ev1);
+    std::unique_lock<std::mutex> stat_lk(E->stat_mu);
     E->gpu_ms_bcd += ms;
     E->chunks++;
     // algorithmic bytes: problems still running at the chunk start stream
@@ -414,6 +433,7 @@ void bcd_loop(cg_engine_s* E) {
       E->bytes_bcd += ran * 2.0 * q->r.n * (double)q->r.m * (q->r.m_f32 ? 4 : 8);
       active[k]->niter = h_states[k].iter;
     }
+    stat_lk.unlock();
     // ---- retire finished problems -----------------------------------------
     std::vector<Req*> keep;
     for (int k = 0; k < P; ++k) {
@@ -448,7 +468,8 @@ void bcd_loop(cg_engine_s* E) {
         finish(E, q);
       }
       active.swap(keep);
-      E->active_bcd = (long long)active.size();
+      E->active_bcd += (long long)active.size() - my_active;
+      my_active = (long long)active.size();
     }
   }
   if (gexec) cudaGraphExecDestroy(gexec);
@@ -472,16 +493,17 @@ void splr_loop(cg_engine_s* E) {
     Req* q = nullptr;
     {
       std::unique_lock<std::mutex> lk(E->mu);
-      E->cv.wait(lk, [&] {
-        if (E->stop) return true;
-        if (E->splr_q.empty()) return false;
-        Req* f = E->splr_q.front();
+      auto ready = [&](std::deque<Req*>& dq) {
+        if (dq.empty()) return false;
+        Req* f = dq.front();
         return f->footprint > E->budget || E->in_use + f->footprint <= E->budget;
-      });
+      };
+      E->cv.wait(lk, [&] { return E->stop || ready(E->splr_q); });
       if (E->stop) break;
-      if (E->splr_q.empty()) continue;
-      q = E->splr_q.front();
-      E->splr_q.pop_front();
+      std::deque<Req*>& dq = E->splr_q;
+      if (dq.empty()) continue;
+      q = dq.front();
+      dq.pop_front();
       if (q->footprint > E->budget) {
         q->status = CG_ERR_ADMISSION;
         lk.unlock();
@@ -558,7 +580,9 @@ int cg_engine_create(size_t budget_bytes, int max_batch, int splr_workers, int c
   E->max_batch = max_batch;
   E->chunk = chunk > 0 ? chunk : 8;
   E->sms = cg::sm_count_current();
-  E->threads.emplace_back(cg::bcd_loop, E);
+  E->threads.emplace_back(cg::bcd_loop, E, 0);
+  E->threads.emplace_back(cg::bcd_loop, E, 1);
+  E->n_workers = splr_workers;
   for (int w = 0; w < splr_workers; ++w) E->threads.emplace_back(cg::splr_loop, E);
   *out = reinterpret_cast<cg_engine*>(E);
   return CG_OK;
@@ -574,6 +598,7 @@ int cg_engine_submit(cg_engine* eng, const cg_request_t* req, uint64_t* id) {
   q->t_submit = cg::now_s();
   if (req->algo == CG_ALGO_BCD) {
     q->footprint = cg::bcd_footprint(q->r, q->prob, E->sms);
+    q->cls = ((size_t)req->n * req->m * (req->m_f32 ? 4 : 8) > cg::kSmallBatchBytes) ? 1 : 0;
   } else {
     if (req->m < 2) {
       delete q;
@@ -584,7 +609,7 @@ int cg_engine_submit(cg_engine* eng, const cg_request_t* req, uint64_t* id) {
   {
     std::lock_guard<std::mutex> lk(E->mu);
     q->id = E->next_id++;
-    if (req->algo == CG_ALGO_BCD) E->bcd_q.push_back(q);
+    if (req->algo == CG_ALGO_BCD) E->bcd_qs[q->cls].push_back(q);
     else E->splr_q.push_back(q);
   }
   E->cv.notify_all();
@@ -625,7 +650,7 @@ int cg_engine_stats(cg_engine* eng, cg_engine_stats_t* out) {
   std::lock_guard<std::mutex> lk(E->mu);
   out->in_use_bytes = E->in_use;
   out->budget_bytes = E->budget;
-  out->queued = (long long)(E->bcd_q.size() + E->splr_q.size());
+  out->queued = (long long)(E->bcd_qs[0].size() + E->bcd_qs[1].size() + E->splr_q.size());
   out->active_bcd = E->active_bcd;
   out->active_splr = E->active_splr;
   out->completed = E->n_done;
@@ -648,7 +673,8 @@ int cg_engine_destroy(cg_engine* eng) {
   E->cv.notify_all();
   for (auto& t : E->threads) t.join();
   for (auto* q : E->done) delete q;
-  for (auto* q : E->bcd_q) delete q;
+  for (auto* q : E->bcd_qs[0]) delete q;
+  for (auto* q : E->bcd_qs[1]) delete q;
   for (auto* q : E->splr_q) delete q;
   delete E;
   return CG_OK;

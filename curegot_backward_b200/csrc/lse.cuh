@@ -1,0 +1,99 @@
+// Base-2 log-sum-exp building blocks shared by the Sinkhorn kernels: online
+// (max, sum) accumulation over chunks of exponents, the pairwise merge of two
+// partial (max, sum) pairs, and raw 16-byte vector loads of M.
+#pragma once
+
+#include "common.cuh"
+
+namespace cg {
+
+constexpr int kUnroll = 4;
+
+// (max, sum) merge in base 2
+__device__ __forceinline__ void lse2_merge(double& mx, double& s, double mx2, double s2,
+                                           const double* tab) {
+  if (s2 == 0.0) return;
+  if (s == 0.0) {
+    mx = mx2;
+    s = s2;
+    return;
+  }
+  if (mx2 > mx) {
+    s = s * exp2_f64(mx - mx2, tab) + s2;
+    mx = mx2;
+  } else {
+    s += s2 * exp2_f64(mx2 - mx, tab);
+  }
+}
+
+// Accumulate K exponents (valid ones only) into the running (mx, s).
+template <bool FAST, int K>
+__device__ __forceinline__ void lse_chunk(const double (&d)[K], const bool (&ok)[K], double& mx,
+                                          double& s, const double* tab) {
+  double cmax = kNegInf;
+#pragma unroll
+  for (int q = 0; q < K; ++q)
+    if (ok[q]) cmax = fmax(cmax, d[q]);
+  if (cmax > mx) {
+    if (s != 0.0) s *= exp2_f64(mx - cmax, tab);
+    mx = cmax;
+  }
+  if (FAST) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int q = 0; q < K; ++q)
+      if (ok[q]) acc += exp2_neg_mixed(d[q] - mx);
+    s += static_cast<double>(acc);
+  } else {
+#pragma unroll
+    for (int q = 0; q < K; ++q)
+      if (ok[q]) s += exp2_neg_f64(d[q] - mx, tab);
+  }
+}
+
+// Same, for a chunk known to be fully in range (no predicates).
+template <bool FAST, int K>
+__device__ __forceinline__ void lse_chunk_full(const double (&d)[K], double& mx, double& s,
+                                               const double* tab) {
+  double cmax = d[0];
+#pragma unroll
+  for (int q = 1; q < K; ++q) cmax = fmax(cmax, d[q]);
+  if (cmax > mx) {
+    if (s != 0.0) s *= exp2_f64(mx - cmax, tab);
+    mx = cmax;
+  }
+  if (FAST) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int q = 0; q < K; ++q) acc += exp2_neg_mixed(d[q] - mx);
+    s += static_cast<double>(acc);
+  } else {
+    double acc = 0.0;
+#pragma unroll
+    for (int q = 0; q < K; ++q) acc += exp2_neg_f64(d[q] - mx, tab);
+    s += acc;
+  }
+}
+
+template <typename TM>
+struct Raw;  // raw 16-byte vector of M
+template <>
+struct Raw<double> {
+  using T = double2;
+  __device__ __forceinline__ static T load(const double* p) {
+    return __ldg(reinterpret_cast<const double2*>(p));
+  }
+  __device__ __forceinline__ static double get(const T& v, int k) { return k == 0 ? v.x : v.y; }
+};
+template <>
+struct Raw<float> {
+  using T = float4;
+  __device__ __forceinline__ static T load(const float* p) {
+    return __ldg(reinterpret_cast<const float4*>(p));
+  }
+  __device__ __forceinline__ static double get(const T& v, int k) {
+    return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
+  }
+};
+
+}  // namespace cg

@@ -69,6 +69,30 @@ int pool_alloc_async(void** ptr, size_t bytes, cudaStream_t stream) {
   return CG_OK;
 }
 
+int read_device(void* host1, const void* dev1, size_t bytes1, cudaStream_t st, void* host2,
+                const void* dev2, size_t bytes2) {
+  struct Pinned {
+    void* p = nullptr;
+    ~Pinned() {
+      if (p) cudaFreeHost(p);
+    }
+  };
+  thread_local Pinned buf;
+  constexpr size_t kBytes = 4096;
+  if (bytes1 + bytes2 > kBytes) {
+    set_last_error("read_device: more than 4096 bytes", __FILE__, __LINE__);
+    return CG_ERR_INVALID_ARG;
+  }
+  if (!buf.p) CG_TRY_CUDA(cudaHostAlloc(&buf.p, kBytes, cudaHostAllocDefault));
+  char* pin = static_cast<char*>(buf.p);
+  if (bytes1) CG_TRY_CUDA(cudaMemcpyAsync(pin, dev1, bytes1, cudaMemcpyDeviceToHost, st));
+  if (bytes2) CG_TRY_CUDA(cudaMemcpyAsync(pin + bytes1, dev2, bytes2, cudaMemcpyDeviceToHost, st));
+  CG_TRY_CUDA(cudaStreamSynchronize(st));
+  if (bytes1) std::memcpy(host1, pin, bytes1);
+  if (bytes2) std::memcpy(host2, pin + bytes1, bytes2);
+  return CG_OK;
+}
+
 void set_last_error(const char* msg, const char* file, int line) {
   g_last_error = std::string(msg) + " (" + file + ":" + std::to_string(line) + ")";
 }
@@ -139,6 +163,41 @@ __global__ void dual_from_state_kernel(const BcdState* st, const BcdProb* p, dou
     dual[i] = (i < n) ? al[i] : be[i - n];
 }
 
+// Whole solve in one cluster-resident launch (problems up to ~3 MB of M).
+template <typename TM>
+int bcd_solve_cluster(int C, const TM* M, const double* a, const double* b, double* Pout,
+                      double reg, int max_iter, double tol, int n, int m, int* niter,
+                      const double* x0, double* dual, cudaStream_t stream) {
+  Workspace ws(stream);
+  const size_t o_st = ws.reserve<BcdState>(1), o_p = ws.reserve<ClusterProb>(1);
+  const bool tmp_dual = (!dual && Pout);
+  const size_t o_d = ws.reserve<double>(tmp_dual ? (size_t)(n + m) : 1);
+  CG_TRY(ws.allocate());
+  ClusterProb hp{};
+  hp.M = M;
+  hp.a = a;
+  hp.b = b;
+  hp.x0 = x0;
+  hp.dual = dual ? dual : (tmp_dual ? ws.at<double>(o_d) : nullptr);
+  hp.st = ws.at<BcdState>(o_st);
+  hp.n = n;
+  hp.m = m;
+  hp.max_iter = max_iter;
+  hp.eta = reg;
+  hp.s2 = kLog2e / reg;
+  hp.tol = tol;
+  ClusterProb* dp = ws.at<ClusterProb>(o_p);
+  CG_TRY_CUDA(cudaMemcpyAsync(dp, &hp, sizeof(ClusterProb), cudaMemcpyHostToDevice, stream));
+  CG_TRY(launch_bcd_cluster<TM>(dp, 1, C, stream));
+  BcdState hs{};
+  CG_TRY(read_device(&hs, hp.st, sizeof(BcdState), stream));
+  *niter = hs.niter;
+  if (Pout) launch_plan<TM>(M, hp.dual, hp.dual + n, Pout, 1.0 / reg, n, m, stream);
+  CG_TRY_CUDA(cudaGetLastError());
+  ws.release();
+  return CG_OK;
+}
+
 template <typename TM>
 int bcd_solve(const TM* M, const double* a, const double* b, double* Pout, double reg,
               int max_iter, double tol, int n, int m, int* niter, const double* x0,
@@ -147,6 +206,9 @@ int bcd_solve(const TM* M, const double* a, const double* b, double* Pout, doubl
     set_last_error("cg_bcd: invalid argument", __FILE__, __LINE__);
     return CG_ERR_INVALID_ARG;
   }
+  if (const int C = bcd_cluster_eligible<TM>(n, m))
+    return bcd_solve_cluster<TM>(C, M, a, b, Pout, reg, max_iter, tol, n, m, niter, x0, dual,
+                                 stream);
   const int sms = sm_count_current();
   BcdProb hp{};
   bcd_geometry(n, m, (int)sizeof(TM), sms, hp);
@@ -211,8 +273,7 @@ int bcd_solve(const TM* M, const double* a, const double* b, double* Pout, doubl
     }
     queued += todo;
     CG_TRY_CUDA(cudaGetLastError());
-    CG_TRY_CUDA(cudaMemcpyAsync(&hs, hp.st, sizeof(BcdState), cudaMemcpyDeviceToHost, stream));
-    CG_TRY_CUDA(cudaStreamSynchronize(stream));
+    CG_TRY(read_device(&hs, hp.st, sizeof(BcdState), stream));
     if (hs.done || queued >= max_iter) break;
     chunk = std::min(chunk * 2, 64);
   }
@@ -364,8 +425,7 @@ int bcd_solve_noalloc(const double* M, const double* a, const double* b, double*
     }
     queued += todo;
     CG_TRY_CUDA(cudaGetLastError());
-    CG_TRY_CUDA(cudaMemcpyAsync(&hs, hp.st, sizeof(BcdState), cudaMemcpyDeviceToHost, stream));
-    CG_TRY_CUDA(cudaStreamSynchronize(stream));
+    CG_TRY(read_device(&hs, hp.st, sizeof(BcdState), stream));
     if (hs.done || queued >= max_iter) break;
     chunk = std::min(chunk * 2, 64);
   }

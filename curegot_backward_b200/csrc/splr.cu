@@ -201,9 +201,7 @@ __global__ void inv_diag_kernel(const double* val, const int* rowptr, int n, int
 
 template <typename T>
 int read_dev(T* host, const T* dev, cudaStream_t st) {
-  CG_TRY_CUDA(cudaMemcpyAsync(host, dev, sizeof(T), cudaMemcpyDeviceToHost, st));
-  CG_TRY_CUDA(cudaStreamSynchronize(st));
-  return CG_OK;
+  return read_device(host, dev, sizeof(T), st);
 }
 
 // ---------------------------------------------------------------------------
@@ -641,13 +639,17 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     if (path == kPathSparse) return spchol_solve(*sc, rhs, x, nrhs, st);
     return schur_solve(sol, hb.A, hb.F, rhs, x, nrhs, hb.tmp, st);
   };
-  // queue the device status of the last factorization into info2[0..1]
-  auto queue_factor_info = [&](int* info2) -> int {
-    info2[0] = info2[1] = 0;
-    if (path == kPathPeel) return peel_info_async(*pf, info2, st);
-    if (path == kPathDense)
-      CG_TRY_CUDA(cudaMemcpyAsync(info2, hb.F.info, sizeof(int), cudaMemcpyDeviceToHost, st));
-    return CG_OK;
+  // device status of the last factorization (pointer, bytes; none for sparse)
+  auto factor_info_src = [&](const int** src, size_t* bytes) {
+    *src = nullptr;
+    *bytes = 0;
+    if (path == kPathPeel) {
+      *src = pf->info;
+      *bytes = 2 * sizeof(int);
+    } else if (path == kPathDense) {
+      *src = hb.F.info;
+      *bytes = sizeof(int);
+    }
   };
 
   auto dual_sphess = [&](double dens, double sh, bool fixed) -> int {
@@ -701,9 +703,11 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
                                         hb.dres); cg::count_launch(); }
     CG_TRY_CUDA(cudaGetLastError());
     DirRes dr{};
-    int info2[2];
-    CG_TRY(queue_factor_info(info2));
-    CG_TRY(read_dev(&dr, hb.dres, st));
+    int info2[2] = {0, 0};
+    const int* isrc = nullptr;
+    size_t ibytes = 0;
+    factor_info_src(&isrc, &ibytes);
+    CG_TRY(read_device(&dr, hb.dres, sizeof(DirRes), st, info2, isrc, ibytes));
     if (sp_bad || info2[0] != 0 || info2[1] != 0) {
       set_last_error("direction solve: sparsified Hessian not positive definite", __FILE__,
                      __LINE__);
@@ -919,12 +923,13 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     c->dres = hb.dres;
     c->err = hb.err;
     int rp = 0;
-    CG_TRY_CUDA(cudaMemcpyAsync(&rp, hb.A.rowptr + H, sizeof(int), cudaMemcpyDeviceToHost, st));
     CG_TRY_CUDA(cudaMemcpyAsync(c->point, c->fallback ? gamma : gamma_prev, H * sizeof(double),
                                 cudaMemcpyDeviceToDevice, st));
-    int info2[2];
-    CG_TRY(queue_factor_info(info2));
-    CG_TRY_CUDA(cudaStreamSynchronize(st));
+    int info2[2] = {0, 0};
+    const int* isrc = nullptr;
+    size_t ibytes = 0;
+    factor_info_src(&isrc, &ibytes);
+    CG_TRY(read_device(&rp, hb.A.rowptr + H, sizeof(int), st, info2, isrc, ibytes));
     const int info = ctx_sp_bad | info2[0] | info2[1];
     c->nnz = rp;
     c->has_point = true;

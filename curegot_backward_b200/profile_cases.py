@@ -55,6 +55,8 @@ def _time(fn, reps):
 
 
 def case_bcd(a):
+    import curegot_backward_b200 as cg
+    cg.set_bcd_cluster_path(a.path != "multi")
     dev = torch.device("cuda", 0)
     dtype = torch.float32 if a.precision == "mixed" else torch.float64
     M, am, bm = _gauss(a.n, a.m, a.d, a.seed, dev, dtype)
@@ -65,7 +67,7 @@ def case_bcd(a):
     bytes_ = 2.0 * a.n * a.m * M.element_size() * niter
     gbs = bytes_ / (ms / 1e3) / 1e9
     peak, kind = _peak()
-    return {"case": "bcd", "n": a.n, "m": a.m, "precision": a.precision, "eta": a.eta,
+    return {"case": "bcd", "path": a.path, "n": a.n, "m": a.m, "precision": a.precision, "eta": a.eta,
             "iterations": niter, "ms_per_solve": ms, "us_per_iteration": 1e3 * ms / niter,
             "algorithmic_GBps": gbs, "peak_GBps": peak, "peak_kind": kind, "frac": gbs / peak}
 
@@ -114,6 +116,8 @@ def main(argv=None):
     p.add_argument("--eta", type=float, default=0.01)
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     p.add_argument("--iters", type=int, default=100, help="bcd: fixed iteration count")
+    p.add_argument("--path", default="auto", choices=["auto", "multi"],
+                   help="bcd: auto = cluster-resident solver when the problem fits")
     p.add_argument("--density", type=float, default=None, help="splr: density_max kwarg")
     p.add_argument("--solver", default=None, choices=[None, "auto", "dense", "peel", "sparse"])
     p.add_argument("--tol", type=float, default=1e-8)

@@ -100,6 +100,16 @@ int cg_bcd_f64_noalloc(const double* M, const double* a, const double* b, double
                        const double* x0, double* dual, cudaStream_t stream);
 
 /*
+ * Sinkhorn path selection (process-wide; default on).  When enabled,
+ * cg_bcd_f64 / cg_bcd_mixed solve problems whose cost matrix fits the shared
+ * memory of one thread-block cluster (up to 16 CTAs, ~3 MB of M) in a single
+ * cluster-resident launch; larger problems, and all problems when disabled,
+ * use the multi-CTA row/column passes.  Same stopping rule and niter
+ * semantics either way.  No reference counterpart.
+ */
+int cg_bcd_set_cluster_path(int enable);
+
+/*
  * Mixed-precision BCD: M stored in FP32, duals and all reductions in FP64.
  * Same contract as cg_bcd_f64; P (nullable) is written in FP64.  The
  * FP32-M form of cuda_sinkhorn_bcd; the stopping rule is evaluated with the

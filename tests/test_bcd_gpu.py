@@ -149,3 +149,52 @@ def test_matches_reference_gpu_solver(cuda_dev, which):
     assert_close(got, ref)
     # and the oracle agrees with the reference's own solver
     assert_close(oracle.bcd(M, a, b, reg, tol=1e-8, max_iter=2000), ref)
+
+
+@pytest.fixture
+def bcd_path():
+    """Selects the Sinkhorn path for one test; restores the default afterwards."""
+    yield cg.set_bcd_cluster_path
+    cg.set_bcd_cluster_path(True)
+
+
+@pytest.mark.parametrize("path", ["cluster", "multi"])
+@pytest.mark.parametrize("n,m,reg,tol", [
+    (256, 320, 0.05, 1e-8), (17, 1000, 0.05, 1e-8), (1000, 3, 0.05, 1e-8), (3, 5, 0.1, 1e-8),
+    (1, 1, 0.1, 1e-8), (600, 1200, 0.01, 1e-8), (100, 100, 0.01, 1e-10), (33, 31, 0.02, 1e-8),
+])
+def test_paths_match_oracle(cuda_dev, bcd_path, path, n, m, reg, tol):
+    # the cluster-resident solver and the multi-CTA passes meet the same bar
+    bcd_path(path == "cluster")
+    M, a, b = rand_problem(n, m, 7 * n + m)
+    got = cg.numpy.sinkhorn_bcd(M, a, b, reg, tol=tol, max_iter=5000)
+    ref = oracle.bcd(M, a, b, reg, tol=tol, max_iter=5000)
+    assert_close(got, ref)
+
+
+def test_cluster_path_is_one_launch(cuda_dev, bcd_path):
+    # problems of up to 768 KB of M take the cluster-resident path
+    from curegot_backward_b200 import _native
+    bcd_path(True)
+    M, a, b = rand_problem(240, 360, 4)
+    L = _native.lib()
+    l0 = L.cg_launch_count()
+    got = cg.numpy.sinkhorn_bcd(M, a, b, 0.05, tol=1e-8, max_iter=1000)
+    # one cluster launch for the whole solve + the plan kernel
+    assert L.cg_launch_count() - l0 <= 2
+    ref = oracle.bcd(M, a, b, 0.05, tol=1e-8, max_iter=1000)
+    assert_close(got, ref)
+
+
+def test_cluster_path_warm_start_and_truncation(cuda_dev, bcd_path):
+    bcd_path(True)
+    M, a, b = rand_problem(300, 200, 3)
+    r = cg.numpy.sinkhorn_bcd(M, a, b, 0.02, tol=1e-9, max_iter=7)
+    o = oracle.bcd(M, a, b, 0.02, tol=1e-9, max_iter=7)
+    assert r["niter"] == 7 == o["niter"]
+    assert_close(r, o)
+    full = cg.numpy.sinkhorn_bcd(M, a, b, 0.02, tol=1e-9, max_iter=5000)
+    warm = cg.numpy.sinkhorn_bcd(M, a, b, 0.02, tol=1e-9, max_iter=5000, x0=full["dual"])
+    ow = oracle.bcd(M, a, b, 0.02, tol=1e-9, max_iter=5000, x0=full["dual"])
+    assert warm["niter"] == ow["niter"]
+    assert np.abs(warm["plan"] - ow["plan"]).max() <= 1e-12

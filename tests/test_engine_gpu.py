@@ -5,7 +5,6 @@ import pytest
 import torch
 
 import curegot_backward_b200 as cg
-from curegot_backward_b200 import _solvers
 from curegot_backward_b200.serving import OTEngine
 from curegot_backward_b200.synthetic import StreamSpec, stream_problem
 
@@ -25,13 +24,17 @@ def specs():
 
 
 def alone(s, M, a, b):
-    if s.algo == "bcd":
-        _, _, dual = _solvers._bcd_device(M, a, b, s.eta, 1e-8, 100000, None, "mixed",
-                                          want_plan=False)
-        return dual
-    dmax = min(10.0 / min(s.n, s.m), 1.0)
-    return _solvers._splr_device(M, a, b, s.eta, 1e-8, 100000, 0, None, "mixed", dmax, 1e-3, 30,
-                                 3, want_plan=False)["dual"]
+    """The same request through an engine that serves nothing else."""
+    eng = OTEngine(budget_bytes=8e9, max_batch=6, splr_workers=2, chunk=4)
+    try:
+        eng.submit(M, a, b, eta=s.eta, algo=s.algo, tol=1e-8, tag=0)
+        while True:
+            res = eng.poll(wait_ms=100)
+            if res:
+                assert res[0]["status"] == 0
+                return res[0]["dual"].to(M.device)
+    finally:
+        eng.close()
 
 
 @pytest.mark.parametrize("host", [False, True])
