@@ -389,10 +389,12 @@ def main():
     eng = OTEngine(budget_bytes=args.budget_gb * 1e9, max_batch=64, splr_workers=SPLR_WORKERS,
                    chunk=8)
 
-    # warm-up steps (untimed)
+    # warm-up steps (untimed): device inputs, and host inputs for the e2e pass
     for st in range(args.warmup):
         probs = make_step(step_specs(args, st, rank, True), dev)
         run_engine_step(eng, probs, False, 0.0)
+        if not args.no_e2e and st < 2:
+            run_engine_step(eng, to_host_pinned(probs), True, 0.0)
     # timed steps: data generated up front (each step streams far more than L2)
     steps = [make_step(step_specs(args, st, rank, False), dev) for st in range(args.steps)]
     n_req = sum(len(p) for p in steps)

@@ -15,7 +15,8 @@
 //   the result is deterministic), one CTA per Schur row assembles the core
 //   Schur complement, cuSOLVER potrf factors it.  The solve is a forward
 //   sweep over the rounds, potrs on the core, and a backward sweep.
-// Small cores (kc <= kSmallCore): the whole factorization and solve run in
+// Small cores (kc <= kPeelSmallCore = 160, 200 KB of shared memory for the
+//   dense core factor): the whole factorization and solve run in
 //   ONE single-CTA kernel -- pivots and forward values in the same rounds,
 //   the core Schur complement assembled and Cholesky-factored in shared
 //   memory, the triangular solves and the backward sweep -- instead of ~6
@@ -33,12 +34,17 @@ namespace {
 
 constexpr int kMaxPeelRounds = 512;
 constexpr int kPeelThreads = 1024;
-constexpr int kSmallCore = 128;  // in-shared-memory Cholesky up to 128 x 128
+constexpr int kSmallCore = kPeelSmallCore;  // in-shared-memory Cholesky
 
 struct PeelPtrs {
   const int *order, *rptr, *diagq, *cptr, *child, *childq, *par, *parq;
   const int *snodes, *enodes, *sptr, *sadj, *sq, *eptr, *eadj, *eq;
+  // contribution lists of the core Schur complement (entry t * kc + t2):
+  // eliminated node ce, value indices of the edges (t, ce) and (ce, t2)
+  const int *ccp, *ce, *cq1, *cq2;
 };
+
+constexpr int kContribMax = kPeelContribMax;
 
 PeelPtrs ptrs_of(const PeelFactor& P) {
   const int* b = P.ints;
@@ -59,6 +65,10 @@ PeelPtrs ptrs_of(const PeelFactor& P) {
   p.eptr = b + P.off_eptr;
   p.eadj = b + P.off_eadj;
   p.eq = b + P.off_eq;
+  p.ccp = P.contrib ? b + P.off_ccp : nullptr;
+  p.ce = P.contrib ? b + P.off_ce : nullptr;
+  p.cq1 = P.contrib ? b + P.off_cq1 : nullptr;
+  p.cq2 = P.contrib ? b + P.off_cq2 : nullptr;
   return p;
 }
 
@@ -99,6 +109,36 @@ __global__ void peel_assemble_kernel(const double* __restrict__ val, PeelPtrs p,
     for (int q2 = p.eptr[e] + threadIdx.x; q2 < p.eptr[e + 1]; q2 += blockDim.x)
       Sr[p.eadj[q2]] -= w * val[p.eq[q2]];
     __syncthreads();
+  }
+}
+
+// Core Schur complement from the contribution lists: one thread per entry.
+__global__ void peel_contrib_kernel(const double* __restrict__ val, PeelPtrs p,
+                                    const double* __restrict__ d, int kc,
+                                    double* __restrict__ S) {
+  const long long total = (long long)kc * kc;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int t = (int)(idx / kc), t2 = (int)(idx - (long long)t * kc);
+    double acc = (t == t2) ? d[p.snodes[t]] : 0.0;
+    for (int q = p.ccp[idx]; q < p.ccp[idx + 1]; ++q)
+      acc -= (val[p.cq1[q]] / d[p.enodes[p.ce[q]]]) * val[p.cq2[q]];
+    S[idx] = acc;
+  }
+}
+
+// Dense Schur complement of the whole graph from a no-peel plan: the pivots
+// of both sides are A's own diagonal entries.
+__global__ void dense_contrib_kernel(const double* __restrict__ val, PeelPtrs p, int kc,
+                                     double* __restrict__ S) {
+  const long long total = (long long)kc * kc;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int t = (int)(idx / kc), t2 = (int)(idx - (long long)t * kc);
+    double acc = (t == t2) ? val[p.diagq[p.snodes[t]]] : 0.0;
+    for (int q = p.ccp[idx]; q < p.ccp[idx + 1]; ++q)
+      acc -= (val[p.cq1[q]] / val[p.diagq[p.enodes[p.ce[q]]]]) * val[p.cq2[q]];
+    S[idx] = acc;
   }
 }
 
@@ -295,7 +335,17 @@ __global__ void __launch_bounds__(kPeelThreads) peel_fused_kernel(
     }
     __syncthreads();
   }
-  if (kc > 0) {
+  if (kc > 0 && p.ccp != nullptr) {
+    // core Schur complement from the contribution lists, one thread per entry
+    for (int idx = threadIdx.x; idx < kc * kc; idx += blockDim.x) {
+      const int t = idx / kc, t2 = idx - t * kc;
+      double acc = (t == t2) ? d[p.snodes[t]] : 0.0;
+      for (int q = p.ccp[idx]; q < p.ccp[idx + 1]; ++q)
+        acc -= (val[p.cq1[q]] / d[p.enodes[p.ce[q]]]) * val[p.cq2[q]];
+      S[idx] = acc;
+    }
+    __syncthreads();
+  } else if (kc > 0) {
     // core Schur complement, one warp per row (same order as the multi-CTA path)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     for (int t = warp; t < kc; t += nw) {
@@ -313,6 +363,8 @@ __global__ void __launch_bounds__(kPeelThreads) peel_fused_kernel(
       }
     }
     __syncthreads();
+  }
+  if (kc > 0) {
     // right-looking Cholesky of the lower triangle
     for (int j = 0; j < kc; ++j) {
       if (threadIdx.x == 0) {
@@ -400,7 +452,7 @@ void peel_release(PeelFactor& P) {
   P.ready = false;
 }
 
-int peel_plan(PeelFactor& P, const SpHess& A, cudaStream_t st) {
+int peel_plan(PeelFactor& P, const SpHess& A, cudaStream_t st, bool no_peel) {
   const int n = A.n, m = A.m, H = A.H;
   P.ready = false;
   P.n = n;
@@ -451,7 +503,7 @@ int peel_plan(PeelFactor& P, const SpHess& A, cudaStream_t st) {
   std::vector<int> rptr(1, 0);
   std::vector<int> cur, next;
   for (int v = 0; v < H; ++v)
-    if (deg[v] <= 1) cur.push_back(v);
+    if (!no_peel && deg[v] <= 1) cur.push_back(v);
   int rounds = 0;
   while (!cur.empty()) {
     if (rounds >= kMaxPeelRounds) {
@@ -576,6 +628,32 @@ int peel_plan(PeelFactor& P, const SpHess& A, cudaStream_t st) {
   P.off_eptr = put(eptr, ke + 1);
   P.off_eadj = put(eadj, eadj.size());
   P.off_eq = put(eq, eq.size());
+  // contribution lists: every pair of S-neighbours (t, t2) of an eliminated
+  // core node e adds (a_{t,e} / d_e) a_{e,t2} to entry (t, t2); listed per
+  // entry in ascending e, the order of the row-wise assembly
+  P.contrib = kc > 0 && kc <= kContribMax;
+  if (P.contrib) {
+    std::vector<int> ccnt((size_t)kc * kc + 1, 0);
+    for (int e = 0; e < ke; ++e)
+      for (int p1 = eptr[e]; p1 < eptr[e + 1]; ++p1)
+        for (int p2 = eptr[e]; p2 < eptr[e + 1]; ++p2) ccnt[(size_t)eadj[p1] * kc + eadj[p2] + 1]++;
+    for (size_t k2 = 0; k2 < (size_t)kc * kc; ++k2) ccnt[k2 + 1] += ccnt[k2];
+    const size_t nc = (size_t)ccnt[(size_t)kc * kc];
+    std::vector<int> ce(std::max<size_t>(nc, 1)), cq1(std::max<size_t>(nc, 1)), cq2(std::max<size_t>(nc, 1));
+    std::vector<int> fill(ccnt.begin(), ccnt.end() - 1);
+    for (int e = 0; e < ke; ++e)
+      for (int p1 = eptr[e]; p1 < eptr[e + 1]; ++p1)
+        for (int p2 = eptr[e]; p2 < eptr[e + 1]; ++p2) {
+          const int pos = fill[(size_t)eadj[p1] * kc + eadj[p2]]++;
+          ce[pos] = e;
+          cq1[pos] = eq[p1];
+          cq2[pos] = eq[p2];
+        }
+    P.off_ccp = put(ccnt, ccnt.size());
+    P.off_ce = put(ce, nc);
+    P.off_cq1 = put(cq1, nc);
+    P.off_cq2 = put(cq2, nc);
+  }
   P.rounds = rounds;
   P.npeel = npeel;
   P.kc = kc;
@@ -586,10 +664,10 @@ int peel_plan(PeelFactor& P, const SpHess& A, cudaStream_t st) {
   return CG_OK;
 }
 
-int peel_upload(PeelFactor& P, cusolverDnHandle_t h, cudaStream_t st) {
+int peel_upload(PeelFactor& P, cusolverDnHandle_t h, cudaStream_t st, bool plan_only) {
   const int H = P.H, kc = P.kc;
   int lwork = 0;
-  if (kc > kSmallCore &&
+  if (!plan_only && kc > kSmallCore &&
       cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, kc, nullptr, kc, &lwork) !=
           CUSOLVER_STATUS_SUCCESS) {
     set_last_error("cusolverDnDpotrf_bufferSize failed", __FILE__, __LINE__);
@@ -597,7 +675,7 @@ int peel_upload(PeelFactor& P, cusolverDnHandle_t h, cudaStream_t st) {
   }
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   const size_t ib = al(P.h_ints.size() * sizeof(int));
-  const size_t bytes = ib + al((size_t)H * 8) + al((size_t)kc * kc * 8) +
+  const size_t bytes = plan_only ? ib : ib + al((size_t)H * 8) + al((size_t)kc * kc * 8) +
                        al((size_t)std::max(lwork, 1) * 8) + al(3 * sizeof(int)) +
                        al((size_t)2 * H * 8) + al((size_t)2 * std::max(kc, 1) * 8);
   if (bytes > P.block_bytes) {
@@ -609,6 +687,15 @@ int peel_upload(PeelFactor& P, cusolverDnHandle_t h, cudaStream_t st) {
   }
   char* p = static_cast<char*>(P.block);
   P.ints = reinterpret_cast<int*>(p); p += ib;
+  if (plan_only) {
+    P.d = P.S = P.work = P.y = P.rs = nullptr;
+    P.info = nullptr;
+    P.lwork = 0;
+    CG_TRY_CUDA(cudaMemcpyAsync(P.ints, P.h_ints.data(), P.h_ints.size() * sizeof(int),
+                                cudaMemcpyHostToDevice, st));
+    P.ready = true;
+    return CG_OK;
+  }
   P.d = reinterpret_cast<double*>(p); p += al((size_t)H * 8);
   P.S = reinterpret_cast<double*>(p); p += al((size_t)kc * kc * 8);
   P.work = reinterpret_cast<double*>(p); p += al((size_t)std::max(lwork, 1) * 8);
@@ -634,7 +721,13 @@ int peel_factor(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, cudaStream
   { peel_factor_kernel<<<1, kPeelThreads, 0, st>>>(A.val, pp, P.rounds, P.d, P.info); count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
   if (P.kc > 0) {
-    { peel_assemble_kernel<<<P.kc, 256, 0, st>>>(A.val, pp, P.d, P.kc, P.S); count_launch(); }
+    if (P.contrib) {
+      const long long total = (long long)P.kc * P.kc;
+      const int grid = (int)std::min<long long>((total + 255) / 256, 148 * 8);
+      { peel_contrib_kernel<<<grid, 256, 0, st>>>(A.val, pp, P.d, P.kc, P.S); count_launch(); }
+    } else {
+      { peel_assemble_kernel<<<P.kc, 256, 0, st>>>(A.val, pp, P.d, P.kc, P.S); count_launch(); }
+    }
     CG_TRY_CUDA(cudaGetLastError());
     if (cusolverDnSetStream(h, st) != CUSOLVER_STATUS_SUCCESS) return CG_ERR_SOLVER;
     if (cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, P.kc, P.S, P.kc, P.work, P.lwork, P.info) !=
@@ -695,6 +788,19 @@ int peel_factor_solve(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, cons
   CG_TRY_CUDA(cudaMemsetAsync(P.info, 0, 3 * sizeof(int), st));
   { peel_fused_kernel<<<1, kPeelThreads, small_smem(P.kc), st>>>(
       A.val, pp, P.rounds, P.kc, P.ke, P.H, rhs, nrhs, x, P.d, P.y, P.S, P.info); count_launch(); }
+  CG_TRY_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
+int peel_assemble_dense(const PeelFactor& P, const SpHess& A, double* S, int k, cudaStream_t st) {
+  if (!P.ready || !P.contrib || P.rounds != 0 || P.kc != k) {
+    set_last_error("dense Schur assembly: no matching contribution plan", __FILE__, __LINE__);
+    return CG_ERR_INVALID_ARG;
+  }
+  const PeelPtrs pp = ptrs_of(P);
+  const long long total = (long long)k * k;
+  const int grid = (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, 148 * 8));
+  { dense_contrib_kernel<<<grid, 256, 0, st>>>(A.val, pp, k, S); count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
   return CG_OK;
 }

@@ -22,6 +22,12 @@
 
 namespace cg {
 
+// Largest core Schur complement factored in shared memory inside one kernel.
+constexpr int kPeelSmallCore = 160;
+// Largest core Schur complement assembled from host-planned contribution
+// lists (one thread per entry); larger ones use the row-wise assembly.
+constexpr int kPeelContribMax = 1024;
+
 struct PeelFactor {
   int H = 0, n = 0, m = 0;
   int rounds = 0;       // peel rounds (the core is processed as one extra round)
@@ -32,7 +38,9 @@ struct PeelFactor {
   std::vector<int> h_ints;  // every int array below, packed in device order
   size_t off_order = 0, off_rptr = 0, off_diagq = 0, off_cptr = 0, off_child = 0, off_childq = 0,
          off_par = 0, off_parq = 0, off_snodes = 0, off_enodes = 0, off_sptr = 0, off_sadj = 0,
-         off_sq = 0, off_eptr = 0, off_eadj = 0, off_eq = 0;
+         off_sq = 0, off_eptr = 0, off_eadj = 0, off_eq = 0, off_ccp = 0, off_ce = 0, off_cq1 = 0,
+         off_cq2 = 0;
+  bool contrib = false;  // per-entry contribution lists of the core Schur complement
   // device
   void* block = nullptr;
   size_t block_bytes = 0;
@@ -51,9 +59,15 @@ struct PeelFactor {
 
 // Host plan of the current pattern of A (copies the pattern to the host and
 // synchronizes the stream).  Sets rounds, kc, ke; ready stays false.
-int peel_plan(PeelFactor& P, const SpHess& A, cudaStream_t st);
-// Device buffers + upload of the plan.
-int peel_upload(PeelFactor& P, cusolverDnHandle_t h, cudaStream_t st);
+// no_peel = true: no elimination rounds, the core is the whole graph -- the
+// contribution lists of the dense Schur complement (see peel_assemble_dense).
+int peel_plan(PeelFactor& P, const SpHess& A, cudaStream_t st, bool no_peel = false);
+// Device buffers + upload of the plan (plan_only: the integer plan alone).
+int peel_upload(PeelFactor& P, cusolverDnHandle_t h, cudaStream_t st, bool plan_only = false);
+// Dense Schur complement S (k x k, the dense direction-solve path) assembled
+// from a no_peel plan, one thread per entry; same values and summation order
+// as the row-wise assembly of schur.cu.
+int peel_assemble_dense(const PeelFactor& P, const SpHess& A, double* S, int k, cudaStream_t st);
 // Numeric factorization of A's current values (async; a non-positive pivot
 // or a potrf failure lands in info[0] / info[1]).
 int peel_factor(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, cudaStream_t st);

@@ -169,9 +169,12 @@ __global__ void back_kernel(int mode, const double* __restrict__ val, const int*
 
 }  // namespace
 
-int schur_factor(cusolverDnHandle_t h, const SpHess& A, SchurFactor& F, cudaStream_t st) {
+int schur_factor(cusolverDnHandle_t h, const SpHess& A, SchurFactor& F, cudaStream_t st,
+                 bool assembled) {
   if (F.k <= 0) return CG_OK;
-  if (F.big_alpha)
+  if (assembled) {
+    // S assembled by the caller
+  } else if (F.big_alpha)
     { assemble_big_alpha<<<F.k, 256, 0, st>>>(A.val, A.col, A.rowptr, A.ipt, A.ij, A.iv, A.n, F.k,
                                             F.S); cg::count_launch(); }
   else

@@ -28,7 +28,9 @@ int solver_handle(cusolverDnHandle_t* out);
 
 // Assemble S from the CSR / per-row lists of A and factor it (async; the
 // potrf status lands in F.info).
-int schur_factor(cusolverDnHandle_t h, const SpHess& A, SchurFactor& F, cudaStream_t st);
+// assembled = true: F.S already holds the Schur complement (factor only).
+int schur_factor(cusolverDnHandle_t h, const SpHess& A, SchurFactor& F, cudaStream_t st,
+                 bool assembled = false);
 
 // x = A^{-1} rhs for nrhs column-major right-hand sides (leading dim H).
 // tmp: [k * nrhs] scratch.

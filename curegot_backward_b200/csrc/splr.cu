@@ -591,11 +591,25 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
   bool pattern_new = true;
   int path = kPathDense;
   const int dir_mode = g_dir_mode.load();
+  // dense path: the Schur complement is assembled from host-planned
+  // contribution lists when k <= kPeelContribMax (same values and order as
+  // the row-wise assembly, without its serial per-row walk)
+  bool dense_planned = false;
+  auto plan_dense = [&]() -> int {
+    dense_planned = false;
+    if (k <= 0 || k > kPeelContribMax) return CG_OK;
+    CG_TRY(peel_plan(*pf, hb.A, st, /*no_peel=*/true));
+    if (!pf->contrib || pf->kc != k) return CG_OK;
+    CG_TRY(peel_upload(*pf, sol, st, /*plan_only=*/true));
+    dense_planned = true;
+    return CG_OK;
+  };
   auto prepare_direction = [&]() -> int {
     if (!pattern_new) return CG_OK;
     pattern_new = false;
     path = kPathDense;
-    if (dir_mode == kDirDense) return CG_OK;
+    dense_planned = false;
+    if (dir_mode == kDirDense) return plan_dense();
     if (dir_mode == kDirSparse) {
       CG_TRY(spchol_order(*sc, hb.A, kInf, st));
       CG_TRY(spchol_analyze(*sc, st));
@@ -603,14 +617,16 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
       return CG_OK;
     }
     // auto / peel: leaf peeling when its core Schur complement is at most
-    // half the dense one (1/8 of the potrf work), else the dense Schur path
+    // half the dense one (1/8 of the potrf work), or small enough for the
+    // single-kernel in-shared-memory factorization; else the dense Schur path
     CG_TRY(peel_plan(*pf, hb.A, st));
     const bool fits = pf->rounds <= kMaxPeelRoundsUsed;
-    if (fits && (dir_mode == kDirPeel || 2 * pf->kc <= k)) {
+    if (fits && (dir_mode == kDirPeel || 2 * pf->kc <= k || pf->kc <= kPeelSmallCore)) {
       CG_TRY(peel_upload(*pf, sol, st));
       path = kPathPeel;
+      return CG_OK;
     }
-    return CG_OK;
+    return plan_dense();
   };
   // factor A (current values); *bad (host) = 1 when the sparse Cholesky met a
   // non-positive pivot.  The dense and peel paths report on the device
@@ -625,6 +641,10 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
       return CG_OK;
     }
     if (path == kPathPeel) return peel_factor(*pf, hb.A, sol, st);
+    if (dense_planned) {
+      CG_TRY(peel_assemble_dense(*pf, hb.A, hb.F.S, k, st));
+      return schur_factor(sol, hb.A, hb.F, st, /*assembled=*/true);
+    }
     return schur_factor(sol, hb.A, hb.F, st);
   };
   // factorization and solve together (one kernel on the small-core peel path)

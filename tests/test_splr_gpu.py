@@ -218,3 +218,15 @@ def test_splr_mixed_precision(cuda_dev):
     ref = oracle.splr(M32.astype(np.float64), a, b, reg, tol=1e-8, max_iter=500)
     assert got["niter"] == ref["niter"]
     assert np.abs(got["dual"] - ref["dual"]).max() <= 1e-10 * np.abs(ref["dual"]).max()
+
+
+def test_peel_large_core_rowwise_assembly(cuda_dev, dirsolver):
+    # a 2-core larger than the contribution-list limit (1024) uses the
+    # row-wise assembly and cuSOLVER on the core; same bar against the oracle
+    dirsolver("peel")
+    M, a, b = problem(1100, 1060, 21, "gauss")
+    got = cg.numpy.sinkhorn_splr(M, a, b, 0.02, tol=1e-8, max_iter=300, density=0.1)
+    assert cg.last_direction_solver() == "peel"
+    ref = oracle.splr(M, a, b, 0.02, tol=1e-8, max_iter=300, density=0.1)
+    assert got["niter"] == ref["niter"]
+    assert np.abs(got["dual"] - ref["dual"]).max() <= 1e-10 * np.abs(ref["dual"]).max()
