@@ -40,8 +40,9 @@ struct PeelPtrs {
   const int *order, *rptr, *diagq, *cptr, *child, *childq, *par, *parq;
   const int *snodes, *enodes, *sptr, *sadj, *sq, *eptr, *eadj, *eq;
   // contribution lists of the core Schur complement (entry t * kc + t2):
-  // eliminated node ce, value indices of the edges (t, ce) and (ce, t2)
-  const int *ccp, *ce, *cq1, *cq2;
+  // eliminated node ce, E-list position cw of the edge (ce, t) (its weight
+  // W[cw] = a / d_ce), value index cq2 of the edge (ce, t2)
+  const int *ccp, *ce, *cw, *cq2;
 };
 
 constexpr int kContribMax = kPeelContribMax;
@@ -67,7 +68,7 @@ PeelPtrs ptrs_of(const PeelFactor& P) {
   p.eq = b + P.off_eq;
   p.ccp = P.contrib ? b + P.off_ccp : nullptr;
   p.ce = P.contrib ? b + P.off_ce : nullptr;
-  p.cq1 = P.contrib ? b + P.off_cq1 : nullptr;
+  p.cw = P.contrib ? b + P.off_cq1 : nullptr;
   p.cq2 = P.contrib ? b + P.off_cq2 : nullptr;
   return p;
 }
@@ -114,30 +115,40 @@ __global__ void peel_assemble_kernel(const double* __restrict__ val, PeelPtrs p,
 
 // Core Schur complement from the contribution lists: one thread per entry.
 __global__ void peel_contrib_kernel(const double* __restrict__ val, PeelPtrs p,
-                                    const double* __restrict__ d, int kc,
-                                    double* __restrict__ S) {
+                                    const double* __restrict__ d, const double* __restrict__ W,
+                                    int kc, double* __restrict__ S) {
   const long long total = (long long)kc * kc;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
        idx += (long long)gridDim.x * blockDim.x) {
     const int t = (int)(idx / kc), t2 = (int)(idx - (long long)t * kc);
     double acc = (t == t2) ? d[p.snodes[t]] : 0.0;
-    for (int q = p.ccp[idx]; q < p.ccp[idx + 1]; ++q)
-      acc -= (val[p.cq1[q]] / d[p.enodes[p.ce[q]]]) * val[p.cq2[q]];
+    for (int q = p.ccp[idx]; q < p.ccp[idx + 1]; ++q) acc -= W[p.cw[q]] * val[p.cq2[q]];
     S[idx] = acc;
+  }
+}
+
+// Edge weights of the core: W[pos] = a_{e,t} / d_e for every E-list entry
+// (pivots d of the peel path, or A's own diagonal when d == nullptr).
+__global__ void peel_weights_kernel(const double* __restrict__ val, PeelPtrs p,
+                                    const double* __restrict__ d, int ke, double* __restrict__ W) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ke; e += gridDim.x * blockDim.x) {
+    const int ev = p.enodes[e];
+    const double de = d ? d[ev] : val[p.diagq[ev]];
+    for (int q = p.eptr[e]; q < p.eptr[e + 1]; ++q) W[q] = val[p.eq[q]] / de;
   }
 }
 
 // Dense Schur complement of the whole graph from a no-peel plan: the pivots
 // of both sides are A's own diagonal entries.
-__global__ void dense_contrib_kernel(const double* __restrict__ val, PeelPtrs p, int kc,
+__global__ void dense_contrib_kernel(const double* __restrict__ val, PeelPtrs p,
+                                     const double* __restrict__ W, int kc,
                                      double* __restrict__ S) {
   const long long total = (long long)kc * kc;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
        idx += (long long)gridDim.x * blockDim.x) {
     const int t = (int)(idx / kc), t2 = (int)(idx - (long long)t * kc);
     double acc = (t == t2) ? val[p.diagq[p.snodes[t]]] : 0.0;
-    for (int q = p.ccp[idx]; q < p.ccp[idx + 1]; ++q)
-      acc -= (val[p.cq1[q]] / val[p.diagq[p.enodes[p.ce[q]]]]) * val[p.cq2[q]];
+    for (int q = p.ccp[idx]; q < p.ccp[idx + 1]; ++q) acc -= W[p.cw[q]] * val[p.cq2[q]];
     S[idx] = acc;
   }
 }
@@ -310,7 +321,8 @@ __device__ void dev_backward(const double* __restrict__ val, const PeelPtrs& p, 
 __global__ void __launch_bounds__(kPeelThreads) peel_fused_kernel(
     const double* __restrict__ val, PeelPtrs p, int rounds, int kc, int ke, int H,
     const double* __restrict__ rhs, int nrhs, double* __restrict__ x, double* __restrict__ d,
-    double* __restrict__ y, double* __restrict__ Lout, int* __restrict__ info) {
+    double* __restrict__ y, double* __restrict__ Lout, int* __restrict__ info,
+    double* __restrict__ W) {
   extern __shared__ double sm[];
   double* S = sm;
   double* z = sm + (size_t)kc * kc;
@@ -336,12 +348,17 @@ __global__ void __launch_bounds__(kPeelThreads) peel_fused_kernel(
     __syncthreads();
   }
   if (kc > 0 && p.ccp != nullptr) {
-    // core Schur complement from the contribution lists, one thread per entry
+    // edge weights, then the core Schur complement from the contribution
+    // lists, one thread per entry
+    for (int e = threadIdx.x; e < ke; e += blockDim.x) {
+      const double de = d[p.enodes[e]];
+      for (int q = p.eptr[e]; q < p.eptr[e + 1]; ++q) W[q] = val[p.eq[q]] / de;
+    }
+    __syncthreads();
     for (int idx = threadIdx.x; idx < kc * kc; idx += blockDim.x) {
       const int t = idx / kc, t2 = idx - t * kc;
       double acc = (t == t2) ? d[p.snodes[t]] : 0.0;
-      for (int q = p.ccp[idx]; q < p.ccp[idx + 1]; ++q)
-        acc -= (val[p.cq1[q]] / d[p.enodes[p.ce[q]]]) * val[p.cq2[q]];
+      for (int q = p.ccp[idx]; q < p.ccp[idx + 1]; ++q) acc -= W[p.cw[q]] * val[p.cq2[q]];
       S[idx] = acc;
     }
     __syncthreads();
@@ -646,7 +663,7 @@ int peel_plan(PeelFactor& P, const SpHess& A, cudaStream_t st, bool no_peel) {
         for (int p2 = eptr[e]; p2 < eptr[e + 1]; ++p2) {
           const int pos = fill[(size_t)eadj[p1] * kc + eadj[p2]]++;
           ce[pos] = e;
-          cq1[pos] = eq[p1];
+          cq1[pos] = p1;  // E-list position: weight index
           cq2[pos] = eq[p2];
         }
     P.off_ccp = put(ccnt, ccnt.size());
@@ -675,7 +692,8 @@ int peel_upload(PeelFactor& P, cusolverDnHandle_t h, cudaStream_t st, bool plan_
   }
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   const size_t ib = al(P.h_ints.size() * sizeof(int));
-  const size_t bytes = plan_only ? ib : ib + al((size_t)H * 8) + al((size_t)kc * kc * 8) +
+  const size_t wb = al((size_t)std::max<long long>(P.ne_adj, 1) * 8);
+  const size_t bytes = plan_only ? ib + wb : ib + wb + al((size_t)H * 8) + al((size_t)kc * kc * 8) +
                        al((size_t)std::max(lwork, 1) * 8) + al(3 * sizeof(int)) +
                        al((size_t)2 * H * 8) + al((size_t)2 * std::max(kc, 1) * 8);
   if (bytes > P.block_bytes) {
@@ -687,6 +705,7 @@ int peel_upload(PeelFactor& P, cusolverDnHandle_t h, cudaStream_t st, bool plan_
   }
   char* p = static_cast<char*>(P.block);
   P.ints = reinterpret_cast<int*>(p); p += ib;
+  P.W = reinterpret_cast<double*>(p); p += wb;
   if (plan_only) {
     P.d = P.S = P.work = P.y = P.rs = nullptr;
     P.info = nullptr;
@@ -724,7 +743,8 @@ int peel_factor(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, cudaStream
     if (P.contrib) {
       const long long total = (long long)P.kc * P.kc;
       const int grid = (int)std::min<long long>((total + 255) / 256, 148 * 8);
-      { peel_contrib_kernel<<<grid, 256, 0, st>>>(A.val, pp, P.d, P.kc, P.S); count_launch(); }
+      { peel_weights_kernel<<<std::max(1, std::min((P.ke + 255) / 256, 148 * 4)), 256, 0, st>>>(A.val, pp, P.d, P.ke, P.W); count_launch(); }
+      { peel_contrib_kernel<<<grid, 256, 0, st>>>(A.val, pp, P.d, P.W, P.kc, P.S); count_launch(); }
     } else {
       { peel_assemble_kernel<<<P.kc, 256, 0, st>>>(A.val, pp, P.d, P.kc, P.S); count_launch(); }
     }
@@ -787,7 +807,7 @@ int peel_factor_solve(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, cons
   const PeelPtrs pp = ptrs_of(P);
   CG_TRY_CUDA(cudaMemsetAsync(P.info, 0, 3 * sizeof(int), st));
   { peel_fused_kernel<<<1, kPeelThreads, small_smem(P.kc), st>>>(
-      A.val, pp, P.rounds, P.kc, P.ke, P.H, rhs, nrhs, x, P.d, P.y, P.S, P.info); count_launch(); }
+      A.val, pp, P.rounds, P.kc, P.ke, P.H, rhs, nrhs, x, P.d, P.y, P.S, P.info, P.W); count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
   return CG_OK;
 }
@@ -800,7 +820,8 @@ int peel_assemble_dense(const PeelFactor& P, const SpHess& A, double* S, int k, 
   const PeelPtrs pp = ptrs_of(P);
   const long long total = (long long)k * k;
   const int grid = (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, 148 * 8));
-  { dense_contrib_kernel<<<grid, 256, 0, st>>>(A.val, pp, k, S); count_launch(); }
+  { peel_weights_kernel<<<std::max(1, std::min((P.ke + 255) / 256, 148 * 4)), 256, 0, st>>>(A.val, pp, nullptr, P.ke, P.W); count_launch(); }
+  { dense_contrib_kernel<<<grid, 256, 0, st>>>(A.val, pp, P.W, k, S); count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
   return CG_OK;
 }

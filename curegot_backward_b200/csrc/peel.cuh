@@ -52,6 +52,7 @@ struct PeelFactor {
   int* info = nullptr;      // [3] potrf info, pivot check, potrs info
   double* y = nullptr;      // [2H] forward-substitution values
   double* rs = nullptr;     // [2 kc] reduced right-hand sides / Schur solution
+  double* W = nullptr;      // [ne_adj] edge weights a_{e,t} / d_e of the core (E-list order)
   bool ready = false;
   bool stream_ordered = false;
   cudaStream_t alloc_stream = nullptr;
