@@ -32,6 +32,12 @@
 #include "bcd.cuh"
 #include "lse.cuh"
 
+#ifndef CG_BCD_MINB
+#define CG_BCD_MINB 3
+#endif
+// Resident CTAs per SM the row/column passes are compiled for (register cap).
+constexpr int kBcdMinBlocks = CG_BCD_MINB;
+
 namespace cg {
 
 namespace {
@@ -155,7 +161,7 @@ template <typename TM>
 __device__ __forceinline__ void row_block(const BcdProb* __restrict__ probs,
                                           const int* __restrict__ cta_prob,
                                           const int* __restrict__ cta_start, int vb) {
-  __shared__ double tab[16];
+  __shared__ double tab[kExp2TableSize];
   __shared__ double sm_mx[kWarps], sm_s[kWarps];
   __shared__ double sm_v[kWarps][2];
   __shared__ double red[kWarps];
@@ -383,7 +389,7 @@ __device__ __forceinline__ void col_block(const BcdProb* __restrict__ probs,
   constexpr int VN = Vec<TM>::N;
   constexpr int W = 32 * VN;
   constexpr int G = kThreads / W;  // merge groups per column
-  __shared__ double tab[16];
+  __shared__ double tab[kExp2TableSize];
   __shared__ double sm_mx[kWarps][W];
   __shared__ double sm_s[kWarps][W];
   __shared__ double red[kWarps];
@@ -527,7 +533,7 @@ __device__ __forceinline__ void col_block(const BcdProb* __restrict__ probs,
 // latency-bound kernels on other streams.
 // LOOP = false: one virtual CTA per CTA (uncapped launches).
 template <typename TM, bool LOOP>
-__global__ void __launch_bounds__(kThreads, 3) bcd_row_kernel(const BcdProb* __restrict__ probs,
+__global__ void __launch_bounds__(kThreads, kBcdMinBlocks) bcd_row_kernel(const BcdProb* __restrict__ probs,
                                                             const int* __restrict__ cta_prob,
                                                             const int* __restrict__ cta_start,
                                                             int total) {
@@ -542,7 +548,7 @@ __global__ void __launch_bounds__(kThreads, 3) bcd_row_kernel(const BcdProb* __r
 }
 
 template <typename TM, bool LOOP>
-__global__ void __launch_bounds__(kThreads, 3) bcd_col_kernel(const BcdProb* __restrict__ probs,
+__global__ void __launch_bounds__(kThreads, kBcdMinBlocks) bcd_col_kernel(const BcdProb* __restrict__ probs,
                                                             const int* __restrict__ cta_prob,
                                                             const int* __restrict__ cta_start,
                                                             int total) {
@@ -629,12 +635,13 @@ void bcd_geometry(int n, int m, int elem_bytes, int sm_count, BcdProb& p) {
   }
   p.rows_per_cta = R;
   p.row_ctas = (n + R - 1) / R;
-  // Column pass: 512-byte strips; split rows until ~2 CTAs per SM, keeping
-  // at least 256 rows per split (bounds the merge work of the last CTA).
+  // Column pass: 512-byte strips.
   const int W = 32 * vn;
   p.col_strips = (m + W - 1) / W;
-  int splits = (2 * sm_count + p.col_strips - 1) / p.col_strips;
-  splits = std::max(1, std::min(splits, n / 256));
+  // as many row splits as fill one wave of resident CTAs (3 per SM) without
+  // starting a partial second one, at least 128 rows per split
+  int splits = (3 * sm_count) / p.col_strips;
+  splits = std::max(1, std::min(splits, n / 128));
   p.col_splits = splits;
 }
 

@@ -89,7 +89,7 @@ __host__ __device__ inline CLayout clayout(int n, int m, int C, int es) {
   L.o_rowslot = o;  o += al16((size_t)kMaxCluster * 4 * 8);
   L.o_colslot = o;  o += al16((size_t)kMaxCluster * 3 * 8);
   L.o_ctrl = o;     o += al16(sizeof(Ctrl));
-  L.o_tab = o;      o += al16(16 * 8);
+  L.o_tab = o;      o += al16(kExp2TableSize * 8);
   L.o_stage = o;    o += al16((size_t)2 * C * L.sl * 8);   // remote (max, sum) of the slice
   L.o_gath = o;     o += al16((size_t)kMaxCluster * 4 * 8); // remote row / column statistics
   L.total = o;

@@ -445,7 +445,7 @@ int bcd_solve_noalloc(const double* M, const double* a, const double* b, double*
 }
 
 __global__ void diag_exp2_kernel(const double* x, double* y, int n, int mode) {
-  __shared__ double tab[16];
+  __shared__ double tab[kExp2TableSize];
   load_exp2_table(tab);
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(kThreads) hist_kernel(const TM* __restrict__ M
                                                         const double* __restrict__ gamma, int n,
                                                         int m, double s2, const SelState* sel,
                                                         unsigned int* __restrict__ hist) {
-  __shared__ double tab[16];
+  __shared__ double tab[kExp2TableSize];
   __shared__ unsigned int sh[kBins];
   load_exp2_table(tab);
   for (int b = threadIdx.x; b < kBins; b += blockDim.x) sh[b] = 0u;
@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(kThreads) count_kernel(const TM* __restrict__ 
                                                          int m, double s2, const SelState* sel,
                                                          int* __restrict__ colcnt,
                                                          int* __restrict__ rowcnt, int coltiles) {
-  __shared__ double tab[16];
+  __shared__ double tab[kExp2TableSize];
   __shared__ int srow[kTile];
   load_exp2_table(tab);
   for (int r = threadIdx.x; r < kTile; r += blockDim.x) srow[r] = 0;
@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(kThreads) emit_kernel(
     const SelState* sel, const int* __restrict__ coloff, const int* __restrict__ rowoff,
     int coltiles, const int* __restrict__ rowptr, const int* __restrict__ ipt, double* val,
     int* col, int* ij, double* iv) {
-  __shared__ double tab[16];
+  __shared__ double tab[kExp2TableSize];
   __shared__ unsigned int bits[kTile][kWarps];
   load_exp2_table(tab);
   __syncthreads();
@@ -399,7 +399,7 @@ template <typename TM>
 __global__ void refresh_byj_kernel(const TM* __restrict__ M, const double* __restrict__ gamma,
                                    int n, int m, double s2, const int* __restrict__ rowptr,
                                    const int* __restrict__ col, double* __restrict__ val) {
-  __shared__ double tab[16];
+  __shared__ double tab[kExp2TableSize];
   load_exp2_table(tab);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -417,7 +417,7 @@ template <typename TM>
 __global__ void refresh_byi_kernel(const TM* __restrict__ M, const double* __restrict__ gamma,
                                    int n, int m, double s2, const int* __restrict__ ipt,
                                    const int* __restrict__ ij, double* __restrict__ iv) {
-  __shared__ double tab[16];
+  __shared__ double tab[kExp2TableSize];
   load_exp2_table(tab);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;

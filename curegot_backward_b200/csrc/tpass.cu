@@ -50,7 +50,7 @@ template <typename TM>
 __global__ void __launch_bounds__(kThreads, 3) tpass_kernel(const TPassArgs A) {
   constexpr int VN = TLayout<TM>::VN, NV = TLayout<TM>::NV;
   constexpr int VS = 32 * VN;  // column stride between a lane's vectors
-  __shared__ double tab[16];
+  __shared__ double tab[kExp2TableSize];
   __shared__ double sm_col[kWarps][kTStrip];
   __shared__ double red[kWarps];
   load_exp2_table(tab);

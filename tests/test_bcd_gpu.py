@@ -131,8 +131,9 @@ def test_exp2_implementations_vs_cuda(cuda_dev):
     _native.call("cg_diag_exp2", xn.data_ptr(), yn.data_ptr(), xn.numel(), 1,
                  torch.cuda.current_stream().cuda_stream)
     refn = torch.exp2(xn)
-    reln = ((yn - refn).abs() / refn).max().item()
-    assert reln < 5e-7, reln
+    # one FP32 rounding of x (relative |x| 2^-24 ln2) plus the SFU's ~2^-22
+    bound = 2.5e-7 + xn.abs() * 4.2e-8
+    assert bool(((yn - refn).abs() / refn <= bound).all())
 
 
 @pytest.mark.skipif(not oracle.ref_bcd_available(), reason="oracle/_ref not built")
