@@ -61,6 +61,7 @@ def parse():
     p.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU work")
     p.add_argument("--budget-gb", type=float, default=120.0)
     p.add_argument("--seed", type=int, default=4)
+    p.add_argument("--splr-workers", type=int, default=SPLR_WORKERS)
     return p.parse_args()
 
 
@@ -386,7 +387,7 @@ def main():
     from curegot_backward_b200.serving import OTEngine
     dev = torch.device("cuda", local if world > 1 else 0)
     _native.lib().cg_launch_count_reset()
-    eng = OTEngine(budget_bytes=args.budget_gb * 1e9, max_batch=64, splr_workers=SPLR_WORKERS,
+    eng = OTEngine(budget_bytes=args.budget_gb * 1e9, max_batch=64, splr_workers=args.splr_workers,
                    chunk=8)
 
     # warm-up steps (untimed): device inputs, and host inputs for the e2e pass
@@ -478,7 +479,7 @@ def main():
                        "requests_per_step": args.requests,
                        "arrivals": f"poisson {args.rate}/s" if args.rate else "saturation",
                        "l2": "inputs larger than L2 (each step streams > 126 MB of M)",
-                       "engine": f"max_batch 64, {SPLR_WORKERS} SPLR workers, 8 ticks per graph launch",
+                       "engine": f"max_batch 64, {args.splr_workers} SPLR workers, 8 ticks per graph launch",
                        "parallelism": f"replicas x{world}"},
             "latency_ms": {"p50": float(np.percentile(lat, 50)),
                            "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},

@@ -16,8 +16,8 @@
 // * LSEs run in the base-2 exponent domain (duals are also kept scaled by
 //   log2(e)/eta) with a running max updated once per 4-vector chunk, so the
 //   exponentials are branch-free.  FP64 passes use exp2_f64 (table-driven,
-//   ~2 ulp); mixed-precision passes split off the integer part in FP64 and
-//   evaluate only the fraction on the SFU (ex2.approx.f32).
+//   ~2 ulp); mixed-precision passes round the max-shifted exponent (<= 0)
+//   to FP32 once and evaluate it on the SFU (ex2.approx.ftz.f32).
 // * The reference's third pass over M (row marginal for the stop test) is
 //   folded into the next row pass:
 //     rowsum_i(alpha^t, beta^t) = a_i * 2^(s2 * (alpha_i^t - alpha_i^{t+1})),
