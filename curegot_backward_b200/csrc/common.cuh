@@ -54,7 +54,13 @@ int library_pool(int device, cudaMemPool_t* out);
 // Device-to-host reads of small solver state through a thread-local pinned
 // buffer (a pageable destination would take the driver's staged-copy path,
 // which serializes concurrent solver threads).  Both copies are queued on
-// `st`, then the stream is synchronized once.  bytes1 + bytes2 <= 4096.
+// `st`, then the stream is synchronized once.  At most 4096 bytes in all.
+struct ReadSpan {
+  void* host;
+  const void* dev;
+  size_t bytes;
+};
+int read_device_spans(const ReadSpan* spans, int count, cudaStream_t st);
 int read_device(void* host1, const void* dev1, size_t bytes1, cudaStream_t st,
                 void* host2 = nullptr, const void* dev2 = nullptr, size_t bytes2 = 0);
 

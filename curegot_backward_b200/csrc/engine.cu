@@ -7,7 +7,8 @@
 //     problem contributes its CTAs to one row pass and one column pass per
 //     tick (bcd.cu kernels map CTAs to problems through cta_prob/cta_start).
 //     A chunk of ticks is captured once per batch composition as a CUDA graph
-//     and replayed; finished problems exit their CTAs immediately and are
+//     (a new composition updates the executable graph's kernel parameters in
+//     place) and replayed; finished problems exit their CTAs immediately and are
 //     retired at the next chunk boundary, when queued requests are admitted
 //     into the freed slots.  Duals and solver state stay on the device.
 //   * Two batches run side by side on their own streams: requests with at
@@ -46,6 +47,15 @@ size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 // Sinkhorn requests with at most this many bytes of M share the small batch.
 constexpr size_t kSmallBatchBytes = size_t(8) << 20;
+
+// Batch passes may run as grid-stride launches of at most this many CTAs per
+// SM.  0 (the default): one CTA per virtual block.  Short CTAs retire often,
+// so the SPLR workers' high-priority kernels find free SM slots sooner; on
+// the serving stream this measured faster than caps of 1, 2 or 3 CTAs/SM.
+#ifndef CG_ENGINE_CAP
+#define CG_ENGINE_CAP 0
+#endif
+constexpr int kBatchCtasPerSm = CG_ENGINE_CAP;
 
 struct Req {
   cg_request_t r;
@@ -365,8 +375,6 @@ void bcd_loop(cg_engine_s* E, int cls) {
       cudaMemcpyAsync(d_map, h_map.data(), h_map.size() * sizeof(int), cudaMemcpyHostToDevice,
                       st);
       cudaStreamSynchronize(st);  // host vectors are reused below
-      if (gexec) cudaGraphExecDestroy(gexec);
-      gexec = nullptr;
       cudaGraph_t g;
       if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
         const int* drp = d_map;
@@ -374,16 +382,29 @@ void bcd_loop(cg_engine_s* E, int cls) {
         const int* dcp = drs + P;
         const int* dcs = dcp + col_total;
         for (int c = 0; c < E->chunk; ++c) {
-          // at most 2 of the 3 resident CTA slots per SM: the third stays
-          // free for the latency-bound SPLR kernels of the worker streams
-          launch_bcd_row(batch_f32, d_probs, drp, drs, row_total, st, 2 * E->sms);
-          launch_bcd_col(batch_f32, d_probs, dcp, dcs, col_total, st, 2 * E->sms);
+          launch_bcd_row(batch_f32, d_probs, drp, drs, row_total, st, kBatchCtasPerSm * E->sms);
+          launch_bcd_col(batch_f32, d_probs, dcp, dcs, col_total, st, kBatchCtasPerSm * E->sms);
         }
         count_launch(-2LL * E->chunk);  // captured, not executed
         if (cudaStreamEndCapture(st, &g) == cudaSuccess) {
-          if (cudaGraphInstantiate(&gexec, g, 0) != cudaSuccess) gexec = nullptr;
+          // Same topology (2 x chunk kernel nodes) for every composition:
+          // update the executable graph's kernel parameters in place when
+          // the kernels match, else instantiate a new one.
+          cudaGraphExecUpdateResultInfo info;
+          if (!gexec || cudaGraphExecUpdate(gexec, g, &info) != cudaSuccess) {
+            cudaGetLastError();
+            if (gexec) cudaGraphExecDestroy(gexec);
+            gexec = nullptr;
+            if (cudaGraphInstantiate(&gexec, g, 0) != cudaSuccess) gexec = nullptr;
+          }
           cudaGraphDestroy(g);
+        } else if (gexec) {
+          cudaGraphExecDestroy(gexec);
+          gexec = nullptr;
         }
+      } else if (gexec) {
+        cudaGraphExecDestroy(gexec);
+        gexec = nullptr;
       }
       {
         std::lock_guard<std::mutex> sl(E->stat_mu);

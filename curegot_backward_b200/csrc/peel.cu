@@ -261,27 +261,86 @@ __device__ void dev_core_rhs(const double* __restrict__ val, const PeelPtrs& p,
 }
 
 // z <- (L L^T)^{-1} z for nrhs columns; L lower, row-major kc x kc (shared).
+// One warp per right-hand side: the column sweeps synchronise with
+// __syncwarp only (the block-wide version paid two __syncthreads per column).
+// Every z entry receives its updates in the same order as a column sweep.
 __device__ void dev_trisolve(const double* __restrict__ L, int kc, double* __restrict__ z,
                              int nrhs) {
-  for (int j = 0; j < kc; ++j) {
-    if ((int)threadIdx.x < nrhs) z[threadIdx.x * kc + j] /= L[j * kc + j];
-    __syncthreads();
-    const int w = kc - j - 1;
-    for (int e = threadIdx.x; e < nrhs * w; e += blockDim.x) {
-      const int c = e / w, i = j + 1 + (e - c * w);
-      z[c * kc + i] -= L[i * kc + j] * z[c * kc + j];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp < nrhs) {
+    double* zc = z + (size_t)warp * kc;
+    for (int j = 0; j < kc; ++j) {
+      const double zj = zc[j] / L[j * kc + j];
+      __syncwarp();
+      for (int i = j + 1 + lane; i < kc; i += 32) zc[i] = fma(-L[i * kc + j], zj, zc[i]);
+      if (lane == 0) zc[j] = zj;
+      __syncwarp();
     }
+    for (int j = kc - 1; j >= 0; --j) {
+      const double zj = zc[j] / L[j * kc + j];
+      __syncwarp();
+      for (int i = lane; i < j; i += 32) zc[i] = fma(-L[j * kc + i], zj, zc[i]);
+      if (lane == 0) zc[j] = zj;
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+}
+
+// In-place Cholesky S = L L^T of the lower triangle (row-major kc x kc,
+// shared), one __syncthreads per column.  Step j applies column j's rank-1
+// update to the trailing lower triangle and, in the same sweep, finishes
+// column c = j+1: every thread recomputes that column's pivot
+// d = S[c][c] - L[c][j]^2 itself (the same fma as a plain right-looking
+// sweep), so the column can be scaled by 1/sqrt(d) without a second barrier.
+// The diagonal entry is read by every thread during the sweep, so it is
+// stored (as sqrt(d)) at the start of the next sweep.  A pivot that is not
+// positive and finite sets info = column + 1 and continues with d = 1.
+__device__ void dev_cholesky(double* __restrict__ S, int kc, int* __restrict__ info) {
+  double d0 = S[0];
+  if (!(d0 > 0.0) || !isfinite(d0)) {
+    if (threadIdx.x == 0) info[0] = 1;
+    d0 = 1.0;
+  }
+  double lj = sqrt(d0);  // L[j][j] of the column finished last
+  for (int i = 1 + threadIdx.x; i < kc; i += blockDim.x) S[i * kc] = S[i * kc] / lj;
+  __syncthreads();
+  for (int j = 0; j + 1 < kc; ++j) {
+    if (threadIdx.x == 0) S[j * kc + j] = lj;  // nobody reads it in this sweep
+    const int c = j + 1;
+    const double lcj = S[c * kc + j];
+    double dc = fma(-lcj, lcj, S[c * kc + c]);
+    if (!(dc > 0.0) || !isfinite(dc)) {
+      if (threadIdx.x == 0) info[0] = c + 1;
+      dc = 1.0;
+    }
+    const double lc = sqrt(dc);
+    // lower triangle of the trailing block without its first diagonal entry:
+    // rows i = c..kc-1, columns k = c..i; rows ii and w-1-ii share one index
+    // range of length w+1
+    const int w = kc - c;
+    const int total = ((w + 1) >> 1) * (w + 1);
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int pr = e / (w + 1), q = e - pr * (w + 1);
+      int ii, kk;
+      if (q <= pr) {
+        ii = pr;
+        kk = q;
+      } else {
+        ii = w - 1 - pr;
+        kk = q - pr - 1;
+        if (ii == pr) continue;  // odd w: the middle row is covered by q <= pr
+      }
+      if (ii == 0) continue;  // S[c][c]: stored next sweep
+      const int i = c + ii, k = c + kk;
+      const double v = fma(-S[i * kc + j], S[k * kc + j], S[i * kc + k]);
+      S[i * kc + k] = (kk == 0) ? v / lc : v;
+    }
+    lj = lc;
     __syncthreads();
   }
-  for (int j = kc - 1; j >= 0; --j) {
-    if ((int)threadIdx.x < nrhs) z[threadIdx.x * kc + j] /= L[j * kc + j];
-    __syncthreads();
-    for (int e = threadIdx.x; e < nrhs * j; e += blockDim.x) {
-      const int c = e / j, i = e - c * j;
-      z[c * kc + i] -= L[j * kc + i] * z[c * kc + j];
-    }
-    __syncthreads();
-  }
+  if (threadIdx.x == 0) S[(kc - 1) * kc + (kc - 1)] = lj;
+  __syncthreads();
 }
 
 // Core back-substitution from the Schur-side solution zc, then the backward
@@ -382,30 +441,7 @@ __global__ void __launch_bounds__(kPeelThreads) peel_fused_kernel(
     __syncthreads();
   }
   if (kc > 0) {
-    // right-looking Cholesky of the lower triangle
-    for (int j = 0; j < kc; ++j) {
-      if (threadIdx.x == 0) {
-        double dj = S[j * kc + j];
-        if (!(dj > 0.0) || !isfinite(dj)) {
-          info[0] = j + 1;
-          dj = 1.0;
-        }
-        S[j * kc + j] = sqrt(dj);
-      }
-      __syncthreads();
-      const double ljj = S[j * kc + j];
-      for (int i = j + 1 + threadIdx.x; i < kc; i += blockDim.x) S[i * kc + j] = S[i * kc + j] / ljj;
-      __syncthreads();
-      const int w = kc - j - 1;
-      for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
-        const int ii = e / w, kk = e - ii * w;
-        if (kk <= ii) {
-          const int i = j + 1 + ii, k = j + 1 + kk;
-          S[i * kc + k] -= S[i * kc + j] * S[k * kc + j];
-        }
-      }
-      __syncthreads();
-    }
+    dev_cholesky(S, kc, info);
     for (int e = threadIdx.x; e < kc * kc; e += blockDim.x) Lout[e] = S[e];
   }
   if (nrhs == 0) return;

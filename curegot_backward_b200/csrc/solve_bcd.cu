@@ -69,8 +69,7 @@ int pool_alloc_async(void** ptr, size_t bytes, cudaStream_t stream) {
   return CG_OK;
 }
 
-int read_device(void* host1, const void* dev1, size_t bytes1, cudaStream_t st, void* host2,
-                const void* dev2, size_t bytes2) {
+int read_device_spans(const ReadSpan* spans, int count, cudaStream_t st) {
   struct Pinned {
     void* p = nullptr;
     ~Pinned() {
@@ -79,18 +78,33 @@ int read_device(void* host1, const void* dev1, size_t bytes1, cudaStream_t st, v
   };
   thread_local Pinned buf;
   constexpr size_t kBytes = 4096;
-  if (bytes1 + bytes2 > kBytes) {
+  size_t total = 0;
+  for (int k = 0; k < count; ++k) total += spans[k].bytes;
+  if (total > kBytes) {
     set_last_error("read_device: more than 4096 bytes", __FILE__, __LINE__);
     return CG_ERR_INVALID_ARG;
   }
   if (!buf.p) CG_TRY_CUDA(cudaHostAlloc(&buf.p, kBytes, cudaHostAllocDefault));
   char* pin = static_cast<char*>(buf.p);
-  if (bytes1) CG_TRY_CUDA(cudaMemcpyAsync(pin, dev1, bytes1, cudaMemcpyDeviceToHost, st));
-  if (bytes2) CG_TRY_CUDA(cudaMemcpyAsync(pin + bytes1, dev2, bytes2, cudaMemcpyDeviceToHost, st));
+  size_t off = 0;
+  for (int k = 0; k < count; ++k) {
+    if (spans[k].bytes)
+      CG_TRY_CUDA(cudaMemcpyAsync(pin + off, spans[k].dev, spans[k].bytes, cudaMemcpyDeviceToHost, st));
+    off += spans[k].bytes;
+  }
   CG_TRY_CUDA(cudaStreamSynchronize(st));
-  if (bytes1) std::memcpy(host1, pin, bytes1);
-  if (bytes2) std::memcpy(host2, pin + bytes1, bytes2);
+  off = 0;
+  for (int k = 0; k < count; ++k) {
+    if (spans[k].bytes) std::memcpy(spans[k].host, pin + off, spans[k].bytes);
+    off += spans[k].bytes;
+  }
   return CG_OK;
+}
+
+int read_device(void* host1, const void* dev1, size_t bytes1, cudaStream_t st, void* host2,
+                const void* dev2, size_t bytes2) {
+  const ReadSpan spans[2] = {{host1, dev1, bytes1}, {host2, dev2, bytes2}};
+  return read_device_spans(spans, 2, st);
 }
 
 void set_last_error(const char* msg, const char* file, int line) {

@@ -542,7 +542,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     CG_TRY(launch_tpass(f32, x, st));
     return read_dev(&host, out, st);
   };
-  auto trial_at = [&](double step, TResult& host) -> int {
+  auto trial_launch = [&](double step) -> int {
     TPassArgs x = ta;
     x.gamma = gamma;
     x.gamma_prev = gamma_prev;
@@ -553,7 +553,10 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     x.cols = cols;
     x.grad = grad;
     x.res = res;
-    CG_TRY(launch_tpass(f32, x, st));
+    return launch_tpass(f32, x, st);
+  };
+  auto trial_at = [&](double step, TResult& host) -> int {
+    CG_TRY(trial_launch(step));
     return read_dev(&host, res, st);
   };
   const int bgrid = grid_for(m, 256, 1024);
@@ -722,12 +725,32 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     { woodbury_kernel<<<1, 1024, 0, st>>>(hb.sol2, hb.sol2 + H, grad, hb.rhs2 + H, hb.s, H, reg, 1,
                                         hb.dres); cg::count_launch(); }
     CG_TRY_CUDA(cudaGetLastError());
+    // save_history (first H entries)
+    CG_TRY_CUDA(cudaMemcpyAsync(gamma_prev, gamma, H * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CG_TRY_CUDA(cudaMemcpyAsync(grad_prev, grad, H * sizeof(double), cudaMemcpyDeviceToDevice, st));
+
+    // The line search's first trial point depends only on the previous step
+    // length, so its pass is queued behind the direction solve and read back
+    // together with the direction's status: one host round trip instead of
+    // two.  Its result is the one the line search (or, for an ascent
+    // direction, the recomputation at the initial step) would produce.
+    const double step_min = 1e-10, step_max = 2.0;
+    double init_step = std::min(1.0, 1.5 * alpha_step);
+    init_step = std::max(init_step, step_min);
+    init_step = std::min(init_step, step_max);
+    CG_TRY(trial_launch(init_step));
     DirRes dr{};
+    TResult t_first{};
     int info2[2] = {0, 0};
     const int* isrc = nullptr;
     size_t ibytes = 0;
     factor_info_src(&isrc, &ibytes);
-    CG_TRY(read_device(&dr, hb.dres, sizeof(DirRes), st, info2, isrc, ibytes));
+    {
+      const ReadSpan spans[3] = {{&dr, hb.dres, sizeof(DirRes)},
+                                 {info2, isrc, ibytes},
+                                 {&t_first, res, sizeof(TResult)}};
+      CG_TRY(read_device_spans(spans, 3, st));
+    }
     if (sp_bad || info2[0] != 0 || info2[1] != 0) {
       set_last_error("direction solve: sparsified Hessian not positive definite", __FILE__,
                      __LINE__);
@@ -737,22 +760,15 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     yy = dr.yy;
     low_rank = dr.low_rank != 0;
 
-    // save_history (first H entries)
-    CG_TRY_CUDA(cudaMemcpyAsync(gamma_prev, gamma, H * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    CG_TRY_CUDA(cudaMemcpyAsync(grad_prev, grad, H * sizeof(double), cudaMemcpyDeviceToDevice, st));
-
     // line_search_wolfe (sinkhorn_splr.cu:667-920)
     bool recompute_fg = false;
+    bool first_pending = true;  // t_first not yet consumed
     int trials = 0;
     double step_out = 0.0;
     double last_trial_gnorm = gnorm;
     {
       const double c1 = 1e-4, c2 = 0.9;
       const int ls_max = 20;
-      const double step_min = 1e-10, step_max = 2.0;
-      double init_step = std::min(1.0, 1.5 * alpha_step);
-      init_step = std::max(init_step, step_min);
-      init_step = std::min(init_step, step_max);
       double step = init_step;
       double dg = dr.dg_init;
       double fx = objfn;
@@ -778,7 +794,12 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
         const double delta_max = 1.1, delta_min = 7.0 / 12, shrink = 0.66;
         for (int it = 0; it < ls_max && !done; ++it) {
           TResult t{};
-          CG_TRY(trial_at(step, t));
+          if (first_pending) {
+            t = t_first;  // step == init_step
+            first_pending = false;
+          } else {
+            CG_TRY(trial_at(step, t));
+          }
           ++trials;
           fx = t.f;
           dg = t.dg;
@@ -850,7 +871,11 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     const double gnorm_pre = gnorm;
     if (recompute_fg) {
       TResult t{};
-      CG_TRY(trial_at(alpha_step, t));
+      if (first_pending && alpha_step == init_step) {
+        t = t_first;  // the queued pass already evaluated this point
+      } else {
+        CG_TRY(trial_at(alpha_step, t));
+      }
       objfn = t.f;
       gnorm = t.gnorm;
     } else {
