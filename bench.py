@@ -44,7 +44,8 @@ if ROOT not in sys.path:
 METRIC = "solves/s + p99 latency, mixed-size OT stream @1e-8 marginal err, vs plain FP64"
 TOL = 1e-8
 TRAFFIC_RATIO_F32 = 1.025
-SPLR_WORKERS = 8
+SPLR_WORKERS = 16
+IN_FLIGHT = 24
 
 
 def parse():
@@ -62,6 +63,8 @@ def parse():
     p.add_argument("--budget-gb", type=float, default=120.0)
     p.add_argument("--seed", type=int, default=4)
     p.add_argument("--splr-workers", type=int, default=SPLR_WORKERS)
+    p.add_argument("--in-flight", type=int, default=IN_FLIGHT,
+                   help="saturation: requests kept in flight by the closed-loop client")
     return p.parse_args()
 
 
@@ -430,7 +433,7 @@ def main():
     s0 = eng.stats()
     l0 = _native.lib().cg_launch_count()
     sampler.start()
-    total_ms, results = timed_engine_pass(eng, steps, False, args.rate, world, args.requests)
+    total_ms, results = timed_engine_pass(eng, steps, False, args.rate, world, args.in_flight)
     clocks = sampler.stop()
     launches = _native.lib().cg_launch_count() - l0
     s1 = eng.stats()
@@ -458,7 +461,7 @@ def main():
         hsteps = [to_host_pinned(p) for p in steps]
         h2d = sum(p[1].numel() * 4 + (p[0].n + p[0].m) * 8 for st in hsteps for p in st)
         d2h = sum((p[0].n + p[0].m) * 8 for st in hsteps for p in st)
-        e_ms, _ = timed_engine_pass(eng, hsteps, True, args.rate, world, args.requests)
+        e_ms, _ = timed_engine_pass(eng, hsteps, True, args.rate, world, args.in_flight)
         e2e = {"value": total_req / (e_ms / 1000.0), "unit": "solves/s",
                "h2d_bytes_per_step": int(h2d / max(args.steps, 1)),
                "d2h_bytes_per_step": int(d2h / max(args.steps, 1))}
@@ -505,7 +508,7 @@ def main():
                        "requests_per_step": args.requests,
                        "arrivals": (f"poisson {args.rate}/s, one stream over the timed steps" if args.rate else
                                     f"saturation: closed loop over the timed steps' {n_req} requests, "
-                                    f"{args.requests} in flight"),
+                                    f"{args.in_flight} in flight"),
                        "l2": "inputs larger than L2 (each step streams > 126 MB of M)",
                        "engine": f"max_batch 64, {args.splr_workers} SPLR workers, 8 ticks per graph launch",
                        "parallelism": f"replicas x{world}"},

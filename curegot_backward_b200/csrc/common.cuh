@@ -55,6 +55,15 @@ int library_pool(int device, cudaMemPool_t* out);
 // buffer (a pageable destination would take the driver's staged-copy path,
 // which serializes concurrent solver threads).  Both copies are queued on
 // `st`, then the stream is synchronized once.  At most 4096 bytes in all.
+// Host wait for all work queued on `st`.  By default the calling thread
+// blocks in cudaStreamSynchronize (the runtime spins while few contexts are
+// active).  A thread that called host_wait_yield(true) -- the serving
+// engine's batch and SPLR worker threads -- instead polls an event and
+// yields its core between polls, so many solver threads can wait at once
+// without occupying every host core.
+int host_wait(cudaStream_t st);
+void host_wait_yield(bool on);
+
 struct ReadSpan {
   void* host;
   const void* dev;

@@ -16,7 +16,9 @@
 //     tens of microseconds, so small requests are not held back by the tick
 //     length of the large problems.
 //   * SPLR requests run on worker threads, each with its own stream, so their
-//     device work overlaps the Sinkhorn batch.
+//     device work overlaps the Sinkhorn batch.  Engine threads wait for their
+//     streams by polling and yielding, so 16 workers and the two batch
+//     threads share the host cores.
 //   * Admission is by HBM footprint: a request enters only while the sum of
 //     the footprints of admitted requests stays within the budget.
 //   * Each request records submit / admit / finish times (host steady clock)
@@ -263,6 +265,7 @@ void bcd_loop(cg_engine_s* E, int cls) {
   std::deque<Req*>& bq = E->bcd_qs[cls];
   long long my_active = 0;
   cudaSetDevice(E->device);
+  host_wait_yield(true);
   cudaStream_t st;
   // lowest priority: the batch passes are throughput work that fills every
   // SM; the latency-bound SPLR kernels of the workers go first
@@ -374,7 +377,7 @@ void bcd_loop(cg_engine_s* E, int cls) {
       cudaMemcpyAsync(d_probs, h_probs.data(), P * sizeof(BcdProb), cudaMemcpyHostToDevice, st);
       cudaMemcpyAsync(d_map, h_map.data(), h_map.size() * sizeof(int), cudaMemcpyHostToDevice,
                       st);
-      cudaStreamSynchronize(st);  // host vectors are reused below
+      host_wait(st);  // host vectors are reused below
       cudaGraph_t g;
       if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
         const int* drp = d_map;
@@ -440,7 +443,7 @@ void bcd_loop(cg_engine_s* E, int cls) {
     // states of all problems: one gather kernel, one copy
     { gather_states_kernel<<<std::max(1, (P + 127) / 128), 128, 0, st>>>(d_probs, P, d_states); cg::count_launch(); }
     cudaMemcpyAsync(h_states, d_states, P * sizeof(BcdState), cudaMemcpyDeviceToHost, st);
-    cudaStreamSynchronize(st);
+    host_wait(st);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ev0, ev1);
     std::unique_lock<std::mutex> stat_lk(E->stat_mu);
@@ -479,7 +482,7 @@ void bcd_loop(cg_engine_s* E, int cls) {
       dirty = true;
     }
     if (dirty) {
-      cudaStreamSynchronize(st);
+      host_wait(st);
       for (int k = 0; k < P; ++k) {
         Req* q = active[k];
         if (!h_states[k].done) continue;
@@ -498,7 +501,7 @@ void bcd_loop(cg_engine_s* E, int cls) {
   if (h_states) cudaFreeHost(h_states);
   if (d_probs) cudaFreeAsync(d_probs, st);
   if (d_map) cudaFreeAsync(d_map, st);
-  cudaStreamSynchronize(st);
+  host_wait(st);
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
   cudaStreamDestroy(st);
@@ -506,6 +509,7 @@ void bcd_loop(cg_engine_s* E, int cls) {
 
 void splr_loop(cg_engine_s* E) {
   cudaSetDevice(E->device);
+  host_wait_yield(true);
   cudaStream_t st;
   int prio_lo = 0, prio_hi = 0;
   cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
@@ -573,7 +577,7 @@ void splr_loop(cg_engine_s* E) {
         cudaMemcpyAsync(r.dual_out, ddual, 8 * (size_t)(n + m),
                         r.host_inputs ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, st);
       cudaFreeAsync(blk, st);
-      cudaStreamSynchronize(st);
+      host_wait(st);
     }
     q->status = rc;
     {

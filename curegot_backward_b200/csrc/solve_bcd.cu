@@ -10,6 +10,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 
 #include "bcd.cuh"
 #include "workspace.cuh"
@@ -69,6 +70,44 @@ int pool_alloc_async(void** ptr, size_t bytes, cudaStream_t stream) {
   return CG_OK;
 }
 
+namespace {
+thread_local bool t_wait_yield = false;
+}
+
+void host_wait_yield(bool on) { t_wait_yield = on; }
+
+int host_wait(cudaStream_t st) {
+  if (!t_wait_yield) {
+    CG_TRY_CUDA(cudaStreamSynchronize(st));
+    return CG_OK;
+  }
+  struct Event {
+    cudaEvent_t e = nullptr;
+    int dev = -1;
+    ~Event() {
+      if (e) cudaEventDestroy(e);
+    }
+  };
+  thread_local Event ev;
+  int dev = 0;
+  CG_TRY_CUDA(cudaGetDevice(&dev));
+  if (ev.e && ev.dev != dev) {
+    cudaEventDestroy(ev.e);
+    ev.e = nullptr;
+  }
+  if (!ev.e) {
+    CG_TRY_CUDA(cudaEventCreateWithFlags(&ev.e, cudaEventDisableTiming));
+    ev.dev = dev;
+  }
+  CG_TRY_CUDA(cudaEventRecord(ev.e, st));
+  while (true) {
+    const cudaError_t q = cudaEventQuery(ev.e);
+    if (q == cudaSuccess) return CG_OK;
+    if (q != cudaErrorNotReady) CG_TRY_CUDA(q);
+    std::this_thread::yield();
+  }
+}
+
 int read_device_spans(const ReadSpan* spans, int count, cudaStream_t st) {
   struct Pinned {
     void* p = nullptr;
@@ -92,7 +131,7 @@ int read_device_spans(const ReadSpan* spans, int count, cudaStream_t st) {
       CG_TRY_CUDA(cudaMemcpyAsync(pin + off, spans[k].dev, spans[k].bytes, cudaMemcpyDeviceToHost, st));
     off += spans[k].bytes;
   }
-  CG_TRY_CUDA(cudaStreamSynchronize(st));
+  CG_TRY(host_wait(st));
   off = 0;
   for (int k = 0; k < count; ++k) {
     if (spans[k].bytes) std::memcpy(spans[k].host, pin + off, spans[k].bytes);

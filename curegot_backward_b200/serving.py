@@ -24,7 +24,7 @@ _ALGOS = {"bcd": _native.CG_ALGO_BCD, "splr": _native.CG_ALGO_SPLR}
 
 
 class OTEngine:
-    def __init__(self, budget_bytes=120e9, max_batch=64, splr_workers=8, chunk=8, device=None):
+    def __init__(self, budget_bytes=120e9, max_batch=64, splr_workers=16, chunk=8, device=None):
         if not torch.cuda.is_available():
             raise RuntimeError("OTEngine: a CUDA device is required (no CPU fallback)")
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None
