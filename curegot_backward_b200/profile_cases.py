@@ -3,6 +3,7 @@
     python -m curegot_backward_b200.profile_cases bcd --n 8192 --m 8192 --precision mixed
     python -m curegot_backward_b200.profile_cases splr --n 4096 --m 4096 --density 0.1
     python -m curegot_backward_b200.profile_cases backward --n 2048 --m 2560
+    python -m curegot_backward_b200.profile_cases precision --n 16384 --algo splr
 
 Each case builds a seeded synthetic problem on cuda:0, runs it once to warm
 up, then times `--reps` runs with CUDA events on the launching stream and
@@ -13,6 +14,11 @@ prints one JSON line.  Achieved bandwidth uses algorithmic bytes:
             right-hand-side and gradient-assembly passes (2 * n * m * 8 reads
             of T and G, n * m * 8 written).
 The SPLR case reports wall time, iterations and the direction-solve path.
+The precision case solves the precision-form problem (X, Y ~ N(0, I_32),
+M = |x - y|^2 / median stored in FP32, Dirichlet(1) marginals floored at
+1e-7, eta = 1e-3) in mixed precision once and reports its time, iterations
+and the marginal errors of the returned duals evaluated in FP64 (torch, on
+the FP32-valued M upcast exactly).
 """
 
 from __future__ import annotations
@@ -107,9 +113,47 @@ def case_backward(a):
             "peak_GBps": peak, "peak_kind": kind, "frac": gbs / peak}
 
 
+def fp64_marginal_errors(M, a, b, dual, eta, rows_per_chunk=1024):
+    """||T 1 - a||_2 and ||T^T 1 - b||_2 of T = exp((alpha_i + beta_j - M_ij) / eta),
+    evaluated in FP64 in row chunks."""
+    n, m = M.shape
+    al, be = dual[:n].double(), dual[n:].double()
+    rows = torch.empty(n, dtype=torch.float64, device=M.device)
+    cols = torch.zeros(m, dtype=torch.float64, device=M.device)
+    for i0 in range(0, n, rows_per_chunk):
+        i1 = min(n, i0 + rows_per_chunk)
+        T = torch.exp((al[i0:i1, None] + be[None, :] - M[i0:i1].double()) / eta)
+        rows[i0:i1] = T.sum(1)
+        cols += T.sum(0)
+    return float(torch.linalg.norm(rows - a)), float(torch.linalg.norm(cols - b))
+
+
+def case_precision(a):
+    dev = torch.device("cuda", 0)
+    M, am, bm, eta = synthetic.config2(device=dev, n=a.n, m=a.n)
+    if a.algo == "bcd":
+        run = lambda: _solvers._bcd_device(M, am, bm, eta, a.tol, a.max_iter, None, "mixed",
+                                           want_plan=False)
+    else:
+        run = lambda: _solvers._splr_device(M, am, bm, eta, a.tol, a.max_iter, 0, None, "mixed",
+                                            0.01, 1e-3, 30, 3, want_plan=False)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    out = run()
+    e1.record()
+    torch.cuda.synchronize()
+    niter, dual = (out[0], out[2]) if a.algo == "bcd" else (out["niter"], out["dual"])
+    row_err, col_err = fp64_marginal_errors(M, am, bm, dual, eta)
+    return {"case": "precision", "algo": a.algo, "n": a.n, "m": a.n, "eta": eta,
+            "M_dtype": "float32", "iterations": int(niter), "max_iter": a.max_iter,
+            "seconds": e0.elapsed_time(e1) / 1e3, "fp64_row_err": row_err,
+            "fp64_col_err": col_err, "tol": a.tol}
+
+
 def main(argv=None):
     p = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    p.add_argument("case", choices=["bcd", "splr", "backward"])
+    p.add_argument("case", choices=["bcd", "splr", "backward", "precision"])
     p.add_argument("--n", type=int, default=8192)
     p.add_argument("--m", type=int, default=8192)
     p.add_argument("--d", type=int, default=16)
@@ -124,8 +168,11 @@ def main(argv=None):
     p.add_argument("--precond", default="diag", choices=["none", "diag", "splr"])
     p.add_argument("--reps", type=int, default=3)
     p.add_argument("--seed", type=int, default=7)
+    p.add_argument("--algo", default="splr", choices=["bcd", "splr"], help="precision case")
+    p.add_argument("--max-iter", type=int, default=100000, help="precision case")
     a = p.parse_args(argv)
-    res = {"bcd": case_bcd, "splr": case_splr, "backward": case_backward}[a.case](a)
+    res = {"bcd": case_bcd, "splr": case_splr, "backward": case_backward,
+           "precision": case_precision}[a.case](a)
     print(json.dumps(res), flush=True)
 
 
