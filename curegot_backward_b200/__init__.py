@@ -22,7 +22,7 @@ import types as _types
 
 from . import _native, _solvers
 from ._context import SPLRBackwardContext
-from . import backward, autograd
+from . import backward, autograd, points
 from .autograd import SPLROT, splr_ot, splr_ot_batch, splr_ot_with_info
 from .backward import solve_backward
 

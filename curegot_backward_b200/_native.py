@@ -24,6 +24,8 @@ CG_ERR_NONFINITE = 6
 CG_ERR_INVALID_CONTEXT = 7
 CG_ERR_SOLVER = 8
 CG_ERR_ADMISSION = 9
+CG_POINTS_FP64 = 0
+CG_POINTS_MIXED = 1
 
 _STATUS_NAMES = {
     CG_ERR_INVALID_ARG: "invalid argument",
@@ -104,6 +106,10 @@ SIGNATURES = {
     "cg_bcd_f64_noalloc": [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_double,
                            c_int, c_int, c_int_p, c_void_p, c_void_p, c_void_p],
     "cg_bcd_set_cluster_path": [c_int],
+    "cg_points_cost_bf16": [c_void_p, c_void_p, c_int, c_int, c_int, c_double, c_void_p, c_void_p],
+    "cg_bcd_points_bf16": [c_void_p, c_void_p, c_int, c_int, c_int, c_double, c_void_p, c_void_p,
+                           c_double, c_int, c_double, c_int, c_int_p, c_void_p, c_int_p,
+                           c_void_p],
     "cg_bcd_mixed": [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_double, c_int,
                      c_int, c_int_p, c_void_p, c_void_p, c_void_p],
     "cg_transport_plan_f64": [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_int,

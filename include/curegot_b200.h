@@ -308,6 +308,35 @@ int cg_test_spd_solve_f64(const double* values, const int* colind, const int* ro
                           const double* rhs, double* x, cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ */
+/* Cost recomputed from point clouds on the tensor cores.                    */
+/* ------------------------------------------------------------------------ */
+/*
+ * No reference counterpart (the reference always takes a materialised M,
+ * src/solvers.h:4-9); this is the BF16-input / FP32-compute cost variant of
+ * the differentiation configuration.  X (n x d) and Y (m x d) are row-major
+ * BF16 device arrays (raw 16-bit patterns), 1 <= d <= 64.  The cost is
+ *   M_ij = max(0, s * ((|x_i|^2 + |y_j|^2) - 2 x_i . y_j))       (FP32)
+ * with x_i . y_j accumulated in FP32 by tcgen05 MMAs and the squared norms
+ * summed in FP32 (s = cost_scale, e.g. 1/d for the mean over features).
+ *
+ * cg_points_cost_bf16 writes M (n x m FP32, row-major, device).
+ * cg_bcd_points_bf16 runs Sinkhorn BCD on that cost without storing it:
+ * alpha, beta updates as cg_bcd_f64 (src/sinkhorn_bcd_kernel.cu:35-634),
+ * stopping when the row-marginal error ||T 1 - a||_2 of an iterate is below
+ * tol (checked for every iterate).  precision CG_POINTS_FP64: FP64
+ * exponentials; CG_POINTS_MIXED: SFU exponentials until the estimate is
+ * below tol/2, then FP64 passes confirm.  dual: device [n + m] (alpha, beta);
+ * niter, fast_iters: host (nullable).
+ */
+enum { CG_POINTS_FP64 = 0, CG_POINTS_MIXED = 1 };
+int cg_points_cost_bf16(const uint16_t* X, const uint16_t* Y, int n, int m, int d,
+                        double cost_scale, float* M, cudaStream_t stream);
+int cg_bcd_points_bf16(const uint16_t* X, const uint16_t* Y, int n, int m, int d,
+                       double cost_scale, const double* a, const double* b, double reg,
+                       int max_iter, double tol, int precision, int* niter, double* dual,
+                       int* fast_iters, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ */
 /* Diagnostics (no reference counterpart).                                   */
 /* ------------------------------------------------------------------------ */
 
