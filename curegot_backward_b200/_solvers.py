@@ -73,8 +73,25 @@ def _verbose_report(name, n, m, reg, tol, max_iter, niter):
         print("Warning: Maximum iterations reached without convergence")
 
 
+def _device_operands(M, a, b, precision):
+    """The native entry points read M as FP32 (mixed) or FP64 and a, b as
+    FP64 contiguous device arrays; anything else is rejected here, before a
+    kernel could read past a buffer."""
+    want = torch.float32 if precision == "mixed" else torch.float64
+    if M.dtype != want:
+        raise TypeError(f"{precision} solve needs M as {want}, got {M.dtype}")
+    for t in (M, a, b):
+        if not t.is_cuda or not t.is_contiguous() or t.device != M.device:
+            raise ValueError("M, a and b must be contiguous tensors on one CUDA device")
+    if a.dtype != torch.float64 or b.dtype != torch.float64:
+        raise TypeError("a and b must be float64")
+    if M.dim() != 2 or a.numel() != M.shape[0] or b.numel() != M.shape[1]:
+        raise ValueError("shapes of M, a and b do not agree")
+
+
 def _bcd_device(M, a, b, reg, tol, max_iter, x0, precision, want_plan=True):
     """Core device call: M/a/b already on one CUDA device, contiguous."""
+    _device_operands(M, a, b, precision)
     dev = M.device
     n, m = int(M.shape[0]), int(M.shape[1])
     opts = dict(device=dev, dtype=torch.float64)
@@ -152,6 +169,7 @@ def _splr_kwargs(kwargs, n, m):
 
 def _splr_device(M, a, b, reg, tol, max_iter, verbose, x0, precision, density_max, shift_max,
                  cycle, cand, want_ctx=False, want_plan=True, trace=False):
+    _device_operands(M, a, b, precision)
     dev = M.device
     n, m = int(M.shape[0]), int(M.shape[1])
     opts = dict(device=dev, dtype=torch.float64)

@@ -25,9 +25,11 @@
 //     other side).  Per column tile: the 128 threads stage both BF16 tiles in
 //     shared memory in the canonical no-swizzle K-major layout, one thread
 //     issues d/16 MMAs (M = N = 128, K = 16) into a 128-column TMEM
-//     accumulator and commits them to an mbarrier; after a bounded wait every
-//     thread loads its row (TMEM lane) and folds the 128 costs into its
-//     running (max, sum).  Partials per (row, column range) go to global.
+//     accumulator and commits them to an mbarrier; after a bounded wait each
+//     of the 8 warps loads 64 columns of its 32 rows (its TMEM lane quarter)
+//     and folds the costs into per-thread running (max, sum) pairs; the two
+//     halves of a row are merged at the end.  Partials per (row, column
+//     range) go to global.
 //   * pts_merge_kernel: one thread per row merges the partials in a fixed
 //     order, writes the new dual (double-buffered by iteration parity) and,
 //     on the row side, the marginal-test term of the previous iterate:
@@ -48,7 +50,12 @@ namespace cg {
 namespace {
 
 constexpr int kPtsTile = 128;     // rows per CTA tile (MMA M) = columns per tile (MMA N)
-constexpr int kPtsThreads = 128;  // one thread per TMEM lane / tile row
+constexpr int kPtsThreads = 128;  // cost tiles: one thread per TMEM lane / tile row
+constexpr int kPtsLseThreads = 256;  // LSE passes: two threads per row, 64 columns each
+#ifndef CG_PTS_MINB
+#define CG_PTS_MINB 4
+#endif
+constexpr int kPtsLseMinBlocks = CG_PTS_MINB;  // resident CTAs per SM (64 registers)
 constexpr int kPtsMaxD = 64;      // padded feature dimension (multiple of 16)
 constexpr int kPtsTmemCols = 128;
 constexpr long kPtsSpinLimit = 1L << 24;  // mbarrier polls before giving up
@@ -65,7 +72,7 @@ constexpr int kTileBytesMax = kSliceBytes * (kPtsMaxD / 16);  // 16 KB
 // Dynamic shared memory per CTA: A and B tiles, beta tile (FP64), norm tile
 // (FP32), plus padding that keeps at most 4 CTAs per SM (4 x 128 TMEM
 // columns = the whole tensor memory, so tcgen05.alloc never waits).
-constexpr int kPtsSmem = 2 * kTileBytesMax + kPtsTile * 8 + kPtsTile * 4 + 1024;
+constexpr int kPtsSmem = 2 * kTileBytesMax + 2 * kPtsTile * 8 + kPtsTile * 4 + 1024;
 constexpr int kPtsSmemLaunch = 50 * 1024;
 static_assert(kPtsSmem <= kPtsSmemLaunch, "points smem");
 
@@ -291,9 +298,9 @@ __global__ void __launch_bounds__(kPtsThreads) pts_cost_kernel(
 
 // Partial LSE over the column tiles [t0, t1) for the 128 rows of tile
 // blockIdx.x: part[(split * rows_pad + r) * 2 + {0, 1}] = (max, sum) in base 2
-// of xs_j - s2 M_rj, xs the other side's scaled duals.
-template <bool FAST>
-__global__ void __launch_bounds__(kPtsThreads) pts_lse_kernel(
+// of xs_j - s2 M_rj, xs the other side's scaled duals.  The state's
+// precision flag picks SFU or FP64 exponentials for the whole pass.
+__global__ void __launch_bounds__(kPtsLseThreads, kPtsLseMinBlocks) pts_lse_kernel(
     const uint16_t* __restrict__ P, const uint16_t* __restrict__ Q, const float* __restrict__ nP,
     const float* __restrict__ nQ, int rows, int cols, int D, float scale,
     const double* __restrict__ xs_base, size_t xs_stride, int xs_parity, double s2,
@@ -302,14 +309,14 @@ __global__ void __launch_bounds__(kPtsThreads) pts_lse_kernel(
   __shared__ PtsShared sh;
   __shared__ double tab[kExp2TableSize];
   if (ldcg(&st->done)) return;
-  if (ldcg(&st->fast) != (FAST ? 1 : 0)) return;  // the other variant runs this pass
+  const bool fast = ldcg(&st->fast) != 0;
   const int k = ldcg(&st->k);
   // row side: beta^k (parity k); column side: the alpha^{k+1} just written
   const double* __restrict__ xs = xs_base + (size_t)((k + xs_parity) & 1) * xs_stride;
   char* tA = smem;
   char* tB = smem + kTileBytesMax;
   double* sx = reinterpret_cast<double*>(smem + 2 * kTileBytesMax);
-  float* sn = reinterpret_cast<float*>(smem + 2 * kTileBytesMax + kPtsTile * 8);
+  float* sn = reinterpret_cast<float*>(smem + 2 * kTileBytesMax + 2 * kPtsTile * 8);
   load_exp2_table(tab);
   pts_setup(sh);
 
@@ -318,8 +325,12 @@ __global__ void __launch_bounds__(kPtsThreads) pts_lse_kernel(
   const int ntiles = (cols + kPtsTile - 1) / kPtsTile;
   const int t0 = split * tiles_per_split, t1 = min(ntiles, t0 + tiles_per_split);
   stage_tile(P, rows, D, r0, tA);
-  const int warp = threadIdx.x >> 5;
-  const int r = r0 + threadIdx.x;
+  // warp w reads TMEM lanes 32 (w % 4) .. + 31 (its lane quarter) and the
+  // accumulator columns 64 (w / 4) .. + 63 of every tile
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int quarter = warp & 3, half = warp >> 2;
+  const int rl = quarter * 32 + lane;  // row within the tile
+  const int r = r0 + rl;
   const float nr = r < rows ? nP[r] : 0.0f;
   double mx = kNegInf, s = 0.0;
   uint32_t phase = 0;
@@ -336,9 +347,9 @@ __global__ void __launch_bounds__(kPtsThreads) pts_lse_kernel(
     ok = pts_tile_mma(sh, tA, tB, D, phase);
     if (!ok) break;
 #pragma unroll 1
-    for (int cb = 0; cb < kPtsTile; cb += 32) {
+    for (int cb = half * 64; cb < half * 64 + 64; cb += 32) {
       float v[32];
-      tmem_ld32(sh.tmem + (static_cast<uint32_t>(warp * 32) << 16) + cb, v);
+      tmem_ld32(sh.tmem + (static_cast<uint32_t>(quarter * 32) << 16) + cb, v);
 #pragma unroll
       for (int q0 = 0; q0 < 32; q0 += 4) {
         double dd[4];
@@ -350,12 +361,25 @@ __global__ void __launch_bounds__(kPtsThreads) pts_lse_kernel(
           const float mc = pts_cost(v[q0 + u], nr, sn[c], scale);
           dd[u] = fma(-s2, static_cast<double>(mc), sx[c]);
         }
-        lse_chunk<FAST, 4>(dd, in, mx, s, tab);
+        if (fast)
+          lse_chunk<true, 4>(dd, in, mx, s, tab);
+        else
+          lse_chunk<false, 4>(dd, in, mx, s, tab);
       }
     }
   }
   if (!ok && threadIdx.x == 0) atomicExch(&st->error, 1);
-  if (r < rows) {
+  // the two column halves of each row, merged in a fixed order
+  double* hmx = sx;  // the tile buffers are free now
+  double* hs = sx + kPtsTile;
+  __syncthreads();
+  if (half == 1) {
+    hmx[rl] = mx;
+    hs[rl] = s;
+  }
+  __syncthreads();
+  if (half == 0 && r < rows) {
+    lse2_merge(mx, s, hmx[rl], hs[rl], tab);
     double* o = part + ((size_t)split * rows_pad + r) * 2;
     o[0] = mx;
     o[1] = s;
@@ -509,10 +533,8 @@ int pts_attrs() {
   if (done_dev == dev) return CG_OK;
   CG_TRY_CUDA(cudaFuncSetAttribute(pts_cost_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    kPtsSmemLaunch));
-  CG_TRY_CUDA(cudaFuncSetAttribute(pts_lse_kernel<true>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, kPtsSmemLaunch));
-  CG_TRY_CUDA(cudaFuncSetAttribute(pts_lse_kernel<false>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, kPtsSmemLaunch));
+  CG_TRY_CUDA(cudaFuncSetAttribute(pts_lse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   kPtsSmemLaunch));
   done_dev = dev;
   return CG_OK;
 }
@@ -640,18 +662,13 @@ extern "C" int cg_bcd_points_bf16(const uint16_t* X, const uint16_t* Y, int n, i
     for (int it0 = 0; it0 < max_iter; it0 += kPtsChunk) {
       const int todo = std::min(kPtsChunk, max_iter - it0);
       for (int q = 0; q < todo; ++q) {
-        // row side: alpha^{k+1} from beta^k (both variants launched; the one
-        // that does not match the state's precision returns at once)
-        { pts_lse_kernel<true><<<grow, kPtsThreads, kPtsSmemLaunch, stream>>>(
-            Xp, Yp, nX, nY, n, m, D, sc, bes, (size_t)m, 0, s2, tps_row, part, n_pad, st); count_launch(); }
-        { pts_lse_kernel<false><<<grow, kPtsThreads, kPtsSmemLaunch, stream>>>(
+        // row side: alpha^{k+1} from beta^k
+        { pts_lse_kernel<<<grow, kPtsLseThreads, kPtsSmemLaunch, stream>>>(
             Xp, Yp, nX, nY, n, m, D, sc, bes, (size_t)m, 0, s2, tps_row, part, n_pad, st); count_launch(); }
         { pts_merge_kernel<<<mb_n, 256, 0, stream>>>(part, n, n_pad, sp_row, reg, s2, loga, a, al, als,
                                                     (size_t)n, 1, cnt, berr, st); count_launch(); }
         // column side: beta^{k+1} from alpha^{k+1}
-        { pts_lse_kernel<true><<<gcol, kPtsThreads, kPtsSmemLaunch, stream>>>(
-            Yp, Xp, nY, nX, m, n, D, sc, als, (size_t)n, 1, s2, tps_col, part, m_pad, st); count_launch(); }
-        { pts_lse_kernel<false><<<gcol, kPtsThreads, kPtsSmemLaunch, stream>>>(
+        { pts_lse_kernel<<<gcol, kPtsLseThreads, kPtsSmemLaunch, stream>>>(
             Yp, Xp, nY, nX, m, n, D, sc, als, (size_t)n, 1, s2, tps_col, part, m_pad, st); count_launch(); }
         { pts_merge_kernel<<<mb_m, 256, 0, stream>>>(part, m, m_pad, sp_col, reg, s2, logb, b, be, bes,
                                                     (size_t)m, 0, cnt + 1, berr, st); count_launch(); }

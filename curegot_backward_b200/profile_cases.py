@@ -4,6 +4,7 @@
     python -m curegot_backward_b200.profile_cases splr --n 4096 --m 4096 --density 0.1
     python -m curegot_backward_b200.profile_cases backward --n 2048 --m 2560
     python -m curegot_backward_b200.profile_cases precision --n 16384 --algo splr
+    python -m curegot_backward_b200.profile_cases points --n 16384 --m 16384 --d 32 --iters 20
 
 Each case builds a seeded synthetic problem on cuda:0, runs it once to warm
 up, then times `--reps` runs with CUDA events on the launching stream and
@@ -14,6 +15,11 @@ prints one JSON line.  Achieved bandwidth uses algorithmic bytes:
             right-hand-side and gradient-assembly passes (2 * n * m * 8 reads
             of T and G, n * m * 8 written).
 The SPLR case reports wall time, iterations and the direction-solve path.
+The points case times Sinkhorn iterations on a cost recomputed from BF16
+point clouds on the tensor cores (never stored) for a fixed iteration
+count, and, with --compare, the stored-cost passes on the same cost;
+throughput is reported as cost elements per second (one exponential
+each) against the nominal SFU rate of 148 SMs x 16 ex2/clk x 1.965 GHz.
 The precision case solves the precision-form problem (X, Y ~ N(0, I_32),
 M = |x - y|^2 / median stored in FP32, Dirichlet(1) marginals floored at
 1e-7, eta = 1e-3) in mixed precision once and reports its time, iterations
@@ -151,9 +157,40 @@ def case_precision(a):
             "fp64_col_err": col_err, "tol": a.tol}
 
 
+def case_points(a):
+    from .points import cost_from_points, sinkhorn_bcd_points
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device=dev).manual_seed(a.seed)
+    X = torch.rand(a.n, a.d, generator=g, device=dev).bfloat16()
+    Y = torch.rand(a.m, a.d, generator=g, device=dev).bfloat16()
+    am = torch.full((a.n,), 1.0 / a.n, dtype=torch.float64, device=dev)
+    bm = torch.full((a.m,), 1.0 / a.m, dtype=torch.float64, device=dev)
+    run = lambda: sinkhorn_bcd_points(X, Y, am, bm, a.eta, tol=0.0, max_iter=a.iters,
+                                      precision=a.precision)
+    ms, out = _time(run, a.reps)
+    it = out["niter"]
+    elems = 2.0 * a.n * a.m * it
+    sfu_peak = 148 * 16 * 1.965e9
+    res = {"case": "points", "n": a.n, "m": a.m, "d": a.d, "eta": a.eta,
+           "precision": a.precision, "iterations": it, "ms_per_iteration": ms / it,
+           "elements_per_s": elems / (ms / 1e3), "sfu_nominal_per_s": sfu_peak,
+           "frac_sfu_nominal": elems / (ms / 1e3) / sfu_peak,
+           "point_bytes_per_pass": (a.n + a.m) * a.d * 2}
+    if a.compare:
+        M = cost_from_points(X, Y)
+        if a.precision == "fp64":
+            M = M.double()
+        run2 = lambda: _solvers._bcd_device(M, am, bm, a.eta, 0.0, a.iters, None, a.precision,
+                                            want_plan=False)
+        ms2, _ = _time(run2, a.reps)
+        res["stored_cost_ms_per_iteration"] = ms2 / a.iters
+        del M
+    return res
+
+
 def main(argv=None):
     p = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    p.add_argument("case", choices=["bcd", "splr", "backward", "precision"])
+    p.add_argument("case", choices=["bcd", "splr", "backward", "precision", "points"])
     p.add_argument("--n", type=int, default=8192)
     p.add_argument("--m", type=int, default=8192)
     p.add_argument("--d", type=int, default=16)
@@ -170,9 +207,10 @@ def main(argv=None):
     p.add_argument("--seed", type=int, default=7)
     p.add_argument("--algo", default="splr", choices=["bcd", "splr"], help="precision case")
     p.add_argument("--max-iter", type=int, default=100000, help="precision case")
+    p.add_argument("--compare", action="store_true", help="points: also time the stored cost")
     a = p.parse_args(argv)
     res = {"bcd": case_bcd, "splr": case_splr, "backward": case_backward,
-           "precision": case_precision}[a.case](a)
+           "precision": case_precision, "points": case_points}[a.case](a)
     print(json.dumps(res), flush=True)
 
 
