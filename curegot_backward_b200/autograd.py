@@ -17,6 +17,9 @@ Contract (reference autograd.py:57-126, :214-298):
 from __future__ import annotations
 
 import math
+import queue
+import threading
+from concurrent.futures import ThreadPoolExecutor
 
 import torch
 from torch.autograd.function import once_differentiable
@@ -155,9 +158,38 @@ def splr_ot_with_info(M, a, b, *, eta, tol=1e-6, max_iter=1000, density=None,
             "niter": int(out["niter"]), "converged": bool(out["converged"])}
 
 
+# Concurrent solves of splr_ot_batch: worker threads, each with its own CUDA
+# stream (the native solver waits on the host between its kernels and
+# releases the GIL while it does, so the solves overlap on the device as the
+# serving engine's SPLR workers do).
+# Above _BATCH_MAX_ELEMS cost entries per problem the solves keep the GPU busy
+# on their own and run one after another (measured on B200: 8 concurrent
+# solves were 1.7x faster than a loop at 512 x 640 and 2.2x at 256 x 256,
+# but 0.77x at 2048 x 2560).
+_BATCH_WORKERS = 8
+_BATCH_MAX_ELEMS = 1 << 21
+_batch_streams = {}
+_batch_lock = threading.Lock()
+
+
+def _worker_streams(dev, k):
+    with _batch_lock:
+        lst = _batch_streams.setdefault(dev.index, [])
+        while len(lst) < k:
+            lst.append(torch.cuda.Stream(dev))
+        return lst[:k]
+
+
 def splr_ot_batch(M, a, b, *, eta, **kwargs):
     """[B, n, m] costs, [B, n] and [B, m] marginals -> [B, n, m] plans;
-    gradients flow to M (one native solve per problem)."""
+    gradients flow to M.
+
+    The reference (curegot/autograd.py:340-367) solves the B problems one
+    after another.  Here, for problems of at most 2^21 cost entries, up to 8
+    solves run at once, each on its own worker thread and CUDA stream; every
+    solve is the same native call as splr_ot on the same inputs, so plans
+    and gradients are bitwise those of the sequential loop.  Each problem's
+    backward runs on its forward stream."""
     if M.dim() != 3:
         raise ValueError(f"splr_ot_batch: M must be [B, n, m], got shape {tuple(M.shape)}")
     B = M.shape[0]
@@ -165,7 +197,35 @@ def splr_ot_batch(M, a, b, *, eta, **kwargs):
         raise ValueError(f"splr_ot_batch: a must be [B, n], got shape {tuple(a.shape)}")
     if tuple(b.shape) != (B, M.shape[2]):
         raise ValueError(f"splr_ot_batch: b must be [B, m], got shape {tuple(b.shape)}")
-    return torch.stack([splr_ot(M[i], a[i], b[i], eta=eta, **kwargs) for i in range(B)])
+    W = min(B, _BATCH_WORKERS)
+    if (W <= 1 or not (isinstance(M, torch.Tensor) and M.is_cuda)
+            or M.shape[1] * M.shape[2] > _BATCH_MAX_ELEMS):
+        return torch.stack([splr_ot(M[i], a[i], b[i], eta=eta, **kwargs) for i in range(B)])
+    dev = M.device
+    main = torch.cuda.current_stream(dev)
+    ready = main.record_event()  # inputs (and anything queued before) are done
+    free = queue.Queue()
+    for st in _worker_streams(dev, W):
+        free.put(st)
+    grad_on = torch.is_grad_enabled()
+
+    def solve(i):
+        st = free.get()
+        try:
+            with torch.cuda.device(dev), torch.cuda.stream(st), torch.set_grad_enabled(grad_on):
+                st.wait_event(ready)
+                P = splr_ot(M[i], a[i], b[i], eta=eta, **kwargs)
+                done = st.record_event()
+            return P, done
+        finally:
+            free.put(st)
+
+    with ThreadPoolExecutor(max_workers=W) as ex:
+        results = [f.result() for f in [ex.submit(solve, i) for i in range(B)]]
+    for P, done in results:
+        main.wait_event(done)
+        P.record_stream(main)  # the plan is consumed on the caller's stream
+    return torch.stack([P for P, _ in results])
 
 
 class SPLROT(torch.nn.Module):

@@ -5,6 +5,7 @@
     python -m curegot_backward_b200.profile_cases backward --n 2048 --m 2560
     python -m curegot_backward_b200.profile_cases precision --n 16384 --algo splr
     python -m curegot_backward_b200.profile_cases points --n 16384 --m 16384 --d 32 --iters 20
+    python -m curegot_backward_b200.profile_cases batch --n 512 --m 640 --batch 16
 
 Each case builds a seeded synthetic problem on cuda:0, runs it once to warm
 up, then times `--reps` runs with CUDA events on the launching stream and
@@ -20,6 +21,8 @@ point clouds on the tensor cores (never stored) for a fixed iteration
 count, and, with --compare, the stored-cost passes on the same cost;
 throughput is reported as cost elements per second (one exponential
 each) against the nominal SFU rate of 148 SMs x 16 ex2/clk x 1.965 GHz.
+The batch case times splr_ot_batch (forward and backward of a weighted sum
+of the plans) against one splr_ot call per problem in a loop.
 The precision case solves the precision-form problem (X, Y ~ N(0, I_32),
 M = |x - y|^2 / median stored in FP32, Dirichlet(1) marginals floored at
 1e-7, eta = 1e-3) in mixed precision once and reports its time, iterations
@@ -188,9 +191,40 @@ def case_points(a):
     return res
 
 
+def case_batch(a):
+    import curegot_backward_b200 as cg
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device=dev).manual_seed(a.seed)
+    B, n, m = a.batch, a.n, a.m
+    X = torch.rand(B, n, a.d, generator=g, device=dev, dtype=torch.float64)
+    Y = torch.rand(B, m, a.d, generator=g, device=dev, dtype=torch.float64)
+    M = ((X[:, :, None, :] - Y[:, None, :, :]) ** 2).mean(-1)
+    am = torch.full((B, n), 1.0 / n, dtype=torch.float64, device=dev)
+    bm = torch.full((B, m), 1.0 / m, dtype=torch.float64, device=dev)
+    W = torch.rand(B, n, m, generator=g, device=dev, dtype=torch.float64)
+
+    def batched():
+        Mr = M.clone().requires_grad_(True)
+        (cg.torch.splr_ot_batch(Mr, am, bm, eta=a.eta, tol=a.tol) * W).sum().backward()
+        return Mr.grad
+
+    def loop():
+        Mr = M.clone().requires_grad_(True)
+        T = torch.stack([cg.torch.splr_ot(Mr[i], am[i], bm[i], eta=a.eta, tol=a.tol)
+                         for i in range(B)])
+        (T * W).sum().backward()
+        return Mr.grad
+
+    ms_b, gb = _time(batched, a.reps)
+    ms_l, gl = _time(loop, a.reps)
+    return {"case": "batch", "batch": B, "n": n, "m": m, "eta": a.eta, "tol": a.tol,
+            "ms_batch": ms_b, "ms_loop": ms_l, "speedup": ms_l / ms_b,
+            "grads_bitwise_equal": bool(torch.equal(gb, gl))}
+
+
 def main(argv=None):
     p = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    p.add_argument("case", choices=["bcd", "splr", "backward", "precision", "points"])
+    p.add_argument("case", choices=["bcd", "splr", "backward", "precision", "points", "batch"])
     p.add_argument("--n", type=int, default=8192)
     p.add_argument("--m", type=int, default=8192)
     p.add_argument("--d", type=int, default=16)
@@ -208,9 +242,10 @@ def main(argv=None):
     p.add_argument("--algo", default="splr", choices=["bcd", "splr"], help="precision case")
     p.add_argument("--max-iter", type=int, default=100000, help="precision case")
     p.add_argument("--compare", action="store_true", help="points: also time the stored cost")
+    p.add_argument("--batch", type=int, default=16, help="batch case: problems per batch")
     a = p.parse_args(argv)
     res = {"bcd": case_bcd, "splr": case_splr, "backward": case_backward,
-           "precision": case_precision, "points": case_points}[a.case](a)
+           "precision": case_precision, "points": case_points, "batch": case_batch}[a.case](a)
     print(json.dumps(res), flush=True)
 
 

@@ -114,3 +114,33 @@ def test_autograd_error_contract(cuda_dev):
     Tb = cg.torch.splr_ot_batch(torch.stack([Mt, Mt]), torch.stack([at, at]),
                                 torch.stack([bt, bt]), eta=0.05, tol=1e-7)
     assert torch.equal(Tb[0], T1) and torch.equal(Tb[1], T1)
+
+
+@pytest.mark.parametrize("B", [3, 11])
+def test_batch_concurrent_matches_sequential(B):
+    """splr_ot_batch runs its solves concurrently on worker streams; plans and
+    gradients must be bitwise those of one splr_ot call per problem."""
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device=dev).manual_seed(100 + B)
+    n, m = 160, 120
+    X = torch.rand(B, n, 8, generator=g, device=dev, dtype=torch.float64)
+    Y = torch.rand(B, m, 8, generator=g, device=dev, dtype=torch.float64)
+    M = ((X[:, :, None, :] - Y[:, None, :, :]) ** 2).mean(-1)
+    a = torch.rand(B, n, generator=g, device=dev, dtype=torch.float64) + 0.5
+    b = torch.rand(B, m, generator=g, device=dev, dtype=torch.float64) + 0.5
+    a, b = a / a.sum(1, keepdim=True), b / b.sum(1, keepdim=True)
+    W = torch.rand(B, n, m, generator=g, device=dev, dtype=torch.float64)
+
+    Mb = M.clone().requires_grad_(True)
+    Tb = cg.torch.splr_ot_batch(Mb, a, b, eta=0.05, tol=1e-8)
+    (Tb * W).sum().backward()
+
+    Ms = M.clone().requires_grad_(True)
+    Ts = torch.stack([cg.torch.splr_ot(Ms[i], a[i], b[i], eta=0.05, tol=1e-8) for i in range(B)])
+    (Ts * W).sum().backward()
+
+    assert torch.equal(Tb, Ts)
+    assert torch.equal(Mb.grad, Ms.grad)
+    with torch.no_grad():
+        Tn = cg.torch.splr_ot_batch(M, a, b, eta=0.05, tol=1e-8)
+    assert Tn.grad_fn is None and torch.equal(Tn, Ts.detach())
