@@ -80,11 +80,11 @@ def _device_operands(M, a, b, precision):
     want = torch.float32 if precision == "mixed" else torch.float64
     if M.dtype != want:
         raise TypeError(f"{precision} solve needs M as {want}, got {M.dtype}")
+    if a.dtype != torch.float64 or b.dtype != torch.float64:
+        raise TypeError("a and b must be float64")
     for t in (M, a, b):
         if not t.is_cuda or not t.is_contiguous() or t.device != M.device:
             raise ValueError("M, a and b must be contiguous tensors on one CUDA device")
-    if a.dtype != torch.float64 or b.dtype != torch.float64:
-        raise TypeError("a and b must be float64")
     if M.dim() != 2 or a.numel() != M.shape[0] or b.numel() != M.shape[1]:
         raise ValueError("shapes of M, a and b do not agree")
 
