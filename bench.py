@@ -80,7 +80,7 @@ def dist_setup(args):
         import datetime
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
     elif torch.cuda.is_available():
         torch.cuda.set_device(0)
     return world, rank, local
@@ -92,24 +92,24 @@ def barrier(world):
         dist.barrier()
 
 
-def max_over_ranks(x, world):
+def _reduce_over_ranks(x, world, op_name):
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    # NCCL reduces device tensors; gloo (the CPU test harness) host tensors
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=getattr(dist.ReduceOp, op_name))
     return float(t.item())
+
+
+def max_over_ranks(x, world):
+    return _reduce_over_ranks(x, world, "MAX")
 
 
 def sum_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce_over_ranks(x, world, "SUM")
 
 
 # ---------------------------------------------------------------------------
