@@ -43,6 +43,8 @@ if ROOT not in sys.path:
 
 METRIC = "solves/s + p99 latency, mixed-size OT stream @1e-8 marginal err, vs plain FP64"
 TOL = 1e-8
+WORKLOAD = ("serving stream: n,m log-uniform [64,8192], d in {8,32}, Gaussian clouds/max, "
+            "eta in {0.1,0.05,0.01}, 70% BCD / 30% SPLR, tol 1e-8, uniform marginals")
 TRAFFIC_RATIO_F32 = 1.025
 SPLR_WORKERS = 16
 IN_FLIGHT = 24
@@ -384,9 +386,7 @@ def reference_arm(args, world, rank):
             "ms_per_step": 1000.0 * args.requests / value if value else None,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": "serving stream: n,m log-uniform [64,8192], d in {8,32}, "
-                                   "Gaussian clouds/max, eta in {0.1,0.05,0.01}, 70% BCD / 30% "
-                                   "SPLR, tol 1e-8", "requests_per_step": args.requests},
+            "config": {"workload": WORKLOAD, "requests_per_step": args.requests},
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": oracle.num_threads(),
                              "kind": "port", "sample": desc},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
@@ -502,9 +502,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / max(args.steps, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32-M/f64", "data": "synthetic",
-            "config": {"workload": "serving stream: n,m log-uniform [64,8192], d in {8,32}, "
-                                   "Gaussian clouds/max, eta in {0.1,0.05,0.01}, 70% BCD / 30% "
-                                   "SPLR, tol 1e-8, uniform marginals",
+            "config": {"workload": WORKLOAD,
                        "requests_per_step": args.requests,
                        "arrivals": (f"poisson {args.rate}/s, one stream over the timed steps" if args.rate else
                                     f"saturation: closed loop over the timed steps' {n_req} requests, "
