@@ -24,6 +24,8 @@ CG_ERR_NONFINITE = 6
 CG_ERR_INVALID_CONTEXT = 7
 CG_ERR_SOLVER = 8
 CG_ERR_ADMISSION = 9
+CG_ERR_CANCELLED = 10
+CG_INJECT_DIRECTION_SOLVE = 1
 CG_POINTS_FP64 = 0
 CG_POINTS_MIXED = 1
 
@@ -37,6 +39,7 @@ _STATUS_NAMES = {
     CG_ERR_INVALID_CONTEXT: "invalid backward context",
     CG_ERR_SOLVER: "linear solver error",
     CG_ERR_ADMISSION: "request exceeds the engine's HBM budget",
+    CG_ERR_CANCELLED: "request cancelled",
 }
 
 _lib = None
@@ -110,6 +113,7 @@ SIGNATURES = {
     "cg_bcd_points_bf16": [c_void_p, c_void_p, c_int, c_int, c_int, c_double, c_void_p, c_void_p,
                            c_double, c_int, c_double, c_int, c_int_p, c_void_p, c_int_p,
                            c_void_p],
+    "cg_points_set_wait_limit": [ctypes.c_longlong],
     "cg_bcd_mixed": [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_double, c_int,
                      c_int, c_int_p, c_void_p, c_void_p, c_void_p],
     "cg_transport_plan_f64": [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_int,
@@ -139,6 +143,8 @@ SIGNATURES = {
     "cg_engine_submit": [c_void_p, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)],
     "cg_engine_poll": [c_void_p, ctypes.POINTER(Result), c_int, c_int, c_int_p],
     "cg_engine_stats": [c_void_p, ctypes.POINTER(EngineStats)],
+    "cg_engine_cancel": [c_void_p, ctypes.c_uint64],
+    "cg_test_inject_failure": [c_int, c_int],
     "cg_engine_clock": [],
     "cg_engine_destroy": [c_void_p],
 }

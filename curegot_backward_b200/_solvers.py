@@ -261,6 +261,12 @@ def torch_sinkhorn_splr_bwd(M, a, b, reg, tol=1e-6, max_iter=1000, verbose=0, **
     context_mode = kwargs.get("context_mode", "adopt")
     if context_mode not in ("adopt", "snapshot"):
         raise RuntimeError('context_mode must be "adopt" or "snapshot"')
+    if context_mode == "snapshot":
+        # The reference's "snapshot" mode (backward_context.cu:306-442) copies
+        # and re-factors the forward state for benchmarking and debugging;
+        # the production mode, and the only one provided here, is "adopt".
+        raise NotImplementedError('context_mode="snapshot" is a benchmark/debug mode of the '
+                                  'reference and is not provided; use context_mode="adopt"')
     out = _splr_device(Md, ad, bd, reg, tol, max_iter, verbose, x0, precision, dmax, smax,
                        cycle, cand, want_ctx=True,
                        trace=bool(kwargs.get("return_trace", False)))

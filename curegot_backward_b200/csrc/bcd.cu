@@ -295,7 +295,12 @@ __device__ __forceinline__ void row_block(const BcdProb* __restrict__ probs,
       const double err = sqrt(tot);
       st->last_err = err;
       st->check_pending = 0;
-      if (!fast) {
+      if (!isfinite(err)) {
+        // non-finite marginal: no later iterate can pass the test
+        st->done = 1;
+        st->nonfinite = 1;
+        st->niter = t;
+      } else if (!fast) {
         if (err < st->tol) {
           st->done = 1;
           st->niter = t;
@@ -515,6 +520,10 @@ __device__ __forceinline__ void col_block(const BcdProb* __restrict__ probs,
       const double diff = sqrt(am2 + an * ea * ea + bm2 + bn * eb * eb);
       st->last_err = diff;
       if (diff < st->tol * 10) st->phase = 2;
+      if (!isfinite(diff)) {
+        st->done = 1;
+        st->nonfinite = 1;
+      }
     }
   } else if (phase == 2 && threadIdx.x == 0) {
     st->check_pending = 1;

@@ -26,7 +26,7 @@ struct BcdState {
   double best_est;    // mixed precision: best fast marginal estimate
   double stat_a[3];   // (count, mean, M2) of alpha^{t+1} - alpha^t
   int fast_iters;     // iterations run with SFU passes
-  int pad_;
+  int nonfinite;      // a stop-test value was NaN / Inf (non-finite M, a, b or x0): done
 };
 
 struct BcdProb {

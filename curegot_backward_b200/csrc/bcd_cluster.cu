@@ -55,7 +55,7 @@ constexpr size_t kBandTarget = 48 * 1024; // preferred bytes of M per CTA
 constexpr size_t kClusterMaxBytes = 768 * 1024;
 
 struct Ctrl {
-  int iter, phase, check_pending, done, niter, fast, stall, fast_iters;
+  int iter, phase, check_pending, done, niter, fast, stall, fast_iters, nonfinite;
   double best_est, last_err, stat_a[3];
 };
 
@@ -239,6 +239,7 @@ __global__ void __launch_bounds__(kCT, 1) bcd_cluster_kernel(const ClusterProb* 
     c.fast = (sizeof(TM) == 4) ? 1 : 0;
     c.stall = 0;
     c.fast_iters = 0;
+    c.nonfinite = 0;
     c.best_est = INFINITY;
     c.last_err = 0.0;
     c.stat_a[0] = c.stat_a[1] = c.stat_a[2] = 0.0;
@@ -344,7 +345,11 @@ __global__ void __launch_bounds__(kCT, 1) bcd_cluster_kernel(const ClusterProb* 
         const double err = sqrt(tot);
         c.last_err = err;
         c.check_pending = 0;
-        if (!fast_row) {
+        if (!isfinite(err)) {
+          c.done = 1;
+          c.nonfinite = 1;
+          c.niter = t;
+        } else if (!fast_row) {
           if (err < P.tol) {
             c.done = 1;
             c.niter = t;
@@ -439,6 +444,10 @@ __global__ void __launch_bounds__(kCT, 1) bcd_cluster_kernel(const ClusterProb* 
         const double diff = sqrt(am2 + an * ea * ea + bm2 + bn * eb * eb);
         c.last_err = diff;
         if (diff < P.tol * 10) c.phase = 2;
+        if (!isfinite(diff)) {
+          c.done = 1;
+          c.nonfinite = 1;
+        }
       } else if (phase == 2) {
         c.check_pending = 1;
       }
@@ -476,6 +485,7 @@ __global__ void __launch_bounds__(kCT, 1) bcd_cluster_kernel(const ClusterProb* 
     st->stat_a[1] = c.stat_a[1];
     st->stat_a[2] = c.stat_a[2];
     st->fast_iters = c.fast_iters;
+    st->nonfinite = c.nonfinite;
   }
 }
 

@@ -140,7 +140,10 @@ static int splr_entry(bool f32, const void* M, const double* a, const double* b,
                       double density_max, double shift_max, int cycle, int cand_iter,
                       int verbose, const double* x0, double* dual, cg_ctx** ctx_out,
                       int* converged, double* trace, cudaStream_t stream) {
-  cg::SplrParams prm{reg, tol, max_iter, density_max, shift_max, cycle, cand_iter, verbose};
+  // FP64: the reference's stopping test (parity).  Mixed precision (an
+  // addition of this library): the full marginal error, gauge column included.
+  cg::SplrParams prm{reg, tol, max_iter, density_max, shift_max, cycle, cand_iter, verbose,
+                     f32 ? 1 : 0};
   cg_ctx_s* c = nullptr;
   int rc;
   if (f32)

@@ -32,6 +32,7 @@
 #include <memory>
 #include <mutex>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "bcd.cuh"
@@ -78,6 +79,7 @@ struct Req {
   BcdProb prob{};
   int slot = -1;
   int cls = 0;  // Sinkhorn batch: 0 small, 1 large
+  std::atomic<bool> cancel{false};  // set by cg_engine_cancel while admitted
 };
 
 size_t bcd_footprint(const cg_request_t& r, BcdProb& geo, int sms) {
@@ -136,6 +138,7 @@ __global__ void engine_init_kernel(const double* a, const double* b, int n, int 
     st->best_est = INFINITY;
     st->stat_a[0] = st->stat_a[1] = st->stat_a[2] = 0.0;
     st->fast_iters = 0;
+    st->nonfinite = 0;
   }
 }
 
@@ -166,6 +169,7 @@ struct cg_engine_s {
   bool stop = false;
   uint64_t next_id = 1;
   std::deque<cg::Req*> bcd_qs[2], splr_q;  // Sinkhorn batches: small, large
+  std::unordered_map<uint64_t, cg::Req*> live;  // submitted, not yet finished (guarded by mu)
   int n_workers = 0;
   std::mutex stat_mu;  // guards the statistics below (two batch threads)
   std::vector<cg::Req*> done;
@@ -195,6 +199,7 @@ void release(cg_engine_s* E, size_t bytes) {
 void finish(cg_engine_s* E, Req* q) {
   q->t_done = now_s();
   std::lock_guard<std::mutex> lk(E->mu);
+  E->live.erase(q->id);
   E->done.push_back(q);
   E->n_done++;
   E->cv.notify_all();
@@ -290,6 +295,23 @@ void bcd_loop(cg_engine_s* E, int cls) {
   bool dirty = true;
   int row_total = 0, col_total = 0;
   double batch_bytes_per_tick = 0.0;
+  // Ends every admitted problem of this batch with status rc (used when the
+  // batch description cannot be allocated): their blocks are released
+  // stream-ordered after the work already queued on the batch stream.
+  auto fail_batch = [&](int rc) {
+    host_wait(st);
+    for (Req* q : active) {
+      if (q->block) cudaFreeAsync(q->block, st);
+      q->block = nullptr;
+      q->status = rc;
+      release(E, q->footprint);
+      finish(E, q);
+    }
+    active.clear();
+    E->active_bcd -= my_active;
+    my_active = 0;
+    dirty = true;
+  };
 
   while (true) {
     // ---- admission --------------------------------------------------------
@@ -364,15 +386,56 @@ void bcd_loop(cg_engine_s* E, int cls) {
         const int nc = active[k]->prob.col_strips * active[k]->prob.col_splits;
         for (int c = 0; c < nc; ++c) cp[co++] = k;
       }
-      if ((size_t)P > cap_probs) {
-        if (d_probs) cudaFreeAsync(d_probs, st);
-        cap_probs = std::max<size_t>(P, 2 * cap_probs);
-        pool_alloc_async(reinterpret_cast<void**>(&d_probs), cap_probs * sizeof(BcdProb), st);
-      }
-      if (h_map.size() > cap_map) {
-        if (d_map) cudaFreeAsync(d_map, st);
-        cap_map = std::max<size_t>(h_map.size(), 2 * cap_map);
-        pool_alloc_async(reinterpret_cast<void**>(&d_map), cap_map * sizeof(int), st);
+      // Regrow the batch description buffers into temporaries: the old
+      // blocks and capacities stay in place unless every allocation
+      // succeeded, so an allocation failure never leaves a stale pointer.
+      if ((size_t)P > cap_probs || h_map.size() > cap_map || (size_t)P > cap_states) {
+        const size_t np_cap = (size_t)P > cap_probs ? std::max<size_t>(P, 2 * cap_probs) : 0;
+        const size_t nm_cap = h_map.size() > cap_map ? std::max<size_t>(h_map.size(), 2 * cap_map) : 0;
+        const size_t ns_cap = (size_t)P > cap_states ? std::max<size_t>(P, 2 * cap_states) : 0;
+        BcdProb* n_probs = nullptr;
+        int* n_map = nullptr;
+        BcdState* n_dst = nullptr;
+        BcdState* n_hst = nullptr;
+        bool ok = true;
+        if (np_cap) ok = ok && pool_alloc_async(reinterpret_cast<void**>(&n_probs),
+                                                np_cap * sizeof(BcdProb), st) == CG_OK;
+        if (nm_cap) ok = ok && pool_alloc_async(reinterpret_cast<void**>(&n_map),
+                                                nm_cap * sizeof(int), st) == CG_OK;
+        if (ns_cap) {
+          ok = ok && pool_alloc_async(reinterpret_cast<void**>(&n_dst), ns_cap * sizeof(BcdState),
+                                      st) == CG_OK;
+          ok = ok && cudaHostAlloc(reinterpret_cast<void**>(&n_hst), ns_cap * sizeof(BcdState),
+                                   cudaHostAllocDefault) == cudaSuccess;
+        }
+        if (!ok) {
+          cudaGetLastError();
+          if (n_probs) cudaFreeAsync(n_probs, st);
+          if (n_map) cudaFreeAsync(n_map, st);
+          if (n_dst) cudaFreeAsync(n_dst, st);
+          if (n_hst) cudaFreeHost(n_hst);
+          set_last_error("engine: batch description allocation failed", __FILE__, __LINE__);
+          fail_batch(CG_ERR_OOM);
+          continue;
+        }
+        if (n_probs) {
+          if (d_probs) cudaFreeAsync(d_probs, st);
+          d_probs = n_probs;
+          cap_probs = np_cap;
+        }
+        if (n_map) {
+          if (d_map) cudaFreeAsync(d_map, st);
+          d_map = n_map;
+          cap_map = nm_cap;
+        }
+        if (n_dst) {
+          host_wait(st);  // the previous pinned block may still be a copy target
+          if (d_states) cudaFreeAsync(d_states, st);
+          if (h_states) cudaFreeHost(h_states);
+          d_states = n_dst;
+          h_states = n_hst;
+          cap_states = ns_cap;
+        }
       }
       cudaMemcpyAsync(d_probs, h_probs.data(), P * sizeof(BcdProb), cudaMemcpyHostToDevice, st);
       cudaMemcpyAsync(d_map, h_map.data(), h_map.size() * sizeof(int), cudaMemcpyHostToDevice,
@@ -413,14 +476,6 @@ void bcd_loop(cg_engine_s* E, int cls) {
         std::lock_guard<std::mutex> sl(E->stat_mu);
         E->graph_builds++;
       }
-      if ((size_t)P > cap_states) {
-        if (h_states) cudaFreeHost(h_states);
-        if (d_states) cudaFreeAsync(d_states, st);
-        cap_states = std::max<size_t>(P, 2 * cap_states);
-        cudaHostAlloc(reinterpret_cast<void**>(&h_states), cap_states * sizeof(BcdState),
-                      cudaHostAllocDefault);
-        pool_alloc_async(reinterpret_cast<void**>(&d_states), cap_states * sizeof(BcdState), st);
-      }
       dirty = false;
     }
     // ---- run one chunk ------------------------------------------------------
@@ -458,17 +513,27 @@ void bcd_loop(cg_engine_s* E, int cls) {
       active[k]->niter = h_states[k].iter;
     }
     stat_lk.unlock();
-    // ---- retire finished problems -----------------------------------------
+    // ---- retire finished (or cancelled) problems -----------------------------
     std::vector<Req*> keep;
+    std::vector<char> retire(P, 0);
     for (int k = 0; k < P; ++k) {
       Req* q = active[k];
       const BcdState& s = h_states[k];
-      if (!s.done) {
+      const bool cancelled = !s.done && q->cancel.load(std::memory_order_relaxed);
+      if (!s.done && !cancelled) {
         keep.push_back(q);
         continue;
       }
+      retire[k] = 1;
+      dirty = true;
+      if (cancelled) {
+        q->status = CG_ERR_CANCELLED;
+        continue;
+      }
       q->niter = s.niter;
-      q->converged = (s.niter < s.max_iter) || (s.phase == 2 && s.last_err < s.tol && !s.fast);
+      if (s.nonfinite) q->status = CG_ERR_NONFINITE;
+      q->converged = !s.nonfinite &&
+                     ((s.niter < s.max_iter) || (s.phase == 2 && s.last_err < s.tol && !s.fast));
       q->fast_iters = s.fast_iters;
       q->last_err = s.last_err;
       // duals -> output (device or host)
@@ -479,13 +544,12 @@ void bcd_loop(cg_engine_s* E, int cls) {
         cudaMemcpyAsync(q->r.dual_out, q->ddual, 8 * (size_t)(q->r.n + q->r.m),
                         q->r.host_inputs ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, st);
       }
-      dirty = true;
     }
     if (dirty) {
       host_wait(st);
       for (int k = 0; k < P; ++k) {
+        if (!retire[k]) continue;
         Req* q = active[k];
-        if (!h_states[k].done) continue;
         cudaFreeAsync(q->block, st);
         q->block = nullptr;
         release(E, q->footprint);
@@ -562,8 +626,11 @@ void splr_loop(cg_engine_s* E) {
         db = dab + n;
       }
       ddual = reinterpret_cast<double*>(p + inb);
+      // the engine stops on the full marginal error, so every SPLR result
+      // meets tol on rows and on all m columns (the reference's test leaves
+      // the gauge column out)
       SplrParams prm{r.eta, r.tol, r.max_iter, std::min(10.0 / std::min(n, m), 1.0), 1e-3, 30, 3,
-                     0};
+                     0, 1, &q->cancel};
       int niter = 0, conv = 0;
       if (r.m_f32)
         rc = splr_solve<float>(static_cast<const float*>(dM), da, db, nullptr, n, m, prm, nullptr,
@@ -573,6 +640,13 @@ void splr_loop(cg_engine_s* E) {
                                 nullptr, ddual, &niter, &conv, nullptr, nullptr, st);
       q->niter = niter;
       q->converged = conv;
+      // the SPLR loop ends early without converging only on a non-finite
+      // objective or gradient norm (the reference's break, sinkhorn_splr.cu:1128)
+      if (rc == CG_OK && !conv && niter < r.max_iter) {
+        set_last_error("engine: SPLR objective or gradient became non-finite", __FILE__,
+                       __LINE__);
+        rc = CG_ERR_NONFINITE;
+      }
       if (rc == CG_OK && r.dual_out)
         cudaMemcpyAsync(r.dual_out, ddual, 8 * (size_t)(n + m),
                         r.host_inputs ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, st);
@@ -634,6 +708,7 @@ int cg_engine_submit(cg_engine* eng, const cg_request_t* req, uint64_t* id) {
   {
     std::lock_guard<std::mutex> lk(E->mu);
     q->id = E->next_id++;
+    E->live[q->id] = q;
     if (req->algo == CG_ALGO_BCD) E->bcd_qs[q->cls].push_back(q);
     else E->splr_q.push_back(q);
   }
@@ -666,6 +741,34 @@ int cg_engine_poll(cg_engine* eng, cg_result_t* results, int capacity, int wait_
   }
   E->done.erase(E->done.begin(), E->done.begin() + k);
   *count = k;
+  return CG_OK;
+}
+
+int cg_engine_cancel(cg_engine* eng, uint64_t id) {
+  if (!eng) return CG_ERR_INVALID_ARG;
+  cg_engine_s* E = reinterpret_cast<cg_engine_s*>(eng);
+  std::unique_lock<std::mutex> lk(E->mu);
+  auto it = E->live.find(id);
+  if (it == E->live.end()) {
+    cg::set_last_error("cg_engine_cancel: unknown or finished request", __FILE__, __LINE__);
+    return CG_ERR_INVALID_ARG;
+  }
+  cg::Req* q = it->second;
+  for (auto* dq : {&E->bcd_qs[0], &E->bcd_qs[1], &E->splr_q}) {
+    auto pos = std::find(dq->begin(), dq->end(), q);
+    if (pos == dq->end()) continue;
+    // still queued: nothing of it is on the device
+    dq->erase(pos);
+    q->status = CG_ERR_CANCELLED;
+    q->t_done = cg::now_s();
+    E->live.erase(it);
+    E->done.push_back(q);
+    E->n_done++;
+    lk.unlock();
+    E->cv.notify_all();
+    return CG_OK;
+  }
+  q->cancel.store(true);  // admitted: its scheduler ends it
   return CG_OK;
 }
 

@@ -38,6 +38,7 @@
 // Both passes use the same operand roles (the updated side as MMA operand A)
 // and the same K order, so row and column passes see identical M_ij.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 
@@ -59,6 +60,9 @@ constexpr int kPtsLseMinBlocks = CG_PTS_MINB;  // resident CTAs per SM (64 regis
 constexpr int kPtsMaxD = 64;      // padded feature dimension (multiple of 16)
 constexpr int kPtsTmemCols = 128;
 constexpr long kPtsSpinLimit = 1L << 24;  // mbarrier polls before giving up
+// Poll limit of the first tensor-core completion wait of each tile
+// (cg_points_set_wait_limit); the drain wait after a timeout keeps the full limit.
+std::atomic<long> g_pts_first_wait{kPtsSpinLimit};
 constexpr int kPtsChunk = 8;      // iterations per host check
 
 // Operand tile in shared memory: kPtsTile rows x D BF16, canonical K-major
@@ -113,9 +117,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity; false after the limit.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (long it = 0; it < kPtsSpinLimit; ++it)
+// Bounded wait for the phase with the given parity; false after `limit`
+// polls (limit 0: give up without polling).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          long limit = kPtsSpinLimit) {
+  for (long it = 0; it < limit; ++it)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -230,9 +236,11 @@ __device__ __forceinline__ void pts_teardown(PtsShared& sh) {
 }
 
 // One column tile: stage B, MMA into TMEM, wait.  Returns false when the
-// wait gave up (the accumulator is then not read).
+// wait gave up (the accumulator is then not read).  first_wait bounds the
+// completion wait; whatever it is, a wait that gave up is followed by one at
+// the full limit, so the MMAs have drained before TMEM can be freed.
 __device__ __forceinline__ bool pts_tile_mma(PtsShared& sh, const char* tA, char* tB, int D,
-                                             uint32_t& phase) {
+                                             uint32_t& phase, long first_wait) {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   tc_fence_before();
   __syncthreads();
@@ -244,7 +252,7 @@ __device__ __forceinline__ bool pts_tile_mma(PtsShared& sh, const char* tA, char
                umma_desc(b0 + s * kSliceBytes, 128, 256), s > 0 ? 1u : 0u);
     mma_commit(&sh.bar);
   }
-  bool ok = mbar_wait(&sh.bar, phase);
+  bool ok = mbar_wait(&sh.bar, phase, first_wait);
   ok = __syncthreads_and(ok) != 0;
   if (!ok) mbar_wait(&sh.bar, phase);  // bounded: let the MMAs drain before TMEM is freed
   phase ^= 1u;
@@ -263,7 +271,7 @@ __device__ __forceinline__ float pts_cost(float dot, float nr, float nc, float s
 __global__ void __launch_bounds__(kPtsThreads) pts_cost_kernel(
     const uint16_t* __restrict__ P, const uint16_t* __restrict__ Q, const float* __restrict__ nP,
     const float* __restrict__ nQ, int rows, int cols, int D, float scale, float* __restrict__ M,
-    int* __restrict__ error) {
+    int* __restrict__ error, long first_wait) {
   extern __shared__ __align__(1024) char smem[];
   __shared__ PtsShared sh;
   char* tA = smem;
@@ -273,7 +281,7 @@ __global__ void __launch_bounds__(kPtsThreads) pts_cost_kernel(
   stage_tile(P, rows, D, r0, tA);
   stage_tile(Q, cols, D, c0, tB);
   uint32_t phase = 0;
-  const bool ok = pts_tile_mma(sh, tA, tB, D, phase);
+  const bool ok = pts_tile_mma(sh, tA, tB, D, phase, first_wait);
   if (!ok) {
     if (threadIdx.x == 0) atomicExch(error, 1);
   } else {
@@ -304,7 +312,8 @@ __global__ void __launch_bounds__(kPtsLseThreads, kPtsLseMinBlocks) pts_lse_kern
     const uint16_t* __restrict__ P, const uint16_t* __restrict__ Q, const float* __restrict__ nP,
     const float* __restrict__ nQ, int rows, int cols, int D, float scale,
     const double* __restrict__ xs_base, size_t xs_stride, int xs_parity, double s2,
-    int tiles_per_split, double* __restrict__ part, int rows_pad, PtsState* __restrict__ st) {
+    int tiles_per_split, double* __restrict__ part, int rows_pad, PtsState* __restrict__ st,
+    long first_wait) {
   extern __shared__ __align__(1024) char smem[];
   __shared__ PtsShared sh;
   __shared__ double tab[kExp2TableSize];
@@ -344,7 +353,7 @@ __global__ void __launch_bounds__(kPtsLseThreads, kPtsLseMinBlocks) pts_lse_kern
       sx[c] = gc < cols ? xs[gc] : 0.0;
       sn[c] = gc < cols ? nQ[gc] : 0.0f;
     }
-    ok = pts_tile_mma(sh, tA, tB, D, phase);
+    ok = pts_tile_mma(sh, tA, tB, D, phase, first_wait);
     if (!ok) break;
 #pragma unroll 1
     for (int cb = half * 64; cb < half * 64 + 64; cb += 32) {
@@ -579,7 +588,8 @@ extern "C" int cg_points_cost_bf16(const uint16_t* X, const uint16_t* Y, int n, 
     { pts_pad_kernel<<<(m + 255) / 256, 256, 0, stream>>>(Y, m, d, D, Yp, nY); count_launch(); }
     dim3 grid((n + kPtsTile - 1) / kPtsTile, (m + kPtsTile - 1) / kPtsTile);
     { pts_cost_kernel<<<grid, kPtsThreads, kPtsSmemLaunch, stream>>>(
-        Xp, Yp, nX, nY, n, m, D, static_cast<float>(cost_scale), M, err); count_launch(); }
+        Xp, Yp, nX, nY, n, m, D, static_cast<float>(cost_scale), M, err,
+        g_pts_first_wait.load()); count_launch(); }
     if ((rc = status_from_cuda(cudaGetLastError())) != CG_OK) break;
     int herr = 0;
     if ((rc = read_device(&herr, err, sizeof(int), stream)) != CG_OK) break;
@@ -648,6 +658,7 @@ extern "C" int cg_bcd_points_bf16(const uint16_t* X, const uint16_t* Y, int n, i
 
   const double s2 = kLog2e / reg;
   const float sc = static_cast<float>(cost_scale);
+  const long first_wait = g_pts_first_wait.load();
   int rc = CG_OK;
   PtsState hs{};
   do {
@@ -664,12 +675,14 @@ extern "C" int cg_bcd_points_bf16(const uint16_t* X, const uint16_t* Y, int n, i
       for (int q = 0; q < todo; ++q) {
         // row side: alpha^{k+1} from beta^k
         { pts_lse_kernel<<<grow, kPtsLseThreads, kPtsSmemLaunch, stream>>>(
-            Xp, Yp, nX, nY, n, m, D, sc, bes, (size_t)m, 0, s2, tps_row, part, n_pad, st); count_launch(); }
+            Xp, Yp, nX, nY, n, m, D, sc, bes, (size_t)m, 0, s2, tps_row, part, n_pad, st,
+            first_wait); count_launch(); }
         { pts_merge_kernel<<<mb_n, 256, 0, stream>>>(part, n, n_pad, sp_row, reg, s2, loga, a, al, als,
                                                     (size_t)n, 1, cnt, berr, st); count_launch(); }
         // column side: beta^{k+1} from alpha^{k+1}
         { pts_lse_kernel<<<gcol, kPtsLseThreads, kPtsSmemLaunch, stream>>>(
-            Yp, Xp, nY, nX, m, n, D, sc, als, (size_t)n, 1, s2, tps_col, part, m_pad, st); count_launch(); }
+            Yp, Xp, nY, nX, m, n, D, sc, als, (size_t)n, 1, s2, tps_col, part, m_pad, st,
+            first_wait); count_launch(); }
         { pts_merge_kernel<<<mb_m, 256, 0, stream>>>(part, m, m_pad, sp_col, reg, s2, logb, b, be, bes,
                                                     (size_t)m, 0, cnt + 1, berr, st); count_launch(); }
       }
@@ -693,4 +706,9 @@ extern "C" int cg_bcd_points_bf16(const uint16_t* X, const uint16_t* Y, int n, i
   } while (false);
   W.release();
   return rc;
+}
+
+extern "C" int cg_points_set_wait_limit(long long polls) {
+  cg::g_pts_first_wait.store(polls < 0 ? cg::kPtsSpinLimit : (long)polls);
+  return CG_OK;
 }

@@ -186,6 +186,7 @@ __global__ void bcd_init_kernel(const double* __restrict__ a, const double* __re
     st->best_est = INFINITY;
     st->stat_a[0] = st->stat_a[1] = st->stat_a[2] = 0.0;
     st->fast_iters = 0;
+    st->nonfinite = 0;
   }
 }
 
@@ -214,6 +215,16 @@ __global__ void dual_from_state_kernel(const BcdState* st, const BcdProb* p, dou
   const int n = p->n, m = p->m;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += gridDim.x * blockDim.x)
     dual[i] = (i < n) ? al[i] : be[i - n];
+}
+
+// A stop-test value became NaN or Inf: M, a, b or x0 holds a non-finite
+// value (or log(a_i), log(b_j) of a zero marginal met an infinite cost).  The
+// reference keeps iterating to max_iter on NaN; here the solve stops at the
+// first non-finite test and reports it.
+static int bcd_nonfinite() {
+  set_last_error("cg_bcd: non-finite stopping-test value (non-finite M, a, b or x0)", __FILE__,
+                 __LINE__);
+  return CG_ERR_NONFINITE;
 }
 
 // Whole solve in one cluster-resident launch (problems up to ~3 MB of M).
@@ -245,6 +256,7 @@ int bcd_solve_cluster(int C, const TM* M, const double* a, const double* b, doub
   BcdState hs{};
   CG_TRY(read_device(&hs, hp.st, sizeof(BcdState), stream));
   *niter = hs.niter;
+  if (hs.nonfinite) return bcd_nonfinite();
   if (Pout) launch_plan<TM>(M, hp.dual, hp.dual + n, Pout, 1.0 / reg, n, m, stream);
   CG_TRY_CUDA(cudaGetLastError());
   ws.release();
@@ -331,6 +343,7 @@ int bcd_solve(const TM* M, const double* a, const double* b, double* Pout, doubl
     chunk = std::min(chunk * 2, 64);
   }
   *niter = hs.niter;
+  if (hs.nonfinite) return bcd_nonfinite();
 
   if (Pout) {
     const size_t total = (size_t)n * m;
@@ -483,6 +496,7 @@ int bcd_solve_noalloc(const double* M, const double* a, const double* b, double*
     chunk = std::min(chunk * 2, 64);
   }
   *niter = hs.niter;
+  if (hs.nonfinite) return bcd_nonfinite();
 
   if (Pout) {
     const size_t total = (size_t)n * m;

@@ -49,10 +49,15 @@ __device__ __forceinline__ Digit digit_of(int level) {
   }
 }
 
+// T_ij with its sign bit cleared.  T >= 0 for finite inputs, so this is the
+// value itself; a NaN (non-finite M or duals) may carry a sign bit, and the
+// radix select's value digits assume a clear one: with it cleared, the
+// histogram, count and emit passes all order every key the same way and the
+// selection holds exactly Ks entries.
 template <typename TM>
 __device__ __forceinline__ double t_at(const TM* __restrict__ M, int i, int j, int m, double as,
                                        double bs, double s2, const double* tab) {
-  return exp2_f64(fma(-ld1(M + (size_t)i * m + j), s2, as + bs), tab);
+  return fabs(exp2_f64(fma(-ld1(M + (size_t)i * m + j), s2, as + bs), tab));
 }
 
 __device__ __forceinline__ unsigned int flat_prime(int n, int H, int i, int j) {
@@ -296,19 +301,27 @@ __device__ long long block_exclusive_scan(const int* in, int len, int* out, long
   return total;
 }
 
+// Row pointers and per-row list starts from the counts.  A selection larger
+// than the buffers' capacity (not reachable when the count predicate and the
+// select agree) leaves a diagonal-only pattern and flags the select state, so
+// the emit pass writes nothing and every later kernel stays in bounds.
 __global__ void __launch_bounds__(1024) scan_kernel(const int* coltot, const int* rowtot, int n,
-                                                    int m, int* scratch_c, int* scratch_r,
-                                                    int* rowptr, int* ipt, long long* kout) {
+                                                    int m, long long kcap, int* scratch_c,
+                                                    int* scratch_r, int* rowptr, int* ipt,
+                                                    long long* kout, SelState* sel) {
   __shared__ long long sh[1024];
   const int m1 = m - 1;
   const long long K = block_exclusive_scan(coltot, m1, scratch_c, sh);
   block_exclusive_scan(rowtot, n, scratch_r, sh);
+  const bool over = K > kcap;
   for (int r = threadIdx.x; r <= n; r += blockDim.x) rowptr[r] = r;
-  for (int j = threadIdx.x; j < m1; j += blockDim.x) rowptr[n + j + 1] = n + scratch_c[j] + coltot[j] + j + 1;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) ipt[i] = scratch_r[i];
+  for (int j = threadIdx.x; j < m1; j += blockDim.x)
+    rowptr[n + j + 1] = over ? n + j + 1 : n + scratch_c[j] + coltot[j] + j + 1;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) ipt[i] = over ? 0 : scratch_r[i];
   if (threadIdx.x == 0) {
-    ipt[n] = (int)K;
-    *kout = K;
+    ipt[n] = over ? 0 : (int)K;
+    *kout = over ? 0 : K;
+    sel->pad = over ? 1 : 0;
   }
 }
 
@@ -326,6 +339,7 @@ __global__ void __launch_bounds__(kThreads) emit_kernel(
   load_exp2_table(tab);
   __syncthreads();
   const SelState S = *sel;
+  if (S.pad) return;  // capacity overflow flagged by scan_kernel: nothing to emit
   const int ct = blockIdx.x % coltiles, rt = blockIdx.x / coltiles;
   const int r0 = rt * kTile, r1 = min(n, r0 + kTile);
   const int c0 = ct * kTile;
@@ -496,7 +510,8 @@ static int select_and_build_t(const TM* M, const double* gamma, const double* ro
   }
   { prefix_rows_kernel<<<grid_for(n, 256, sms * 4), 256, 0, st>>>(w.rowcnt, w.rowtot, n,
                                                                  Te > 0 ? coltiles : 0); cg::count_launch(); }
-  { scan_kernel<<<1, 1024, 0, st>>>(w.coltot, w.rowtot, n, m, scr_c, scr_r, h.rowptr, h.ipt, w.kout); cg::count_launch(); }
+  { scan_kernel<<<1, 1024, 0, st>>>(w.coltot, w.rowtot, n, m, h.kcap, scr_c, scr_r, h.rowptr,
+                                   h.ipt, w.kout, w.sel); cg::count_launch(); }
   if (Te > 0)
     { emit_kernel<TM><<<rowtiles * coltiles, kThreads, 0, st>>>(
         M, gamma, n, m, s2, w.sel, w.colcnt, w.rowcnt, coltiles, h.rowptr, h.ipt, h.val, h.col,

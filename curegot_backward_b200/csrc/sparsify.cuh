@@ -30,7 +30,7 @@ struct SelState {
   int done;
   unsigned long long tv;      // final predicate: key > tv || (key == tv && idx' >= ti)
   unsigned int ti;
-  int pad;
+  int pad;                    // 1: the selection exceeded the CSR capacity (nothing emitted)
 };
 
 struct SparsifyWork {

@@ -44,6 +44,16 @@ constexpr int kMaxPeelRoundsUsed = 512;
 enum { kPathDense = 0, kPathSparse = 1, kPathPeel = 2 };
 
 std::atomic<int> g_dir_mode{kDirAuto};
+// Failure injection (cg_test_inject_failure): direction solves still to be
+// reported as failed, counted down by the solver threads that consume them.
+std::atomic<int> g_inject_dirsolve{0};
+
+bool take_injected_dirsolve_failure() {
+  int v = g_inject_dirsolve.load();
+  while (v > 0)
+    if (g_inject_dirsolve.compare_exchange_weak(v, v - 1)) return true;
+  return false;
+}
 thread_local int g_last_dir = -1;
 
 // ---------------------------------------------------------------------------
@@ -178,6 +188,7 @@ __global__ void bcd_seed_kernel(const double* beta_src, int zero, double* beta0,
     st->last_err = 0.0;
     st->best_est = 0.0;
     st->fast_iters = 0;
+    st->nonfinite = 0;
   }
 }
 
@@ -586,7 +597,10 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
   TResult tr{};
   CG_TRY(eval_at(gamma, grad, rows, cols, res, tr, nullptr));
   double objfn = tr.f, gnorm = tr.gnorm;
+  double gfull = tr.gfull;  // full marginal error, for the full_stop test
   const double gnorm_init = gnorm;
+  // the quantity the stopping test compares with tol
+  auto stop_norm = [&]() { return prm.full_stop ? gfull : gnorm; };
   double shift = std::min(gnorm, prm.shift_max);
   long long Kcur = 0;
 
@@ -693,9 +707,13 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
   bool low_rank = false, converged = false, invalid_state = false;
   int niter = 0;
   for (int iter = 0; iter < prm.max_iter; ++iter) {
+    if (prm.cancel && prm.cancel->load(std::memory_order_relaxed)) {
+      set_last_error("cg_splr: cancelled", __FILE__, __LINE__);
+      return CG_ERR_CANCELLED;
+    }
     if (prm.verbose >= 1)
       printf("iter = %d, objval = %.10g, ||grad|| = %.10g\n", iter, objfn, gnorm);
-    if (gnorm < prm.tol) {
+    if (stop_norm() < prm.tol) {
       converged = true;
       break;
     }
@@ -751,6 +769,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
                                  {&t_first, res, sizeof(TResult)}};
       CG_TRY(read_device_spans(spans, 3, st));
     }
+    if (take_injected_dirsolve_failure()) info2[0] = 1;  // host-side test hook
     if (sp_bad || info2[0] != 0 || info2[1] != 0) {
       set_last_error("direction solve: sparsified Hessian not positive definite", __FILE__,
                      __LINE__);
@@ -765,7 +784,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     bool first_pending = true;  // t_first not yet consumed
     int trials = 0;
     double step_out = 0.0;
-    double last_trial_gnorm = gnorm;
+    double last_trial_gnorm = gnorm, last_trial_gfull = gfull;
     {
       const double c1 = 1e-4, c2 = 0.9;
       const int ls_max = 20;
@@ -805,6 +824,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
           dg = t.dg;
           objfn = fx;
           last_trial_gnorm = t.gnorm;
+          last_trial_gfull = t.gfull;
           const double psit = fx - fx_init - step * test_decr;
           const double dpsit = dg - test_decr;
           if (psit <= 0.0 && std::fabs(dg) <= test_curv) { step_out = step; done = true; break; }
@@ -878,8 +898,10 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
       }
       objfn = t.f;
       gnorm = t.gnorm;
+      gfull = t.gfull;
     } else {
       gnorm = last_trial_gnorm;  // f, g and ||g|| of the last trial are current
+      gfull = last_trial_gfull;
     }
 
     bool cand_accepted = false;
@@ -891,6 +913,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
         CG_TRY(eval_at(gamma, grad, rows, cols, res, t, nullptr));
         objfn = t.f;
         gnorm = t.gnorm;
+        gfull = t.gfull;
       }
     }
 
@@ -906,7 +929,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
       t[4] = low_rank; t[5] = recompute_fg; t[6] = cand_accepted; t[7] = trials;
     }
 
-    const bool converged_after = std::isfinite(gnorm) && (gnorm < prm.tol);
+    const bool converged_after = std::isfinite(stop_norm()) && (stop_norm() < prm.tol);
     const bool max_iter_reached = (iter + 1 >= prm.max_iter);
     const bool invalid_after = !std::isfinite(objfn) || !std::isfinite(gnorm);
     const bool stop_after = converged_after || max_iter_reached || invalid_after;
@@ -1011,5 +1034,15 @@ int cg_splr_set_direction_solver(int mode) {
 }
 
 int cg_splr_last_direction_solver(void) { return cg::g_last_dir; }
+
+int cg_test_inject_failure(int what, int count) {
+  if (what != CG_INJECT_DIRECTION_SOLVE || count < 0) {
+    cg::set_last_error("cg_test_inject_failure: unknown failure kind or negative count", __FILE__,
+                       __LINE__);
+    return CG_ERR_INVALID_ARG;
+  }
+  cg::g_inject_dirsolve.store(count);
+  return CG_OK;
+}
 
 }  // extern "C"

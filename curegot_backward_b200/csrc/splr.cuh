@@ -2,6 +2,8 @@
 // adjoint (PCG) solver.
 #pragma once
 
+#include <atomic>
+
 #include "schur.cuh"
 #include "peel.cuh"
 #include "spchol.cuh"
@@ -29,6 +31,14 @@ struct SplrParams {
   int max_iter;
   double density_max, shift_max;
   int cycle, cand_iter, verbose;
+  // 0: stop on ||g|| < tol with g over the first n + m - 1 dual entries (the
+  // reference's test, sinkhorn_splr.cu:1128-1132); 1: stop on the full
+  // marginal error ||(T1 - a, T^T 1 - b)||_2 < tol, which adds the gauge
+  // column's error (the serving engine's per-result accuracy guarantee).
+  int full_stop = 0;
+  // set by another thread to stop the solve at the next iteration with
+  // CG_ERR_CANCELLED (the serving engine's request cancellation); may be null
+  const std::atomic<bool>* cancel = nullptr;
 };
 
 // The SPLR solve (splr.cu).  M is float (mixed) or double; everything else FP64.

@@ -150,17 +150,18 @@ __global__ void __launch_bounds__(kThreads, 3) tpass_kernel(const TPassArgs A) {
     s_g2 = cta_sum(s_g2, red);
     s_gd = cta_sum(s_gd, red);
     if (threadIdx.x == 0) {
-      double* o = A.scal + (size_t)split * 4;
+      double* o = A.scal + (size_t)split * kTScal;
       o[0] = s_r;
       o[1] = s_aa;
       o[2] = s_g2;
       o[3] = s_gd;
+      o[4] = 0.0;
     }
     if (elect_last(cnt_all, nfin)) final_role = true;
   }
   // Column finisher: columns of this strip.
   if (elect_last(&cnt_strip[strip], (unsigned)A.splits)) {
-    double s_bb = 0, s_g2 = 0, s_gd = 0;
+    double s_bb = 0, s_g2 = 0, s_gd = 0, s_gl = 0;
     const int j = c0 + threadIdx.x;
     if (j < m) {
       double c = 0.0;
@@ -169,39 +170,45 @@ __global__ void __launch_bounds__(kThreads, 3) tpass_kernel(const TPassArgs A) {
       if (A.trial) A.gamma[n + j] = be;
       A.cols[j] = c;
       s_bb = A.ab[n + j] * be;
+      const double g = c - A.ab[n + j];
       if (j < m - 1) {
-        const double g = c - A.ab[n + j];
         A.grad[n + j] = g;
         s_g2 = g * g;
         if (A.direc) s_gd = g * A.direc[n + j];
+      } else {
+        s_gl = g * g;  // the gauge column: outside g, inside the full marginal error
       }
     }
     s_bb = cta_sum(s_bb, red);
     s_g2 = cta_sum(s_g2, red);
     s_gd = cta_sum(s_gd, red);
+    s_gl = cta_sum(s_gl, red);
     if (threadIdx.x == 0) {
-      double* o = A.scal + (size_t)(A.splits + strip) * 4;
+      double* o = A.scal + (size_t)(A.splits + strip) * kTScal;
       o[0] = 0.0;
       o[1] = s_bb;
       o[2] = s_g2;
       o[3] = s_gd;
+      o[4] = s_gl;
     }
     if (elect_last(cnt_all, nfin)) final_role = true;
   }
   if (!final_role) return;
   if (threadIdx.x == 0) {
-    double tsum = 0, dot = 0, g2 = 0, gd = 0;
+    double tsum = 0, dot = 0, g2 = 0, gd = 0, gl = 0;
     for (int q = 0; q < A.splits + A.strips; ++q) {
-      const double* o = A.scal + (size_t)q * 4;
+      const double* o = A.scal + (size_t)q * kTScal;
       tsum += ldcg(o);
       dot += ldcg(o + 1);
       g2 += ldcg(o + 2);
       gd += ldcg(o + 3);
+      gl += ldcg(o + 4);
     }
     A.res->f = A.eta * tsum - dot;
     A.res->gnorm = sqrt(g2);
     A.res->dg = gd;
     A.res->tsum = tsum;
+    A.res->gfull = sqrt(g2 + gl);
   }
   (void)H;
 }
@@ -214,7 +221,7 @@ void tpass_geometry(int n, int m, int sm_count, int& strips, int& splits) {
 }
 
 size_t tpass_workspace_doubles(int n, int m, int strips, int splits) {
-  return (size_t)strips * n + (size_t)splits * m + (size_t)(splits + strips) * 4;
+  return (size_t)strips * n + (size_t)splits * m + (size_t)(splits + strips) * kTScal;
 }
 
 int launch_tpass(bool f32, const TPassArgs& a, cudaStream_t stream) {

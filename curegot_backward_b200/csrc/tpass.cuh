@@ -12,6 +12,7 @@ struct TResult {
   double gnorm;   // ||g||_2, g = (r - a, c_{:m-1} - b_{:m-1})
   double dg;      // <g, direc> (trial mode)
   double tsum;    // sum(T)
+  double gfull;   // full marginal error ||(r - a, c - b)||_2 (all m columns)
 };
 
 struct TPassArgs {
@@ -34,11 +35,12 @@ struct TPassArgs {
   int strips, splits;      // tile grid: strips of 256 columns x row splits
   double* rowpart;         // [strips * n]
   double* colpart;         // [splits * m]
-  double* scal;            // [(splits + strips) * 4]
+  double* scal;            // [(splits + strips) * kTScal]
   unsigned int* counters;  // [splits + strips + 1], zero-initialised
 };
 
 constexpr int kTStrip = 256;  // columns per strip
+constexpr int kTScal = 5;     // partial scalars per finisher CTA
 
 void tpass_geometry(int n, int m, int sm_count, int& strips, int& splits);
 size_t tpass_workspace_doubles(int n, int m, int strips, int splits);

@@ -85,6 +85,11 @@ class OTEngine:
                         "t_done": r.t_done, "dual": dual})
         return out
 
+    def cancel(self, rid):
+        """Cancel a submitted request; its result comes back from poll() with
+        status CG_ERR_CANCELLED.  Raises if the id is unknown or finished."""
+        _native.call("cg_engine_cancel", self._h, int(rid))
+
     def stats(self):
         s = _native.EngineStats()
         _native.call("cg_engine_stats", self._h, ctypes.byref(s))

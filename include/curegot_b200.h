@@ -35,7 +35,8 @@ enum {
   CG_ERR_NONFINITE = 6,        /* non-finite state where one is not allowed  */
   CG_ERR_INVALID_CONTEXT = 7,  /* backward context missing or invalid        */
   CG_ERR_SOLVER = 8,           /* linear-solver library error                */
-  CG_ERR_ADMISSION = 9         /* request does not fit the engine budget     */
+  CG_ERR_ADMISSION = 9,        /* request does not fit the engine budget     */
+  CG_ERR_CANCELLED = 10        /* engine request cancelled by the caller     */
 };
 
 /* Human-readable text of the last error raised on the calling thread. */
@@ -79,9 +80,13 @@ int cg_bcd_f64(const double* M, const double* a, const double* b, double* P, dou
  * framework that owns HBM (a preallocating allocator, or a caching allocator
  * that has reserved nearly all of it), where a stream-ordered allocation
  * inside the call can fail with out-of-memory or grow a second pool beside
- * the framework's.  Same arguments, kernels and results as cg_bcd_f64; the
- * scratch is a 4 MiB file-scope device array inside this library instead of
- * a cudaMallocAsync block, and nothing else is allocated.
+ * the framework's.  Same arguments and stopping rule as cg_bcd_f64, and the same
+ * kernels and results as cg_bcd_f64 takes with the cluster path disabled
+ * (cg_bcd_set_cluster_path(0)): this entry point always runs the multi-CTA
+ * row/column passes, so for small problems that cg_bcd_f64 would solve in
+ * one cluster launch the two can differ in rounding (and, rarely, niter by
+ * one).  The scratch is a 4 MiB file-scope device array inside this library
+ * instead of a cudaMallocAsync block, and nothing else is allocated.
  *   - n and m must each be <= 16384, otherwise CG_ERR_INVALID_ARG (before any
  *     launch; cg_last_error() says why).
  *   - Nothing has to start at zero: every call initialises the state, the
@@ -170,7 +175,10 @@ int cg_splr_f64(const double* M, const double* a, const double* b, double* P, do
                 double shift_max, int sparsity_pattern_cycle, int candidate_sinkhorn_iter,
                 int verbose, const double* x0, double* dual, cg_ctx** ctx_out, int* converged,
                 double* trace, cudaStream_t stream);
-/* Same with M in FP32 (all arithmetic, duals, line search and solve in FP64). */
+/* Same with M in FP32 (all arithmetic, duals, line search and solve in FP64).
+ * Stopping test: the full marginal error ||(T1 - a, T^T 1 - b)||_2 < tol,
+ * i.e. the reference's ||g|| plus the gauge column's error, so every column
+ * meets tol too (the reference's test leaves column m-1 out). */
 int cg_splr_mixed(const float* M, const double* a, const double* b, double* P, double reg,
                   int max_iter, double tol, int n, int m, int* niter, double density_max,
                   double shift_max, int sparsity_pattern_cycle, int candidate_sinkhorn_iter,
@@ -283,6 +291,12 @@ int cg_engine_poll(cg_engine* eng, cg_result_t* results, int capacity, int wait_
 int cg_engine_stats(cg_engine* eng, cg_engine_stats_t* out);
 /* The engine's clock (seconds, monotonic), for latency accounting. */
 double cg_engine_clock(void);
+/* Cancels a request: a queued one ends at once, an admitted Sinkhorn one at
+ * the end of its batch's current chunk, an admitted SPLR one at its next
+ * iteration.  Its result (status CG_ERR_CANCELLED, no duals written) is
+ * returned by cg_engine_poll like any other.  CG_ERR_INVALID_ARG when the id
+ * is unknown or already finished.  No reference counterpart. */
+int cg_engine_cancel(cg_engine* eng, uint64_t id);
 /* Stops the engine (admitted work finishes; queued requests are dropped). */
 int cg_engine_destroy(cg_engine* eng);
 
@@ -302,6 +316,15 @@ int cg_test_t_sparsify_f64(const double* alpha, const double* beta, const double
                            int n, int m, double* rows, double* cols, double* grad,
                            double* objfn_gnorm, double* csr_val, int* csr_colind,
                            int* csr_rowptr, long long* k_actual, cudaStream_t stream);
+/* Host-side failure injection for tests (process-wide).  what =
+ * CG_INJECT_DIRECTION_SOLVE: the next `count` SPLR direction solves report a
+ * failed factorization, as a non-positive pivot would, so the solve returns
+ * CG_ERR_NOT_SPD (the reference exits the process on a cuDSS failure,
+ * src/linsolve.cu:19-26).  Nothing on the device is altered; count = 0
+ * clears it. */
+enum { CG_INJECT_DIRECTION_SOLVE = 1 };
+int cg_test_inject_failure(int what, int count);
+
 /* SPD solve with a CSR matrix (full or lower storage, lower triangle read)
  * (sparse_cholesky_solve_host, src/linsolve.cu:312-350).  Device arrays. */
 int cg_test_spd_solve_f64(const double* values, const int* colind, const int* rowptr, int n,
@@ -335,6 +358,14 @@ int cg_bcd_points_bf16(const uint16_t* X, const uint16_t* Y, int n, int m, int d
                        double cost_scale, const double* a, const double* b, double reg,
                        int max_iter, double tol, int precision, int* niter, double* dual,
                        int* fast_iters, cudaStream_t stream);
+/* Poll limit of the first wait for each tile's tensor-core MMAs in the two
+ * functions above (process-wide; polls < 0 restores the default of 2^24).
+ * When a wait gives up, the kernel waits once more at the full limit for the
+ * MMAs to drain, frees its tensor memory and flags the error: the call
+ * returns CG_ERR_TIMEOUT and the device stays usable.  polls = 0 makes every
+ * first wait give up at once -- the way tests exercise that path without a
+ * fault.  No reference counterpart. */
+int cg_points_set_wait_limit(long long polls);
 
 /* ------------------------------------------------------------------------ */
 /* Diagnostics (no reference counterpart).                                   */

@@ -41,10 +41,20 @@ def build() -> str:
     return _LIB_PATH
 
 
-def build_ref() -> str | None:
+def reference_root() -> str | None:
+    """The reference checkout: $REFERENCE_ROOT, else a `reference` directory
+    beside this repository; None when neither holds its sources."""
+    cand = os.environ.get("REFERENCE_ROOT") or os.path.join(os.path.dirname(_HERE), os.pardir,
+                                                            "reference")
+    cand = os.path.abspath(cand)
+    return cand if os.path.isfile(os.path.join(cand, "src", "sinkhorn_bcd_kernel.cu")) else None
+
+
+def build_ref(root: str | None = None) -> str | None:
     """Compile the reference's GPU BCD into oracle/_ref when its sources exist."""
+    root = root or reference_root()
     script = os.path.join(_HERE, "build_ref.sh")
-    subprocess.run(["bash", script], check=True)
+    subprocess.run(["bash", script] + ([root] if root else []), check=True)
     return _REF_PATH if os.path.exists(_REF_PATH) else None
 
 

@@ -119,3 +119,58 @@ def test_points_arguments_rejected_without_gpu():
         _check_points(X, X[:, :2])
     with pytest.raises(ValueError):
         _check_points(X, X)  # host tensors
+
+
+def test_cpu_sample_full_budget_solves_everything():
+    """With a budget above the whole set's cost, every request is solved
+    (p = 1) and the estimate is the measured total."""
+    from curegot_backward_b200.synthetic import stream_problem
+    specs = stream_specs(6, seed=5, n_lo=8, n_hi=48)
+    got = bench.cpu_sample(specs, lambda i: stream_problem(specs[i], device="cpu"), 1e9)
+    sps, cores, desc = got
+    assert desc.startswith("6 of 6 requests")
+    assert sps > 0 and cores >= 1
+
+
+def test_cpu_sample_estimate_is_unbiased(monkeypatch):
+    """Horvitz-Thompson: with a fake oracle whose solve time equals the
+    predicted cost times a per-request factor, the mean of 1/solves-rate over
+    seeds converges to the true total time per request."""
+    import oracle
+    specs = stream_specs(40, seed=9, n_hi=4096)
+    times = {id(s): 1e-9 * bench._predicted_cpu_cost(s) * (0.5 + (k % 3)) for k, s in
+             enumerate(specs)}
+    current = {}
+
+    class FakeM:
+        def double(self):
+            return self
+
+        def numpy(self):
+            return None
+
+    def get(i):
+        current["s"] = specs[i]
+        return FakeM(), FakeM(), FakeM()
+
+    clock = {"t": 0.0}
+    monkeypatch.setattr(bench.time, "perf_counter", lambda: clock["t"])
+
+    def fake_solve(*a, **k):
+        clock["t"] += times[id(current["s"])]
+        return {"niter": 1}
+
+    monkeypatch.setattr(oracle, "bcd", fake_solve)
+    monkeypatch.setattr(oracle, "splr", fake_solve)
+    true_total = sum(times.values())
+    budget = 0.2 * true_total
+    est = [len(specs) / bench.cpu_sample(specs, get, budget, seed=sd)[0] for sd in range(400)]
+    import numpy as np
+    assert abs(np.mean(est) - true_total) < 0.05 * true_total
+
+
+def test_per_step_rates():
+    res = [{"t_submit": 0.0, "t_done": 0.1 * (k + 1)} for k in range(20)]
+    rates = bench.per_step_rates(res, 5)
+    assert len(rates) == 4
+    assert all(abs(r - 10.0) < 1e-9 for r in rates)

@@ -62,6 +62,55 @@ def test_two_calls_in_a_row_match_allocating_entry(cuda_dev):
         assert np.linalg.norm(g["plan"].sum(1) - p[1]) < tol
 
 
+def test_small_problem_matches_pass_path(cuda_dev):
+    """64 x 80: cg_bcd_f64 would take the cluster path; with it disabled the
+    two entry points run the same passes.  The marginal error is also checked
+    against the oracle's evaluation of the returned duals."""
+    import curegot_backward_b200 as cg
+    import oracle
+    M, a, b = _problem(64, 80, 14)
+    got = _solve("cg_bcd_f64_noalloc", M, a, b, 0.05, 1e-8, 3000, cuda_dev)
+    cg.set_bcd_cluster_path(False)
+    try:
+        ref = _solve("cg_bcd_f64", M, a, b, 0.05, 1e-8, 3000, cuda_dev)
+    finally:
+        cg.set_bcd_cluster_path(True)
+    _assert_same(got, ref)
+    o = oracle.bcd(M, a, b, 0.05, tol=1e-8, max_iter=3000)
+    assert got["niter"] == o["niter"]
+    P = np.exp((got["dual"][:64, None] + got["dual"][None, 64:] - M) / 0.05)
+    assert np.linalg.norm(P.sum(1) - a) < 1e-8
+
+
+@pytest.mark.parametrize("n,m", [(16384, 64), (64, 16384), (16384, 16384)])
+def test_largest_accepted_shapes_fit_the_scratch(cuda_dev, n, m):
+    """The scratch carve depends on the SM count through the column-pass
+    splits and the row-pass CTAs; the extreme shapes inside the documented
+    n, m <= 16384 limit must be accepted and agree with cg_bcd_f64.  Inputs
+    stay on the device, no plan is written, and a few iterations at tol 0
+    keep the 2 GB case short."""
+    L = _native.lib()
+    g = torch.Generator(device=cuda_dev).manual_seed(n + 7 * m)
+    M = torch.rand((n, m), dtype=torch.float64, device=cuda_dev, generator=g)
+    a = torch.full((n,), 1.0 / n, dtype=torch.float64, device=cuda_dev)
+    b = torch.full((m,), 1.0 / m, dtype=torch.float64, device=cuda_dev)
+    stream = torch.cuda.current_stream(cuda_dev).cuda_stream
+    out = {}
+    for fn in ("cg_bcd_f64_noalloc", "cg_bcd_f64"):
+        dual = torch.empty(n + m, dtype=torch.float64, device=cuda_dev)
+        niter = ctypes.c_int(-1)
+        status = getattr(L, fn)(M.data_ptr(), a.data_ptr(), b.data_ptr(), None, 0.1, 3, 0.0,
+                                n, m, ctypes.byref(niter), None, dual.data_ptr(), stream)
+        _native.check(fn, status)
+        torch.cuda.synchronize(cuda_dev)
+        out[fn] = (niter.value, dual.cpu().numpy())
+    (n0, d0), (n1, d1) = out["cg_bcd_f64_noalloc"], out["cg_bcd_f64"]
+    assert n0 == n1 == 3
+    assert np.abs(d0 - d1).max() <= DUAL_RTOL * max(np.abs(d1).max(), 1e-300)
+    del M
+    torch.cuda.empty_cache()
+
+
 class _PoolProbe:
     """High-water mark of a stream-ordered memory pool (driver API)."""
 
