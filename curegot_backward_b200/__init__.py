@@ -10,7 +10,11 @@ curegot/__init__.py:1-43 and src/bindings.cpp:83-137):
     curegot_backward_b200.tests   test_T_computation_sparsify,
                                   test_sparse_cholesky_solve
 
-``import curegot_backward_b200 as curegot`` is the drop-in spelling.  All
+``import curegot_backward_b200 as curegot`` is the drop-in spelling; with
+``curegot_backward_b200/compat`` on ``sys.path`` (or after
+``install_reference_names()``) the reference's own names work unchanged:
+``import curegot``, ``from curegot.torch import splr_ot``, and the
+repo-root modules ``backward_core``, ``splr_backward``, ``splr_autograd``.  All
 numerical work runs in the sm_100a CUDA library ``_lib/libcuregot_b200.so``
 through its C ABI (``include/curegot_b200.h``); there is no CPU fallback.
 """
@@ -68,6 +72,13 @@ def set_bcd_cluster_path(enabled: bool = True) -> None:
     _native.call("cg_bcd_set_cluster_path", 1 if enabled else 0)
 
 
+def set_bcd_staging(enabled: bool = True) -> None:
+    """Enable (default) or disable the shared-memory staging of the Sinkhorn
+    passes: long rows and column strips stream through per-warp rings filled
+    by bulk asynchronous copies.  Results are bitwise the same either way."""
+    _native.call("cg_bcd_set_staging", 1 if enabled else 0)
+
+
 _DIRSOLVE = {"auto": 0, "dense": 1, "sparse": 2, "peel": 3}
 
 
@@ -87,3 +98,16 @@ def last_direction_solver() -> str | None:
     """Path of the last SPLR direction solve on this thread."""
     v = _native.lib().cg_splr_last_direction_solver()
     return {0: "dense", 1: "sparse", 2: "peel"}.get(v)
+
+
+def install_reference_names() -> str:
+    """Put the reference's import names on sys.path: ``curegot`` (with
+    ``curegot.numpy/torch/tests/autograd/backward/_backward_core``) and the
+    reference's repo-root modules ``backward_core``, ``splr_backward`` and
+    ``splr_autograd``, all served by this package.  Returns the directory
+    added."""
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "compat")
+    if path not in _sys.path:
+        _sys.path.insert(0, path)
+    return path

@@ -31,45 +31,51 @@ __all__ = ["splr_ot", "splr_ot_with_info", "splr_ot_batch", "SPLROT", "SPLROTFun
 
 
 def _check_inputs(M, a, b):
+    """Operand checks of the reference's splr_ot (curegot/autograd.py:57-126):
+    the exception type per condition is the API contract."""
     for name, t in (("M", M), ("a", a), ("b", b)):
         if not isinstance(t, torch.Tensor):
-            raise TypeError(f"splr_ot: {name} must be a torch.Tensor, got {type(t).__name__}")
+            raise TypeError(f"splr_ot: operand {name} is a {type(t).__name__}, "
+                            "expected a torch.Tensor")
         if not t.is_cuda:
-            raise RuntimeError(f"splr_ot: {name} must be a CUDA tensor (CUDA float64 only)")
+            raise RuntimeError(f"splr_ot: operand {name} lives on {t.device}; the solver "
+                               "runs on CUDA float64 tensors only")
         if t.dtype != torch.float64:
-            raise RuntimeError(f"splr_ot: {name} must be float64, got {t.dtype}; silent "
-                               "conversion would make the gradient dtype misleading")
+            raise RuntimeError(f"splr_ot: operand {name} has dtype {t.dtype}; pass float64 "
+                               "(no implicit cast, so gradients keep the caller's dtype)")
     if M.dim() != 2:
-        raise ValueError(f"splr_ot: M must be 2D (one problem per call; splr_ot_batch takes "
-                         f"[B, n, m]), got shape {tuple(M.shape)}")
+        raise ValueError(f"splr_ot: M needs shape [n, m] (use splr_ot_batch for [B, n, m]); "
+                         f"got {tuple(M.shape)}")
     n, m = M.shape
     if a.dim() != 1 or a.shape[0] != n:
-        raise ValueError(f"splr_ot: a must be 1D of length {n}, got shape {tuple(a.shape)}")
+        raise ValueError(f"splr_ot: a needs shape [{n}] to match M's rows; got "
+                         f"{tuple(a.shape)}")
     if b.dim() != 1 or b.shape[0] != m:
-        raise ValueError(f"splr_ot: b must be 1D of length {m}, got shape {tuple(b.shape)}")
+        raise ValueError(f"splr_ot: b needs shape [{m}] to match M's columns; got "
+                         f"{tuple(b.shape)}")
     if not (M.device == a.device == b.device):
-        raise ValueError(f"splr_ot: M/a/b must share one device, got {M.device}, {a.device}, "
-                         f"{b.device}")
+        raise ValueError(f"splr_ot: M, a and b are on different devices "
+                         f"({M.device}, {a.device}, {b.device})")
 
 
 def _validate_scalars(eta, tol, max_iter, density, candidate_sinkhorn_iter, backward_tol,
                       backward_max_iter):
-    if not (math.isfinite(eta) and eta > 0):
-        raise ValueError(f"splr_ot: eta must be a positive finite scalar, got {eta}")
-    if not (math.isfinite(tol) and tol > 0):
-        raise ValueError(f"splr_ot: tol must be positive, got {tol}")
-    if not int(max_iter) > 0:
-        raise ValueError(f"splr_ot: max_iter must be positive, got {max_iter}")
-    if density is not None and not (0.0 < float(density) <= 1.0):
-        raise ValueError(f"splr_ot: density must be in (0, 1], got {density}")
-    if not int(candidate_sinkhorn_iter) >= 0:
-        raise ValueError(f"splr_ot: candidate_sinkhorn_iter must be >= 0, got "
-                         f"{candidate_sinkhorn_iter}")
-    if not (math.isfinite(backward_tol) and backward_tol > 0):
-        raise ValueError(f"splr_ot: backward_tol must be positive, got {backward_tol}")
-    if not int(backward_max_iter) > 0:
-        raise ValueError(f"splr_ot: backward_max_iter must be positive, got "
-                         f"{backward_max_iter}")
+    checks = (
+        (math.isfinite(eta) and eta > 0, f"eta must be finite and > 0 (got {eta})"),
+        (math.isfinite(tol) and tol > 0, f"tol must be > 0 (got {tol})"),
+        (int(max_iter) > 0, f"max_iter must be at least 1 (got {max_iter})"),
+        (density is None or 0.0 < float(density) <= 1.0,
+         f"density must lie in (0, 1] (got {density})"),
+        (int(candidate_sinkhorn_iter) >= 0,
+         f"candidate_sinkhorn_iter must be 0 or more (got {candidate_sinkhorn_iter})"),
+        (math.isfinite(backward_tol) and backward_tol > 0,
+         f"backward_tol must be > 0 (got {backward_tol})"),
+        (int(backward_max_iter) > 0,
+         f"backward_max_iter must be at least 1 (got {backward_max_iter})"),
+    )
+    for ok, msg in checks:
+        if not ok:
+            raise ValueError("splr_ot: " + msg)
 
 
 def _forward_native(M, a, b, eta, tol, max_iter, density, candidate_sinkhorn_iter):

@@ -28,8 +28,11 @@
 //   cancellation), so no pass needs a second sweep over the duals.
 // * Every reduction has a fixed order: results are bitwise reproducible.
 #include <algorithm>
+#include <atomic>
+#include <mutex>
 
 #include "bcd.cuh"
+#include "bulk.cuh"
 #include "lse.cuh"
 
 #ifndef CG_BCD_MINB
@@ -113,6 +116,85 @@ __device__ __forceinline__ void row_segment(const TM* __restrict__ Mrow,
   }
 }
 
+// row_segment for rows whose 16-byte vectors are aligned (vec_ok) and long
+// enough to stream: the whole spans of [c0, c1) reach shared memory through
+// the warp's ring (bulk copies issued kRingStages chunks ahead, so the HBM
+// latency is covered without registers held by in-flight loads), then each
+// span is processed exactly like row_segment's loop body -- same grouping,
+// same order, bitwise the same (mx, s).  The tail (< one span) is read as in
+// row_segment.  A ring wait that gives up leaves ring.failed set.
+template <typename TM, bool FAST>
+__device__ __forceinline__ void row_segment_staged(const TM* __restrict__ Mrow,
+                                                   const double* __restrict__ betas, double s2,
+                                                   int c0, int c1, int lane, const double* tab,
+                                                   WarpRing& ring, double& mx, double& s) {
+  constexpr int VN = Vec<TM>::N;
+  constexpr int U = RowU<TM>::U;
+  constexpr int step = 32 * VN;
+  constexpr int span = step * U;
+  constexpr int span_bytes = span * (int)sizeof(TM);
+  constexpr int SPC = kRingBytes / span_bytes;  // spans per ring chunk
+  static_assert(SPC >= 1 && kRingBytes % span_bytes == 0, "ring chunk size");
+  using RT = typename Raw<TM>::T;
+  const int nspans = (c1 - c0) / span;
+  const int nchunks = (nspans + SPC - 1) / SPC;
+  const uint32_t g0 = ring.issued;
+  auto issue = [&](int k) {  // lane 0
+    const int sp0 = k * SPC;
+    const uint32_t bytes = (uint32_t)min(SPC, nspans - sp0) * span_bytes;
+    const uint32_t g = g0 + (uint32_t)k;
+    mbar_expect_tx(ring.barrier(g), bytes);
+    bulk_g2s(ring.stage(g), Mrow + c0 + (size_t)sp0 * span, bytes, ring.barrier(g));
+  };
+  const int pre = min(nchunks, kRingStages);
+  if (lane == 0)
+    for (int k = 0; k < pre; ++k) issue(k);
+  ring.issued = g0 + (uint32_t)pre;
+  for (int k = 0; k < nchunks; ++k) {
+    if (!ring.wait_next()) {
+      ring.drain();
+      return;
+    }
+    const RT* chunk = reinterpret_cast<const RT*>(ring.stage(ring.consumed));
+    const int sp0 = k * SPC, nsp = min(SPC, nspans - sp0);
+    for (int q = 0; q < nsp; ++q) {
+      const int cb = c0 + (sp0 + q) * span;
+      double d[U * VN];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const RT v = chunk[q * (span / VN) + u * 32 + lane];
+        double bv[VN];
+        ld_duals<VN>(betas + cb + lane * VN + u * step, bv);
+#pragma unroll
+        for (int kk = 0; kk < VN; ++kk) d[u * VN + kk] = fma(-Raw<TM>::get(v, kk), s2, bv[kk]);
+      }
+      lse_chunk_full<FAST, U * VN>(d, mx, s, tab);
+    }
+    ring.consumed++;
+    __syncwarp();
+    if (k + kRingStages < nchunks) {
+      if (lane == 0) {
+        fence_proxy_async_smem();  // this stage's reads before the copy that refills it
+        issue(k + kRingStages);
+      }
+      ring.issued++;
+    }
+  }
+  for (int j = c0 + nspans * span + lane * VN; j < c1; j += step) {
+    double d[VN];
+    bool ok[VN];
+    double mv[VN], bv[VN];
+    Vec<TM>::load(Mrow + j, mv);
+    ld_duals<VN>(betas + j, bv);
+#pragma unroll
+    for (int k = 0; k < VN; ++k) {
+      ok[k] = true;
+      d[k] = fma(-mv[k], s2, bv[k]);
+    }
+    lse_chunk<FAST, VN>(d, ok, mx, s, tab);
+  }
+}
+
 // CTA-wide Chan combine; thread 0 ends with the total.  sh: 3 * kThreads.
 __device__ __forceinline__ void cta_chan(double& n, double& mu, double& m2, double* sh) {
   const int t = threadIdx.x;
@@ -160,7 +242,8 @@ __device__ __forceinline__ void cta_stats(double v, bool valid, double* red, dou
 template <typename TM>
 __device__ __forceinline__ void row_block(const BcdProb* __restrict__ probs,
                                           const int* __restrict__ cta_prob,
-                                          const int* __restrict__ cta_start, int vb) {
+                                          const int* __restrict__ cta_start, int vb,
+                                          bool staged, WarpRing& ring) {
   __shared__ double tab[kExp2TableSize];
   __shared__ double sm_mx[kWarps], sm_s[kWarps];
   __shared__ double sm_v[kWarps][2];
@@ -203,10 +286,23 @@ __device__ __forceinline__ void row_block(const BcdProb* __restrict__ probs,
     const int c0 = seg * chunk;
     const int c1 = min(m, c0 + chunk);
     const TM* __restrict__ Mrow = M + (size_t)row * m;
-    if (fast)
+    // stream through the ring when the segment holds at least two chunks
+    const bool use_ring = staged && vec_ok && (c1 - c0) * (int)sizeof(TM) >= 2 * kRingBytes;
+    if (use_ring) {
+      if (fast)
+        row_segment_staged<TM, true>(Mrow, betas, s2, c0, c1, lane, tab, ring, mx, s);
+      else
+        row_segment_staged<TM, false>(Mrow, betas, s2, c0, c1, lane, tab, ring, mx, s);
+    } else if (fast) {
       row_segment<TM, true>(Mrow, betas, s2, c0, c1, lane, vec_ok, tab, mx, s);
-    else
+    } else {
       row_segment<TM, false>(Mrow, betas, s2, c0, c1, lane, vec_ok, tab, mx, s);
+    }
+  }
+  if (ring.failed && lane == 0) {
+    // a staging wait gave up: the problem ends with an error status
+    atomicExch(&st->error, 1);
+    atomicExch(&st->done, 1);
   }
   // warp combine: exact max by butterfly, then one rescale and a sum tree
   double wmx = mx;
@@ -386,11 +482,98 @@ __device__ __forceinline__ void col_rows(const TM* __restrict__ M, const double*
   }
 }
 
+// col_rows for strips whose 16-byte vectors are aligned (vec_ok): the warp's
+// full U-row groups reach shared memory through its ring, kRingBytes / 512
+// rows (one 512-byte strip segment each) per chunk, and are processed
+// exactly like col_rows's loop body -- same groups, same order, bitwise the
+// same (mx, s).  The remaining rows (fewer than U) are read as in col_rows.
+// lane_in: this lane's columns exist (the last strip may be partial);
+// strip_bytes: bytes of the strip in one row.
+template <typename TM, bool FAST>
+__device__ __forceinline__ void col_rows_staged(const TM* __restrict__ M,
+                                                const double* __restrict__ alphas, double s2,
+                                                int m, int strip_c0, int strip_bytes, int jb,
+                                                bool lane_in, int r0, int r1, int warp, int lane,
+                                                const double* tab, WarpRing& ring, double* mx,
+                                                double* s) {
+  constexpr int VN = Vec<TM>::N;
+  constexpr int U = (VN == 4) ? 2 : 4;
+  constexpr int RPC = kRingBytes / 512;  // warp rows per ring chunk
+  static_assert(RPC % U == 0, "ring chunk must hold whole row groups");
+  using RT = typename Raw<TM>::T;
+  const int i_first = r0 + warp;
+  const int nr = (r1 > i_first) ? (r1 - i_first + kWarps - 1) / kWarps : 0;
+  const int grouped = (nr / U) * U;  // rows taken in full groups
+  const int nchunks = (grouped + RPC - 1) / RPC;
+  const uint32_t g0 = ring.issued;
+  auto issue = [&](int k) {  // lane 0
+    const int q0 = k * RPC, nq = min(RPC, grouped - q0);
+    const uint32_t g = g0 + (uint32_t)k;
+    mbar_expect_tx(ring.barrier(g), (uint32_t)(nq * strip_bytes));
+    unsigned char* dst = ring.stage(g);
+    for (int q = 0; q < nq; ++q)
+      bulk_g2s(dst + q * 512, M + (size_t)(i_first + (q0 + q) * kWarps) * m + strip_c0,
+               (uint32_t)strip_bytes, ring.barrier(g));
+  };
+  const int pre = min(nchunks, kRingStages);
+  if (lane == 0)
+    for (int k = 0; k < pre; ++k) issue(k);
+  ring.issued = g0 + (uint32_t)pre;
+  for (int k = 0; k < nchunks; ++k) {
+    if (!ring.wait_next()) {
+      ring.drain();
+      return;
+    }
+    const unsigned char* chunk = ring.stage(ring.consumed);
+    const int q0 = k * RPC, nq = min(RPC, grouped - q0);
+    if (lane_in) {
+      for (int qg = 0; qg < nq; qg += U) {
+        RT cur[U];
+        double ai[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          cur[u] = reinterpret_cast<const RT*>(chunk + (qg + u) * 512)[lane];
+          ai[u] = alphas[i_first + (q0 + qg + u) * kWarps];
+        }
+#pragma unroll
+        for (int kk = 0; kk < VN; ++kk) {
+          double d[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) d[u] = fma(-Raw<TM>::get(cur[u], kk), s2, ai[u]);
+          lse_chunk_full<FAST, U>(d, mx[kk], s[kk], tab);
+        }
+      }
+    }
+    ring.consumed++;
+    __syncwarp();
+    if (k + kRingStages < nchunks) {
+      if (lane == 0) {
+        fence_proxy_async_smem();  // this stage's reads before the copy that refills it
+        issue(k + kRingStages);
+      }
+      ring.issued++;
+    }
+  }
+  if (!lane_in) return;
+  for (int i = i_first + grouped * kWarps; i < r1; i += kWarps) {
+    const double ai = alphas[i];
+    double mv[VN];
+    Vec<TM>::load(M + (size_t)i * m + jb, mv);
+#pragma unroll
+    for (int kk = 0; kk < VN; ++kk) {
+      double d[1] = {fma(-mv[kk], s2, ai)};
+      bool ok[1] = {true};
+      lse_chunk<FAST, 1>(d, ok, mx[kk], s[kk], tab);
+    }
+  }
+}
+
 // One virtual CTA (index vb) of the column pass.
 template <typename TM>
 __device__ __forceinline__ void col_block(const BcdProb* __restrict__ probs,
                                           const int* __restrict__ cta_prob,
-                                          const int* __restrict__ cta_start, int vb) {
+                                          const int* __restrict__ cta_start, int vb,
+                                          bool staged, WarpRing& ring) {
   constexpr int VN = Vec<TM>::N;
   constexpr int W = 32 * VN;
   constexpr int G = kThreads / W;  // merge groups per column
@@ -430,7 +613,23 @@ __device__ __forceinline__ void col_block(const BcdProb* __restrict__ probs,
     mx[k] = kNegInf;
     s[k] = 0.0;
   }
-  if (jb < m) {
+  // stream through the ring when every warp has at least two chunks of rows
+  const bool use_ring = staged && vec_ok && (r1 - r0) >= 2 * kWarps * (kRingBytes / 512);
+  if (use_ring) {
+    const int strip_c0 = strip * W;
+    const int strip_bytes = min(W, m - strip_c0) * (int)sizeof(TM);
+    if (fast)
+      col_rows_staged<TM, true>(M, alphas, s2, m, strip_c0, strip_bytes, jb, jb < m, r0, r1,
+                                warp, lane, tab, ring, mx, s);
+    else
+      col_rows_staged<TM, false>(M, alphas, s2, m, strip_c0, strip_bytes, jb, jb < m, r0, r1,
+                                 warp, lane, tab, ring, mx, s);
+    if (ring.failed && lane == 0) {
+      // a staging wait gave up: the problem ends with an error status
+      atomicExch(&st->error, 1);
+      atomicExch(&st->done, 1);
+    }
+  } else if (jb < m) {
     if (fast)
       col_rows<TM, true>(M, alphas, s2, m, jb, r0, r1, warp, vec_ok, tab, mx, s);
     else
@@ -541,17 +740,23 @@ __device__ __forceinline__ void col_block(const BcdProb* __restrict__ probs,
 // the same work, in the same per-block order, leaving SM slots free for
 // latency-bound kernels on other streams.
 // LOOP = false: one virtual CTA per CTA (uncapped launches).
+// staged != 0: long rows / column strips stream through per-warp shared-memory
+// rings filled by bulk copies (dynamic shared memory: kRingDynBytes).
 template <typename TM, bool LOOP>
 __global__ void __launch_bounds__(kThreads, kBcdMinBlocks) bcd_row_kernel(const BcdProb* __restrict__ probs,
                                                             const int* __restrict__ cta_prob,
                                                             const int* __restrict__ cta_start,
-                                                            int total) {
+                                                            int total, int staged) {
+  extern __shared__ __align__(128) unsigned char ring_smem[];
+  __shared__ uint64_t ring_bars[kWarps * kRingStages];
+  WarpRing ring;
+  rings_init(ring_smem, ring_bars, kWarps, ring);
   if (!LOOP) {
-    row_block<TM>(probs, cta_prob, cta_start, (int)blockIdx.x);
+    row_block<TM>(probs, cta_prob, cta_start, (int)blockIdx.x, staged != 0, ring);
     return;
   }
   for (int vb = blockIdx.x; vb < total; vb += gridDim.x) {
-    row_block<TM>(probs, cta_prob, cta_start, vb);
+    row_block<TM>(probs, cta_prob, cta_start, vb, staged != 0, ring);
     __syncthreads();
   }
 }
@@ -560,13 +765,17 @@ template <typename TM, bool LOOP>
 __global__ void __launch_bounds__(kThreads, kBcdMinBlocks) bcd_col_kernel(const BcdProb* __restrict__ probs,
                                                             const int* __restrict__ cta_prob,
                                                             const int* __restrict__ cta_start,
-                                                            int total) {
+                                                            int total, int staged) {
+  extern __shared__ __align__(128) unsigned char ring_smem[];
+  __shared__ uint64_t ring_bars[kWarps * kRingStages];
+  WarpRing ring;
+  rings_init(ring_smem, ring_bars, kWarps, ring);
   if (!LOOP) {
-    col_block<TM>(probs, cta_prob, cta_start, (int)blockIdx.x);
+    col_block<TM>(probs, cta_prob, cta_start, (int)blockIdx.x, staged != 0, ring);
     return;
   }
   for (int vb = blockIdx.x; vb < total; vb += gridDim.x) {
-    col_block<TM>(probs, cta_prob, cta_start, vb);
+    col_block<TM>(probs, cta_prob, cta_start, vb, staged != 0, ring);
     __syncthreads();
   }
 }
@@ -585,31 +794,60 @@ __global__ void plan_kernel(const TM* __restrict__ M, const double* __restrict__
   }
 }
 
+namespace {
+constexpr int kRingDynBytes = kWarps * kRingStages * kRingBytes;
+std::atomic<int> g_staged{1};
+std::once_flag g_ring_attr_once;
+
+// Opt the pass kernels into kRingDynBytes of dynamic shared memory (once per
+// process; above the 48 KB default together with their static arrays).
+void set_ring_attributes() {
+  std::call_once(g_ring_attr_once, [] {
+    cudaFuncSetAttribute(bcd_row_kernel<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingDynBytes);
+    cudaFuncSetAttribute(bcd_row_kernel<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingDynBytes);
+    cudaFuncSetAttribute(bcd_row_kernel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingDynBytes);
+    cudaFuncSetAttribute(bcd_row_kernel<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingDynBytes);
+    cudaFuncSetAttribute(bcd_col_kernel<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingDynBytes);
+    cudaFuncSetAttribute(bcd_col_kernel<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingDynBytes);
+    cudaFuncSetAttribute(bcd_col_kernel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingDynBytes);
+    cudaFuncSetAttribute(bcd_col_kernel<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingDynBytes);
+  });
+}
+}  // namespace
+
+void bcd_set_staging(bool on) { g_staged.store(on ? 1 : 0); }
+
 void launch_bcd_row(bool f32, const BcdProb* d_probs, const int* d_cta_prob,
                     const int* d_cta_start, int total_ctas, cudaStream_t stream, int grid_cap) {
+  set_ring_attributes();
   const bool loop = grid_cap > 0 && grid_cap < total_ctas;
   const int grid = loop ? grid_cap : total_ctas;
+  const int sg = g_staged.load();
+  const size_t sm = kRingDynBytes;
   if (f32 && loop)
-    { bcd_row_kernel<float, true><<<grid, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas); cg::count_launch(); }
+    { bcd_row_kernel<float, true><<<grid, kThreads, sm, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas, sg); cg::count_launch(); }
   else if (f32)
-    { bcd_row_kernel<float, false><<<grid, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas); cg::count_launch(); }
+    { bcd_row_kernel<float, false><<<grid, kThreads, sm, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas, sg); cg::count_launch(); }
   else if (loop)
-    { bcd_row_kernel<double, true><<<grid, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas); cg::count_launch(); }
+    { bcd_row_kernel<double, true><<<grid, kThreads, sm, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas, sg); cg::count_launch(); }
   else
-    { bcd_row_kernel<double, false><<<grid, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas); cg::count_launch(); }
+    { bcd_row_kernel<double, false><<<grid, kThreads, sm, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas, sg); cg::count_launch(); }
 }
 void launch_bcd_col(bool f32, const BcdProb* d_probs, const int* d_cta_prob,
                     const int* d_cta_start, int total_ctas, cudaStream_t stream, int grid_cap) {
+  set_ring_attributes();
   const bool loop = grid_cap > 0 && grid_cap < total_ctas;
   const int grid = loop ? grid_cap : total_ctas;
+  const int sg = g_staged.load();
+  const size_t sm = kRingDynBytes;
   if (f32 && loop)
-    { bcd_col_kernel<float, true><<<grid, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas); cg::count_launch(); }
+    { bcd_col_kernel<float, true><<<grid, kThreads, sm, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas, sg); cg::count_launch(); }
   else if (f32)
-    { bcd_col_kernel<float, false><<<grid, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas); cg::count_launch(); }
+    { bcd_col_kernel<float, false><<<grid, kThreads, sm, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas, sg); cg::count_launch(); }
   else if (loop)
-    { bcd_col_kernel<double, true><<<grid, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas); cg::count_launch(); }
+    { bcd_col_kernel<double, true><<<grid, kThreads, sm, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas, sg); cg::count_launch(); }
   else
-    { bcd_col_kernel<double, false><<<grid, kThreads, 0, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas); cg::count_launch(); }
+    { bcd_col_kernel<double, false><<<grid, kThreads, sm, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas, sg); cg::count_launch(); }
 }
 template <typename TM>
 void launch_plan(const TM* M, const double* alpha, const double* beta, double* P,

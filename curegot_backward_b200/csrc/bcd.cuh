@@ -27,6 +27,8 @@ struct BcdState {
   double stat_a[3];   // (count, mean, M2) of alpha^{t+1} - alpha^t
   int fast_iters;     // iterations run with SFU passes
   int nonfinite;      // a stop-test value was NaN / Inf (non-finite M, a, b or x0): done
+  int error;          // a bounded device wait gave up (staging ring): done
+  int pad_;
 };
 
 struct BcdProb {
@@ -64,6 +66,11 @@ void launch_bcd_col(bool f32, const BcdProb* d_probs, const int* d_cta_prob,
 template <typename TM>
 void launch_plan(const TM* M, const double* alpha, const double* beta, double* P,
                  double inv_eta, int n, int m, cudaStream_t stream);
+
+// Pass kernels stream long rows / column strips through shared-memory rings
+// filled by bulk copies (process-wide; default on).  Off: every pass reads M
+// with vector loads straight into registers.  Same results either way.
+void bcd_set_staging(bool on);
 
 // Launch geometry for one problem.
 void bcd_geometry(int n, int m, int elem_bytes, int sm_count, BcdProb& p);

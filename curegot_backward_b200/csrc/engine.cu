@@ -139,6 +139,7 @@ __global__ void engine_init_kernel(const double* a, const double* b, int n, int 
     st->stat_a[0] = st->stat_a[1] = st->stat_a[2] = 0.0;
     st->fast_iters = 0;
     st->nonfinite = 0;
+    st->error = 0;
   }
 }
 
@@ -532,6 +533,7 @@ void bcd_loop(cg_engine_s* E, int cls) {
       }
       q->niter = s.niter;
       if (s.nonfinite) q->status = CG_ERR_NONFINITE;
+      if (s.error) q->status = CG_ERR_TIMEOUT;
       q->converged = !s.nonfinite &&
                      ((s.niter < s.max_iter) || (s.phase == 2 && s.last_err < s.tol && !s.fast));
       q->fast_iters = s.fast_iters;

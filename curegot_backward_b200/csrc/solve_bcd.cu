@@ -187,6 +187,7 @@ __global__ void bcd_init_kernel(const double* __restrict__ a, const double* __re
     st->stat_a[0] = st->stat_a[1] = st->stat_a[2] = 0.0;
     st->fast_iters = 0;
     st->nonfinite = 0;
+    st->error = 0;
   }
 }
 
@@ -221,6 +222,13 @@ __global__ void dual_from_state_kernel(const BcdState* st, const BcdProb* p, dou
 // value (or log(a_i), log(b_j) of a zero marginal met an infinite cost).  The
 // reference keeps iterating to max_iter on NaN; here the solve stops at the
 // first non-finite test and reports it.
+// A bounded wait of a pass kernel's staging ring gave up (the state's error
+// flag); the solve stopped there.
+static int bcd_timeout() {
+  set_last_error("cg_bcd: a staging wait of a pass kernel timed out", __FILE__, __LINE__);
+  return CG_ERR_TIMEOUT;
+}
+
 static int bcd_nonfinite() {
   set_last_error("cg_bcd: non-finite stopping-test value (non-finite M, a, b or x0)", __FILE__,
                  __LINE__);
@@ -344,6 +352,7 @@ int bcd_solve(const TM* M, const double* a, const double* b, double* Pout, doubl
   }
   *niter = hs.niter;
   if (hs.nonfinite) return bcd_nonfinite();
+  if (hs.error) return bcd_timeout();
 
   if (Pout) {
     const size_t total = (size_t)n * m;
@@ -497,6 +506,7 @@ int bcd_solve_noalloc(const double* M, const double* a, const double* b, double*
   }
   *niter = hs.niter;
   if (hs.nonfinite) return bcd_nonfinite();
+  if (hs.error) return bcd_timeout();
 
   if (Pout) {
     const size_t total = (size_t)n * m;
@@ -556,6 +566,11 @@ int cg_bcd_f64_noalloc(const double* M, const double* a, const double* b, double
                        int max_iter, double tol, int n, int m, int* niter, const double* x0,
                        double* dual, cudaStream_t stream) {
   return cg::bcd_solve_noalloc(M, a, b, P, reg, max_iter, tol, n, m, niter, x0, dual, stream);
+}
+
+int cg_bcd_set_staging(int enable) {
+  cg::bcd_set_staging(enable != 0);
+  return CG_OK;
 }
 
 int cg_bcd_mixed(const float* M, const double* a, const double* b, double* P, double reg,

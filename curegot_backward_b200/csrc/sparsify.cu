@@ -4,7 +4,7 @@
 //   T_fused_kernel's Tvalues/Tflatind output       :214-345
 //   launch_H_sparsification (cub::DeviceTopK, thrust::sort_by_key,
 //     write_diagonal_kernel)                        :554-675
-//   recompute_nonzero_values_kernel                 :681-734
+//   recompute_nonzero_values_kernel                 :681-734  (refresh_all_kernel)
 //   extract_columns_and_count_kernel + DeviceScan   :741-820
 //
 // Design: T_t values are never materialised.  The K-th largest value is found
@@ -409,37 +409,56 @@ __global__ void diag_kernel(const double* rows, const double* cols, int n, int m
   }
 }
 
+// Fixed-pattern refresh (reference recompute_nonzero_values_kernel,
+// sinkhorn_splr_kernel.cu:681-734) in one launch: blocks [0, gj) recompute
+// the off-diagonal values of the CSR rows n + j (warp per row), blocks
+// [gj, gj + gi) those of the per-row lists (warp per row i), the rest write
+// the diagonal rows/cols + shift (as diag_kernel).  The roles touch disjoint
+// entries.
 template <typename TM>
-__global__ void refresh_byj_kernel(const TM* __restrict__ M, const double* __restrict__ gamma,
+__global__ void refresh_all_kernel(const TM* __restrict__ M, const double* __restrict__ gamma,
                                    int n, int m, double s2, const int* __restrict__ rowptr,
-                                   const int* __restrict__ col, double* __restrict__ val) {
+                                   int* __restrict__ col, double* __restrict__ val,
+                                   const int* __restrict__ ipt, const int* __restrict__ ij,
+                                   double* __restrict__ iv, const double* __restrict__ rows,
+                                   const double* __restrict__ cols, double shift, int gj, int gi) {
   __shared__ double tab[kExp2TableSize];
-  load_exp2_table(tab);
-  __syncthreads();
+  const int b = blockIdx.x;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int j = blockIdx.x * kWarps + warp; j < m - 1; j += gridDim.x * kWarps) {
-    const int r = n + j;
-    const double bs = gamma[n + j] * s2;
-    for (int q = rowptr[r] + lane; q < rowptr[r + 1] - 1; q += 32) {
-      const int i = col[q];
-      val[q] = t_at(M, i, j, m, gamma[i] * s2, bs, s2, tab);
-    }
+  if (b < gj + gi) {
+    load_exp2_table(tab);
+    __syncthreads();
   }
-}
-
-template <typename TM>
-__global__ void refresh_byi_kernel(const TM* __restrict__ M, const double* __restrict__ gamma,
-                                   int n, int m, double s2, const int* __restrict__ ipt,
-                                   const int* __restrict__ ij, double* __restrict__ iv) {
-  __shared__ double tab[kExp2TableSize];
-  load_exp2_table(tab);
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int i = blockIdx.x * kWarps + warp; i < n; i += gridDim.x * kWarps) {
-    const double as = gamma[i] * s2;
-    for (int q = ipt[i] + lane; q < ipt[i + 1]; q += 32) {
-      const int j = ij[q];
-      iv[q] = t_at(M, i, j, m, as, gamma[n + j] * s2, s2, tab);
+  if (b < gj) {
+    for (int j = b * kWarps + warp; j < m - 1; j += gj * kWarps) {
+      const int r = n + j;
+      const double bs = gamma[n + j] * s2;
+      for (int q = rowptr[r] + lane; q < rowptr[r + 1] - 1; q += 32) {
+        const int i = col[q];
+        val[q] = t_at(M, i, j, m, gamma[i] * s2, bs, s2, tab);
+      }
+    }
+  } else if (b < gj + gi) {
+    const int bb = b - gj;
+    for (int i = bb * kWarps + warp; i < n; i += gi * kWarps) {
+      const double as = gamma[i] * s2;
+      for (int q = ipt[i] + lane; q < ipt[i + 1]; q += 32) {
+        const int j = ij[q];
+        iv[q] = t_at(M, i, j, m, as, gamma[n + j] * s2, s2, tab);
+      }
+    }
+  } else {
+    const int H = n + m - 1;
+    const int gd = gridDim.x - gj - gi;
+    for (int r = (b - gj - gi) * blockDim.x + threadIdx.x; r < H; r += gd * blockDim.x) {
+      if (r < n) {
+        col[r] = r;
+        val[r] = rows[r] + shift;
+      } else {
+        const int p = rowptr[r + 1] - 1;
+        col[p] = r;
+        val[p] = cols[r - n] + shift;
+      }
     }
   }
 }
@@ -537,22 +556,17 @@ int sparsify_refresh(bool f32, const void* M, const double* gamma, const double*
                      const double* cols, int n, int m, double s2, double shift, const SpHess& h,
                      cudaStream_t st) {
   const int sms = 148;
-  if (m > 1) {
-    const int gj = grid_for(m - 1, kWarps, sms * 8), gi = grid_for(n, kWarps, sms * 8);
-    if (f32) {
-      { refresh_byj_kernel<float><<<gj, kThreads, 0, st>>>(static_cast<const float*>(M), gamma, n, m,
-                                                         s2, h.rowptr, h.col, h.val); cg::count_launch(); }
-      { refresh_byi_kernel<float><<<gi, kThreads, 0, st>>>(static_cast<const float*>(M), gamma, n, m,
-                                                         s2, h.ipt, h.ij, h.iv); cg::count_launch(); }
-    } else {
-      { refresh_byj_kernel<double><<<gj, kThreads, 0, st>>>(static_cast<const double*>(M), gamma, n,
-                                                          m, s2, h.rowptr, h.col, h.val); cg::count_launch(); }
-      { refresh_byi_kernel<double><<<gi, kThreads, 0, st>>>(static_cast<const double*>(M), gamma, n,
-                                                          m, s2, h.ipt, h.ij, h.iv); cg::count_launch(); }
-    }
-  }
-  { diag_kernel<<<grid_for(h.H, 256, sms * 4), 256, 0, st>>>(rows, cols, n, m, shift, h.rowptr,
-                                                            h.val, h.col); cg::count_launch(); }
+  const int gj = (m > 1) ? grid_for(m - 1, kWarps, sms * 8) : 0;
+  const int gi = (m > 1) ? grid_for(n, kWarps, sms * 8) : 0;
+  const int gd = grid_for(h.H, kThreads, sms * 2);
+  if (f32)
+    { refresh_all_kernel<float><<<gj + gi + gd, kThreads, 0, st>>>(
+        static_cast<const float*>(M), gamma, n, m, s2, h.rowptr, h.col, h.val, h.ipt, h.ij, h.iv,
+        rows, cols, shift, gj, gi); cg::count_launch(); }
+  else
+    { refresh_all_kernel<double><<<gj + gi + gd, kThreads, 0, st>>>(
+        static_cast<const double*>(M), gamma, n, m, s2, h.rowptr, h.col, h.val, h.ipt, h.ij, h.iv,
+        rows, cols, shift, gj, gi); cg::count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
   return CG_OK;
 }

@@ -80,14 +80,17 @@ __device__ __forceinline__ double block_sum1024(double v, double* sh) {
 
 // y = g - g_prev, s = gamma - gamma_prev, ys, yy, low-rank rule
 // (sinkhorn_splr_kernel_low_rank.cu:92-206, sinkhorn_splr.cu:1378-1382).
+// Also copies g into the first right-hand-side column of the direction solve.
 __global__ void __launch_bounds__(1024) lowrank_kernel(const double* g, const double* gp,
                                                        const double* gam, const double* gamp,
-                                                       double* y, double* s, int H, int iter,
-                                                       DirRes* out) {
+                                                       double* y, double* s, double* rhs_g, int H,
+                                                       int iter, DirRes* out) {
   __shared__ double sh[32];
   double ys = 0.0, yy = 0.0;
   for (int k = threadIdx.x; k < H; k += blockDim.x) {
-    const double yv = g[k] - gp[k], sv = gam[k] - gamp[k];
+    const double gv = g[k];
+    const double yv = gv - gp[k], sv = gam[k] - gamp[k];
+    rhs_g[k] = gv;
     y[k] = yv;
     s[k] = sv;
     ys += yv * sv;
@@ -106,11 +109,21 @@ __global__ void __launch_bounds__(1024) lowrank_kernel(const double* g, const do
 // d = -reg * x and dg_init = <g, d>
 // (launch_low_rank_search_direc, sinkhorn_splr_kernel_low_rank.cu:296-390;
 //  compute_scaling_inplace_cuda; dot in line_search_wolfe :690).
+// save_hist (nullable gam): also gamma_prev <- gamma, g_prev <- g over the
+// first H entries (the solver's save_history before the line search).
 __global__ void __launch_bounds__(1024) woodbury_kernel(double* x, const double* u,
                                                         const double* g, const double* y,
                                                         const double* s, int H, double reg,
-                                                        int scale, DirRes* dr) {
+                                                        int scale, DirRes* dr,
+                                                        const double* gam, double* gamp,
+                                                        double* gp) {
   __shared__ double sh[32];
+  if (gam) {
+    for (int k = threadIdx.x; k < H; k += blockDim.x) {
+      gamp[k] = gam[k];
+      gp[k] = g[k];
+    }
+  }
   const bool lr = dr->low_rank != 0;
   if (lr) {
     double sg = 0, yu = 0, yx = 0;
@@ -189,6 +202,20 @@ __global__ void bcd_seed_kernel(const double* beta_src, int zero, double* beta0,
     st->best_est = 0.0;
     st->fast_iters = 0;
     st->nonfinite = 0;
+    st->error = 0;
+  }
+}
+
+// Slot 1 -> slot 0 of the trial-pass outputs (gamma [n + m], grad [n + m - 1],
+// rows [n], cols [m]), when the line search ended on a speculative point.
+__global__ void copy_slot_kernel(double* gamma, double* grad, double* rows, double* cols, int n,
+                                 int m) {
+  const int H = n + m - 1;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n + m; k += gridDim.x * blockDim.x) {
+    gamma[k] = gamma[n + m + k];
+    if (k < H) grad[k] = grad[H + k];
+    if (k < n) rows[k] = rows[n + k];
+    else cols[k - n] = cols[m + (k - n)];
   }
 }
 
@@ -216,7 +243,12 @@ int read_dev(T* host, const T* dev, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------
-// Line-search step selection (utils.h:76-230), identical arithmetic.
+// Line-search step selection: quadratic_minimizer (x2), cubic_minimizer and
+// step_selection of the reference's src/utils.h:76-230, ported expression for
+// expression with the same branch order and constants (1.1, 0.66).  This is
+// kept alike on purpose: the parity bar requires the same line-search trial
+// counts as the reference, so the floating-point order of every step must be
+// the reference's.
 // ---------------------------------------------------------------------------
 double quad_min_fg(double a, double b, double fa, double ga, double fb) {
   const double ba = b - a;
@@ -448,14 +480,20 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
   const int bcount = 2 + cp.col_strips;
   Workspace ws(st);
   const size_t o_ab = ws.reserve<double>(n + m), o_logab = ws.reserve<double>(n + m);
-  const size_t o_g = ws.reserve<double>(n + m), o_gp = ws.reserve<double>(n + m);
+  // gamma, grad, rows, cols, the pass results and the pass workspace have
+  // kMaxTrialSteps slots (multi-step trial passes); slot 0 is the current one
+  const size_t o_g = ws.reserve<double>((size_t)kMaxTrialSteps * (n + m)),
+               o_gp = ws.reserve<double>(n + m);
   const size_t o_gb = ws.reserve<double>(n + m);
-  const size_t o_gr = ws.reserve<double>(H), o_grp = ws.reserve<double>(H);
+  const size_t o_gr = ws.reserve<double>((size_t)kMaxTrialSteps * H),
+               o_grp = ws.reserve<double>(H);
   const size_t o_grc = ws.reserve<double>(H);
-  const size_t o_rows = ws.reserve<double>(n), o_cols = ws.reserve<double>(m);
+  const size_t o_rows = ws.reserve<double>((size_t)kMaxTrialSteps * n),
+               o_cols = ws.reserve<double>((size_t)kMaxTrialSteps * m);
   const size_t o_rowsc = ws.reserve<double>(n), o_colsc = ws.reserve<double>(m);
-  const size_t o_res = ws.reserve<TResult>(2);
-  const size_t o_tw = ws.reserve<double>(tpass_workspace_doubles(n, m, tstrips, tsplits));
+  const size_t o_res = ws.reserve<TResult>(kMaxTrialSteps + 1);
+  const size_t o_tw =
+      ws.reserve<double>(kMaxTrialSteps * tpass_workspace_doubles(n, m, tstrips, tsplits));
   const size_t o_tc = ws.reserve<unsigned int>(tsplits + tstrips + 1);
   const size_t o_sw = ws.reserve<char>(sparsify_work_bytes(n, m));
   size_t o_bal[2], o_bbe[2], o_bals[2], o_bbes[2];
@@ -487,7 +525,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
   double* rows_c = ws.at<double>(o_rowsc);
   double* cols_c = ws.at<double>(o_colsc);
   TResult* res = ws.at<TResult>(o_res);
-  TResult* res_c = res + 1;
+  TResult* res_c = res + kMaxTrialSteps;
   double* tw = ws.at<double>(o_tw);
   unsigned int* tcnt = ws.at<unsigned int>(o_tc);
   SparsifyWork sw;
@@ -553,7 +591,20 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     CG_TRY(launch_tpass(f32, x, st));
     return read_dev(&host, out, st);
   };
-  auto trial_launch = [&](double step) -> int {
+  // Trial passes.  A pass evaluates `step` in slot 0 and, when spec > 0, a
+  // speculative second step in slot 1 (one read of M, the same values as two
+  // one-step passes).  `latest` remembers what the last pass left in its
+  // slots; the line search asks trial(step) and gets a slot's result without
+  // a pass when the step is bitwise one already evaluated -- its decisions,
+  // and so its trial counts, are those of one pass per trial.
+  struct PassSlot {
+    double step = 0.0;
+    TResult r{};
+    bool valid = false;
+  };
+  PassSlot latest[kMaxTrialSteps];
+  int cur_slot = 0;  // slot holding gamma / grad / rows / cols of the last evaluation
+  auto trial_launch = [&](double step, double spec) -> int {
     TPassArgs x = ta;
     x.gamma = gamma;
     x.gamma_prev = gamma_prev;
@@ -564,11 +615,44 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     x.cols = cols;
     x.grad = grad;
     x.res = res;
+    x.nsteps = (spec > 0.0) ? 2 : 1;
+    x.steps[0] = step;
+    x.steps[1] = spec;
+    for (int k = 0; k < kMaxTrialSteps; ++k) latest[k].valid = false;
+    latest[0].step = step;
+    latest[1].step = spec;
     return launch_tpass(f32, x, st);
   };
-  auto trial_at = [&](double step, TResult& host) -> int {
-    CG_TRY(trial_launch(step));
-    return read_dev(&host, res, st);
+  // results of the pass just launched (after the read)
+  auto trial_latch = [&](const TResult* r, int nsteps) {
+    for (int k = 0; k < nsteps; ++k) {
+      latest[k].r = r[k];
+      latest[k].valid = true;
+    }
+  };
+  auto trial = [&](double step, double spec, TResult& host) -> int {
+    for (int k = 0; k < kMaxTrialSteps; ++k)
+      if (latest[k].valid && latest[k].step == step) {
+        host = latest[k].r;
+        cur_slot = k;
+        return CG_OK;
+      }
+    CG_TRY(trial_launch(step, spec));
+    TResult r2[kMaxTrialSteps];
+    CG_TRY(read_device(r2, res, (spec > 0.0 ? 2 : 1) * sizeof(TResult), st));
+    trial_latch(r2, spec > 0.0 ? 2 : 1);
+    host = r2[0];
+    cur_slot = 0;
+    return CG_OK;
+  };
+  // Make slot 0 the current point when the last evaluation came from slot 1.
+  auto settle_slot = [&]() -> int {
+    if (cur_slot == 0) return CG_OK;
+    { copy_slot_kernel<<<grid_for(n + m, 256, 1024), 256, 0, st>>>(gamma, grad, rows, cols, n,
+                                                                 m); cg::count_launch(); }
+    CG_TRY_CUDA(cudaGetLastError());
+    cur_slot = 0;
+    return CG_OK;
   };
   const int bgrid = grid_for(m, 256, 1024);
   // alpha_bcd = A(beta) then `sweeps` x (beta, alpha): BCD passes, phase 0.
@@ -702,6 +786,12 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
   };
   CG_TRY(dual_sphess(density, shift * reg, false));
 
+  // Speculative second trial point in the line search's passes: always for
+  // problems whose pass is latency-bound (the second point costs no time),
+  // else after an iteration whose line search took more than one trial.
+  const bool small_problem = (long long)n * m <= (1LL << 22);
+  bool speculate = small_problem;
+
   double alpha_step = 1.0;
   double ys = 0.0, yy = 0.0;
   bool low_rank = false, converged = false, invalid_state = false;
@@ -719,8 +809,8 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     }
     if (!std::isfinite(objfn)) break;
 
-    { lowrank_kernel<<<1, 1024, 0, st>>>(grad, grad_prev, gamma, gamma_prev, hb.rhs2 + H, hb.s, H,
-                                       iter, hb.dres); cg::count_launch(); }
+    { lowrank_kernel<<<1, 1024, 0, st>>>(grad, grad_prev, gamma, gamma_prev, hb.rhs2 + H, hb.s,
+                                       hb.rhs2, H, iter, hb.dres); cg::count_launch(); }
     const bool analyze = (iter % prm.cycle == 0);
     const bool update = (iter % prm.cycle == (prm.cycle - 1));
 
@@ -734,18 +824,17 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
       CG_TRY(eval_at(gamma_bcd, grad_c, rows_c, cols_c, res_c, trc, nullptr));
     }
 
-    // search direction (sinkhorn_splr.cu:538-649)
-    CG_TRY_CUDA(cudaMemcpyAsync(hb.rhs2, grad, H * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    // search direction (sinkhorn_splr.cu:538-649); rhs2 = [g, y] was
+    // written by lowrank_kernel
     int sp_bad = 0;
     const int nrhs = (iter > 0) ? 2 : 1;
     CG_TRY(factor_solve_direction(&sp_bad, hb.rhs2, hb.sol2, nrhs));
     g_last_dir = path;
+    // Woodbury correction, scaling, <g, d>, and save_history (first H
+    // entries of gamma and g) in one launch
     { woodbury_kernel<<<1, 1024, 0, st>>>(hb.sol2, hb.sol2 + H, grad, hb.rhs2 + H, hb.s, H, reg, 1,
-                                        hb.dres); cg::count_launch(); }
+                                        hb.dres, gamma, gamma_prev, grad_prev); cg::count_launch(); }
     CG_TRY_CUDA(cudaGetLastError());
-    // save_history (first H entries)
-    CG_TRY_CUDA(cudaMemcpyAsync(gamma_prev, gamma, H * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    CG_TRY_CUDA(cudaMemcpyAsync(grad_prev, grad, H * sizeof(double), cudaMemcpyDeviceToDevice, st));
 
     // The line search's first trial point depends only on the previous step
     // length, so its pass is queued behind the direction solve and read back
@@ -753,21 +842,32 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     // two.  Its result is the one the line search (or, for an ascent
     // direction, the recomputation at the initial step) would produce.
     const double step_min = 1e-10, step_max = 2.0;
+    const double delta_max_spec = 1.1;  // the line search's extrapolation factor
     double init_step = std::min(1.0, 1.5 * alpha_step);
     init_step = std::max(init_step, step_min);
     init_step = std::min(init_step, step_max);
-    CG_TRY(trial_launch(init_step));
+    // speculative second point: the step the line search extrapolates to
+    // when the first trial still descends (its "case 2", from I_lo = 0)
+    auto spec_after = [&](double step, double I_lo) {
+      if (!speculate) return 0.0;
+      const double t = std::min(step_max, step + delta_max_spec * (step - I_lo));
+      return (t > step) ? t : 0.0;
+    };
+    CG_TRY(trial_launch(init_step, spec_after(init_step, 0.0)));
     DirRes dr{};
-    TResult t_first{};
+    TResult t_first[kMaxTrialSteps]{};
     int info2[2] = {0, 0};
     const int* isrc = nullptr;
     size_t ibytes = 0;
     factor_info_src(&isrc, &ibytes);
     {
+      const int nfirst = latest[1].step > 0.0 ? 2 : 1;
       const ReadSpan spans[3] = {{&dr, hb.dres, sizeof(DirRes)},
                                  {info2, isrc, ibytes},
-                                 {&t_first, res, sizeof(TResult)}};
+                                 {t_first, res, nfirst * sizeof(TResult)}};
       CG_TRY(read_device_spans(spans, 3, st));
+      trial_latch(t_first, nfirst);
+      cur_slot = 0;
     }
     if (take_injected_dirsolve_failure()) info2[0] = 1;  // host-side test hook
     if (sp_bad || info2[0] != 0 || info2[1] != 0) {
@@ -779,9 +879,10 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     yy = dr.yy;
     low_rank = dr.low_rank != 0;
 
-    // line_search_wolfe (sinkhorn_splr.cu:667-920)
+    // line_search_wolfe, ported from the reference's src/sinkhorn_splr.cu:667-920
+    // with its variable names and update order (decision parity, see above);
+    // each trial point is evaluated on the device by the fused pass.
     bool recompute_fg = false;
-    bool first_pending = true;  // t_first not yet consumed
     int trials = 0;
     double step_out = 0.0;
     double last_trial_gnorm = gnorm, last_trial_gfull = gfull;
@@ -813,12 +914,10 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
         const double delta_max = 1.1, delta_min = 7.0 / 12, shrink = 0.66;
         for (int it = 0; it < ls_max && !done; ++it) {
           TResult t{};
-          if (first_pending) {
-            t = t_first;  // step == init_step
-            first_pending = false;
-          } else {
-            CG_TRY(trial_at(step, t));
-          }
+          // the first trial (init_step) comes from the pass queued behind the
+          // direction solve; later ones from the latest pass when it holds
+          // the step, else from a new pass
+          CG_TRY(trial(step, spec_after(step, I_lo), t));
           ++trials;
           fx = t.f;
           dg = t.dg;
@@ -891,11 +990,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     const double gnorm_pre = gnorm;
     if (recompute_fg) {
       TResult t{};
-      if (first_pending && alpha_step == init_step) {
-        t = t_first;  // the queued pass already evaluated this point
-      } else {
-        CG_TRY(trial_at(alpha_step, t));
-      }
+      CG_TRY(trial(alpha_step, 0.0, t));  // no pass when the latest one holds it
       objfn = t.f;
       gnorm = t.gnorm;
       gfull = t.gfull;
@@ -903,6 +998,8 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
       gnorm = last_trial_gnorm;  // f, g and ||g|| of the last trial are current
       gfull = last_trial_gfull;
     }
+    CG_TRY(settle_slot());
+    speculate = small_problem || trials > 1;
 
     bool cand_accepted = false;
     if (use_cand) {

@@ -1,4 +1,4 @@
-// Fused plan pass (SPLR objective / gradient / line-search trial).
+// Fused plan pass (SPLR objective / gradient / line-search trials).
 //
 // Replaces, in one kernel per evaluation (reference benben-cd/curegot_backward):
 //   T_fused_kernel + obj_grad_kernel + launch_T_objfn_grad
@@ -35,19 +35,44 @@ struct TLayout<float> {
   static constexpr int VN = 4, NV = 2;  // 2 x float4 per lane, stride 128 columns
 };
 
-__device__ __forceinline__ double point_alpha(const TPassArgs& A, int i) {
-  return A.trial ? fma(A.step, A.direc[i], A.gamma_prev[i]) : A.gamma[i];
+__device__ __forceinline__ double point_alpha(const TPassArgs& A, int i, double step) {
+  return A.trial ? fma(step, A.direc[i], A.gamma_prev[i]) : A.gamma[i];
 }
-__device__ __forceinline__ double point_beta(const TPassArgs& A, int j) {
+__device__ __forceinline__ double point_beta(const TPassArgs& A, int j, double step) {
   const int k = A.n + j;
   if (j == A.m - 1 && A.trial) return 0.0;
-  return A.trial ? fma(A.step, A.direc[k], A.gamma_prev[k]) : A.gamma[k];
+  return A.trial ? fma(step, A.direc[k], A.gamma_prev[k]) : A.gamma[k];
+}
+
+// Slot k's view of the outputs and workspace (see TPassArgs).
+struct Slot {
+  double *gamma, *rows, *cols, *grad, *rowpart, *colpart, *scal;
+  TResult* res;
+  double step;
+};
+__device__ __forceinline__ Slot slot_of(const TPassArgs& A, int k) {
+  const size_t n = A.n, m = A.m;
+  Slot o;
+  o.gamma = A.gamma + k * (n + m);
+  o.rows = A.rows + k * n;
+  o.cols = A.cols + k * m;
+  o.grad = A.grad + k * (n + m - 1);
+  o.rowpart = A.rowpart + k * (size_t)A.strips * n;
+  o.colpart = A.colpart + k * (size_t)A.splits * m;
+  o.scal = A.scal + k * (size_t)(A.splits + A.strips) * kTScal;
+  o.res = A.res + k;
+  o.step = (k == 0) ? A.step : A.steps[k];
+  return o;
 }
 
 }  // namespace
 
-template <typename TM>
-__global__ void __launch_bounds__(kThreads, 3) tpass_kernel(const TPassArgs A) {
+// K trial points per pass (K = 1: the plain pass).  Every element of M is
+// loaded once; for each point k the exponent, the row / column sums and the
+// finishers' reductions are exactly those of a one-point pass at step k, in
+// the same order, so slot k is bitwise what a one-point pass would give.
+template <typename TM, int K>
+__global__ void __launch_bounds__(kThreads, (K == 1) ? 3 : 2) tpass_kernel(const TPassArgs A) {
   constexpr int VN = TLayout<TM>::VN, NV = TLayout<TM>::NV;
   constexpr int VS = 32 * VN;  // column stride between a lane's vectors
   __shared__ double tab[kExp2TableSize];
@@ -66,9 +91,12 @@ __global__ void __launch_bounds__(kThreads, 3) tpass_kernel(const TPassArgs A) {
   const TM* __restrict__ M = static_cast<const TM*>(A.M);
   const double s2 = A.s2;
   const bool vec_ok = (m % VN) == 0 && (reinterpret_cast<uintptr_t>(M) % 16) == 0;
+  double stp[K];
+#pragma unroll
+  for (int p = 0; p < K; ++p) stp[p] = (p == 0) ? A.step : A.steps[p];
 
   // this lane's columns and their scaled beta
-  double bs[NV * VN];
+  double bs[K][NV * VN];
   bool cin[NV * VN];
 #pragma unroll
   for (int v = 0; v < NV; ++v)
@@ -76,16 +104,24 @@ __global__ void __launch_bounds__(kThreads, 3) tpass_kernel(const TPassArgs A) {
     for (int k = 0; k < VN; ++k) {
       const int j = c0 + v * VS + lane * VN + k;
       cin[v * VN + k] = j < m;
-      bs[v * VN + k] = (j < m) ? point_beta(A, j) * s2 : 0.0;
-    }
-  double cacc[NV * VN];
 #pragma unroll
-  for (int q = 0; q < NV * VN; ++q) cacc[q] = 0.0;
+      for (int p = 0; p < K; ++p)
+        bs[p][v * VN + k] = (j < m) ? point_beta(A, j, stp[p]) * s2 : 0.0;
+    }
+  double cacc[K][NV * VN];
+#pragma unroll
+  for (int p = 0; p < K; ++p)
+#pragma unroll
+    for (int q = 0; q < NV * VN; ++q) cacc[p][q] = 0.0;
 
   for (int i = r0 + warp; i < r1; i += kWarps) {
-    const double as = point_alpha(A, i) * s2;
+    double as[K], rsum[K];
+#pragma unroll
+    for (int p = 0; p < K; ++p) {
+      as[p] = point_alpha(A, i, stp[p]) * s2;
+      rsum[p] = 0.0;
+    }
     const TM* __restrict__ Mi = M + (size_t)i * m;
-    double rsum = 0.0;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
       const int jb = c0 + v * VS + lane * VN;
@@ -99,26 +135,34 @@ __global__ void __launch_bounds__(kThreads, 3) tpass_kernel(const TPassArgs A) {
 #pragma unroll
       for (int k = 0; k < VN; ++k) {
         const int q = v * VN + k;
-        const double T = cin[q] ? exp2_f64(fma(-mv[k], s2, as + bs[q]), tab) : 0.0;
-        rsum += T;
-        cacc[q] += T;
+#pragma unroll
+        for (int p = 0; p < K; ++p) {
+          const double T = cin[q] ? exp2_f64(fma(-mv[k], s2, as[p] + bs[p][q]), tab) : 0.0;
+          rsum[p] += T;
+          cacc[p][q] += T;
+        }
       }
     }
-    rsum = warp_sum_down(rsum);
-    if (lane == 0) A.rowpart[(size_t)strip * n + i] = rsum;
+#pragma unroll
+    for (int p = 0; p < K; ++p) {
+      const double r = warp_sum_down(rsum[p]);
+      if (lane == 0) slot_of(A, p).rowpart[(size_t)strip * n + i] = r;
+    }
   }
 #pragma unroll
-  for (int v = 0; v < NV; ++v)
+  for (int p = 0; p < K; ++p) {
+    if (p > 0) __syncthreads();  // sm_col reused
 #pragma unroll
-    for (int k = 0; k < VN; ++k) sm_col[warp][v * VS + lane * VN + k] = cacc[v * VN + k];
-  __syncthreads();
-  {
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+      for (int k = 0; k < VN; ++k) sm_col[warp][v * VS + lane * VN + k] = cacc[p][v * VN + k];
+    __syncthreads();
     const int c = threadIdx.x;
     const int j = c0 + c;
     if (j < m) {
       double s = 0.0;
       for (int w = 0; w < kWarps; ++w) s += sm_col[w][c];
-      A.colpart[(size_t)split * m + j] = s;
+      slot_of(A, p).colpart[(size_t)split * m + j] = s;
     }
   }
 
@@ -126,91 +170,96 @@ __global__ void __launch_bounds__(kThreads, 3) tpass_kernel(const TPassArgs A) {
   unsigned int* cnt_split = A.counters;               // [splits]
   unsigned int* cnt_strip = A.counters + A.splits;    // [strips]
   unsigned int* cnt_all = A.counters + A.splits + A.strips;
-  const int H = n + m - 1;
   bool final_role = false;
 
-  // Row finisher: rows [r0, r1) of this split.
+  // Row finisher: rows [r0, r1) of this split, every slot.
   if (elect_last(&cnt_split[split], (unsigned)A.strips)) {
-    double s_r = 0, s_aa = 0, s_g2 = 0, s_gd = 0;
-    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-      double r = 0.0;
-      for (int s = 0; s < A.strips; ++s) r += ldcg(A.rowpart + (size_t)s * n + i);
-      const double al = point_alpha(A, i);
-      if (A.trial) A.gamma[i] = al;
-      const double g = r - A.ab[i];
-      A.rows[i] = r;
-      A.grad[i] = g;
-      s_r += r;
-      s_aa += A.ab[i] * al;
-      s_g2 += g * g;
-      if (A.direc) s_gd += g * A.direc[i];
-    }
-    s_r = cta_sum(s_r, red);
-    s_aa = cta_sum(s_aa, red);
-    s_g2 = cta_sum(s_g2, red);
-    s_gd = cta_sum(s_gd, red);
-    if (threadIdx.x == 0) {
-      double* o = A.scal + (size_t)split * kTScal;
-      o[0] = s_r;
-      o[1] = s_aa;
-      o[2] = s_g2;
-      o[3] = s_gd;
-      o[4] = 0.0;
+    for (int p = 0; p < K; ++p) {
+      const Slot S = slot_of(A, p);
+      double s_r = 0, s_aa = 0, s_g2 = 0, s_gd = 0;
+      for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        double r = 0.0;
+        for (int s = 0; s < A.strips; ++s) r += ldcg(S.rowpart + (size_t)s * n + i);
+        const double al = point_alpha(A, i, S.step);
+        if (A.trial) S.gamma[i] = al;
+        const double g = r - A.ab[i];
+        S.rows[i] = r;
+        S.grad[i] = g;
+        s_r += r;
+        s_aa += A.ab[i] * al;
+        s_g2 += g * g;
+        if (A.direc) s_gd += g * A.direc[i];
+      }
+      s_r = cta_sum(s_r, red);
+      s_aa = cta_sum(s_aa, red);
+      s_g2 = cta_sum(s_g2, red);
+      s_gd = cta_sum(s_gd, red);
+      if (threadIdx.x == 0) {
+        double* o = S.scal + (size_t)split * kTScal;
+        o[0] = s_r;
+        o[1] = s_aa;
+        o[2] = s_g2;
+        o[3] = s_gd;
+        o[4] = 0.0;
+      }
     }
     if (elect_last(cnt_all, nfin)) final_role = true;
   }
-  // Column finisher: columns of this strip.
+  // Column finisher: columns of this strip, every slot.
   if (elect_last(&cnt_strip[strip], (unsigned)A.splits)) {
-    double s_bb = 0, s_g2 = 0, s_gd = 0, s_gl = 0;
-    const int j = c0 + threadIdx.x;
-    if (j < m) {
-      double c = 0.0;
-      for (int s = 0; s < A.splits; ++s) c += ldcg(A.colpart + (size_t)s * m + j);
-      const double be = point_beta(A, j);
-      if (A.trial) A.gamma[n + j] = be;
-      A.cols[j] = c;
-      s_bb = A.ab[n + j] * be;
-      const double g = c - A.ab[n + j];
-      if (j < m - 1) {
-        A.grad[n + j] = g;
-        s_g2 = g * g;
-        if (A.direc) s_gd = g * A.direc[n + j];
-      } else {
-        s_gl = g * g;  // the gauge column: outside g, inside the full marginal error
+    for (int p = 0; p < K; ++p) {
+      const Slot S = slot_of(A, p);
+      double s_bb = 0, s_g2 = 0, s_gd = 0, s_gl = 0;
+      const int j = c0 + threadIdx.x;
+      if (j < m) {
+        double c = 0.0;
+        for (int s = 0; s < A.splits; ++s) c += ldcg(S.colpart + (size_t)s * m + j);
+        const double be = point_beta(A, j, S.step);
+        if (A.trial) S.gamma[n + j] = be;
+        S.cols[j] = c;
+        s_bb = A.ab[n + j] * be;
+        const double g = c - A.ab[n + j];
+        if (j < m - 1) {
+          S.grad[n + j] = g;
+          s_g2 = g * g;
+          if (A.direc) s_gd = g * A.direc[n + j];
+        } else {
+          s_gl = g * g;  // the gauge column: outside g, inside the full marginal error
+        }
       }
-    }
-    s_bb = cta_sum(s_bb, red);
-    s_g2 = cta_sum(s_g2, red);
-    s_gd = cta_sum(s_gd, red);
-    s_gl = cta_sum(s_gl, red);
-    if (threadIdx.x == 0) {
-      double* o = A.scal + (size_t)(A.splits + strip) * kTScal;
-      o[0] = 0.0;
-      o[1] = s_bb;
-      o[2] = s_g2;
-      o[3] = s_gd;
-      o[4] = s_gl;
+      s_bb = cta_sum(s_bb, red);
+      s_g2 = cta_sum(s_g2, red);
+      s_gd = cta_sum(s_gd, red);
+      s_gl = cta_sum(s_gl, red);
+      if (threadIdx.x == 0) {
+        double* o = S.scal + (size_t)(A.splits + strip) * kTScal;
+        o[0] = 0.0;
+        o[1] = s_bb;
+        o[2] = s_g2;
+        o[3] = s_gd;
+        o[4] = s_gl;
+      }
     }
     if (elect_last(cnt_all, nfin)) final_role = true;
   }
   if (!final_role) return;
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < K) {
+    const Slot S = slot_of(A, threadIdx.x);
     double tsum = 0, dot = 0, g2 = 0, gd = 0, gl = 0;
     for (int q = 0; q < A.splits + A.strips; ++q) {
-      const double* o = A.scal + (size_t)q * kTScal;
+      const double* o = S.scal + (size_t)q * kTScal;
       tsum += ldcg(o);
       dot += ldcg(o + 1);
       g2 += ldcg(o + 2);
       gd += ldcg(o + 3);
       gl += ldcg(o + 4);
     }
-    A.res->f = A.eta * tsum - dot;
-    A.res->gnorm = sqrt(g2);
-    A.res->dg = gd;
-    A.res->tsum = tsum;
-    A.res->gfull = sqrt(g2 + gl);
+    S.res->f = A.eta * tsum - dot;
+    S.res->gnorm = sqrt(g2);
+    S.res->dg = gd;
+    S.res->tsum = tsum;
+    S.res->gfull = sqrt(g2 + gl);
   }
-  (void)H;
 }
 
 void tpass_geometry(int n, int m, int sm_count, int& strips, int& splits) {
@@ -226,10 +275,15 @@ size_t tpass_workspace_doubles(int n, int m, int strips, int splits) {
 
 int launch_tpass(bool f32, const TPassArgs& a, cudaStream_t stream) {
   const int grid = a.strips * a.splits;
-  if (f32)
-    { tpass_kernel<float><<<grid, kThreads, 0, stream>>>(a); cg::count_launch(); }
+  const bool multi = a.trial && a.nsteps > 1;
+  if (f32 && multi)
+    { tpass_kernel<float, 2><<<grid, kThreads, 0, stream>>>(a); cg::count_launch(); }
+  else if (f32)
+    { tpass_kernel<float, 1><<<grid, kThreads, 0, stream>>>(a); cg::count_launch(); }
+  else if (multi)
+    { tpass_kernel<double, 2><<<grid, kThreads, 0, stream>>>(a); cg::count_launch(); }
   else
-    { tpass_kernel<double><<<grid, kThreads, 0, stream>>>(a); cg::count_launch(); }
+    { tpass_kernel<double, 1><<<grid, kThreads, 0, stream>>>(a); cg::count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
   return CG_OK;
 }

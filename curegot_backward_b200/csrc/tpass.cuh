@@ -15,6 +15,9 @@ struct TResult {
   double gfull;   // full marginal error ||(r - a, c - b)||_2 (all m columns)
 };
 
+// Trial points evaluated by one multi-step pass (batched line search).
+constexpr int kMaxTrialSteps = 2;
+
 struct TPassArgs {
   const void* M;
   int n, m;
@@ -26,6 +29,13 @@ struct TPassArgs {
   const double* direc;     // [n + m - 1]
   double step;
   int trial;
+  // Multi-step trial mode (nsteps > 1): step k = steps[k] (steps[0] = step)
+  // is evaluated as a separate trial point whose outputs and workspace sit at
+  // slot k: gamma + k (n + m), rows + k n, cols + k m, grad + k (n + m - 1),
+  // res + k, rowpart + k strips n, colpart + k splits m, scal + k (splits +
+  // strips) kTScal.  Each slot gets exactly the values of a one-step pass.
+  int nsteps;
+  double steps[kMaxTrialSteps];
   // outputs
   double* rows;            // [n]
   double* cols;            // [m]

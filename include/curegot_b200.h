@@ -115,6 +115,18 @@ int cg_bcd_f64_noalloc(const double* M, const double* a, const double* b, double
 int cg_bcd_set_cluster_path(int enable);
 
 /*
+ * Memory pipeline of the multi-CTA Sinkhorn passes (process-wide; default
+ * on).  When enabled, rows and column strips long enough to stream are
+ * brought into per-warp shared-memory rings by bulk asynchronous copies
+ * (three 2 KB stages per warp, completion on mbarriers with bounded waits)
+ * and read from there; disabled, the passes load M straight into registers.
+ * Same arithmetic in the same order: results are bitwise identical.  A
+ * staging wait that gives up ends the solve with CG_ERR_TIMEOUT.  No
+ * reference counterpart.
+ */
+int cg_bcd_set_staging(int enable);
+
+/*
  * Mixed-precision BCD: M stored in FP32, duals and all reductions in FP64.
  * Same contract as cg_bcd_f64; P (nullable) is written in FP64.  The
  * FP32-M form of cuda_sinkhorn_bcd; the stopping rule is evaluated with the

@@ -312,3 +312,18 @@ def ref_bcd(M, a, b, reg, tol=1e-6, max_iter=1000, x0=None):
     f(_p(M), _p(a), _p(b), _p(P), float(reg), int(max_iter), float(tol), n, m,
       ctypes.byref(niter), _p(x0), _p(dual))
     return {"niter": int(niter.value), "plan": P, "dual": dual}
+
+
+def ref_bcd_device(M_ptr, a_ptr, b_ptr, P_ptr, reg, tol, max_iter, n, m, dual_ptr):
+    """The reference's cuda_sinkhorn_bcd on device pointers (input and output
+    on the device), from oracle/_ref; returns niter.  For timing its GPU path
+    beside ours on data already in HBM."""
+    L = ctypes.CDLL(_REF_PATH)
+    f = L.ref_sinkhorn_bcd_device
+    vp = ctypes.c_void_p
+    f.argtypes = [vp, vp, vp, vp, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                  ctypes.c_int, _ip, vp, vp]
+    niter = ctypes.c_int(0)
+    f(M_ptr, a_ptr, b_ptr, P_ptr, float(reg), int(max_iter), float(tol), n, m,
+      ctypes.byref(niter), None, dual_ptr)
+    return int(niter.value)

@@ -14,3 +14,13 @@ extern "C" int ref_sinkhorn_bcd_host(const double* M, const double* a, const dou
   cuda_sinkhorn_bcd(M, a, b, P, reg, max_iter, tol, n, m, niter, x0, dual, false, false);
   return 0;
 }
+
+// Device-resident inputs and outputs (input_on_device = output_on_device =
+// true): what a timing of the reference's own GPU path on data already in
+// HBM calls.
+extern "C" int ref_sinkhorn_bcd_device(const double* M, const double* a, const double* b,
+                                       double* P, double reg, int max_iter, double tol, int n,
+                                       int m, int* niter, const double* x0, double* dual) {
+  cuda_sinkhorn_bcd(M, a, b, P, reg, max_iter, tol, n, m, niter, x0, dual, true, true);
+  return 0;
+}

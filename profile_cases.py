@@ -1,11 +1,11 @@
 """Fixed single-GPU cases of the hot kernels, for timing and for profilers.
 
-    python -m curegot_backward_b200.profile_cases bcd --n 8192 --m 8192 --precision mixed
-    python -m curegot_backward_b200.profile_cases splr --n 4096 --m 4096 --density 0.1
-    python -m curegot_backward_b200.profile_cases backward --n 2048 --m 2560
-    python -m curegot_backward_b200.profile_cases precision --n 16384 --algo splr
-    python -m curegot_backward_b200.profile_cases points --n 16384 --m 16384 --d 32 --iters 20
-    python -m curegot_backward_b200.profile_cases batch --n 512 --m 640 --batch 16
+    python profile_cases.py bcd --n 8192 --m 8192 --precision mixed
+    python profile_cases.py splr --n 4096 --m 4096 --density 0.1
+    python profile_cases.py backward --n 2048 --m 2560
+    python profile_cases.py precision --n 16384 --algo splr
+    python profile_cases.py points --n 16384 --m 16384 --d 32 --iters 20
+    python profile_cases.py batch --n 512 --m 640 --batch 16
 
 Each case builds a seeded synthetic problem on cuda:0, runs it once to warm
 up, then times `--reps` runs with CUDA events on the launching stream and
@@ -36,15 +36,18 @@ import argparse
 import json
 import os
 
+import sys
+
 import torch
 
-from . import _solvers, synthetic
-from .backward import solve_backward
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+
+from curegot_backward_b200 import _solvers, synthetic  # noqa: E402
+from curegot_backward_b200.backward import solve_backward  # noqa: E402
 
 
 def _peak():
-    p = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
-                     "MEASURED_PEAKS.json")
+    p = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
     try:
         return float(json.load(open(p))["hbm_gbs"]), "measured"
     except Exception:
@@ -72,6 +75,7 @@ def _time(fn, reps):
 def case_bcd(a):
     import curegot_backward_b200 as cg
     cg.set_bcd_cluster_path(a.path != "multi")
+    cg.set_bcd_staging(a.staging == "on")
     dev = torch.device("cuda", 0)
     dtype = torch.float32 if a.precision == "mixed" else torch.float64
     M, am, bm = _gauss(a.n, a.m, a.d, a.seed, dev, dtype)
@@ -82,9 +86,59 @@ def case_bcd(a):
     bytes_ = 2.0 * a.n * a.m * M.element_size() * niter
     gbs = bytes_ / (ms / 1e3) / 1e9
     peak, kind = _peak()
-    return {"case": "bcd", "path": a.path, "n": a.n, "m": a.m, "precision": a.precision, "eta": a.eta,
+    return {"case": "bcd", "path": a.path, "staging": a.staging, "n": a.n, "m": a.m,
+            "precision": a.precision, "eta": a.eta,
             "iterations": niter, "ms_per_solve": ms, "us_per_iteration": 1e3 * ms / niter,
             "algorithmic_GBps": gbs, "peak_GBps": peak, "peak_kind": kind, "frac": gbs / peak}
+
+
+def case_c0(a):
+    """Sinkhorn at the C0 configuration (n = 512, m = 640, X, Y ~ U[0,1]^8,
+    M = mean squared difference, uniform marginals, eta = 0.05, tol = 1e-8):
+    the reference's own GPU solver (cuda_sinkhorn_bcd built from its sources
+    into oracle/_ref, device-resident inputs and outputs) beside this
+    library's FP64 solver (cluster path and multi-CTA passes) and mixed
+    solver, each timed with CUDA events over --reps solves, plan included."""
+    import ctypes
+
+    import numpy as np
+
+    import curegot_backward_b200 as cg
+    import oracle
+    dev = torch.device("cuda", 0)
+    M, an, bn, eta = synthetic.config0()
+    Md = torch.tensor(M, device=dev)
+    ad, bd = torch.tensor(an, device=dev), torch.tensor(bn, device=dev)
+    n, m = M.shape
+    P = torch.empty((n, m), dtype=torch.float64, device=dev)
+    dual = torch.empty(n + m, dtype=torch.float64, device=dev)
+    out = {"case": "c0", "n": n, "m": m, "eta": eta, "tol": 1e-8, "reps": a.reps}
+    if oracle.ref_bcd_available():
+        ms, it = _time(lambda: oracle.ref_bcd_device(Md.data_ptr(), ad.data_ptr(), bd.data_ptr(),
+                                                     P.data_ptr(), eta, 1e-8, 100000, n, m,
+                                                     dual.data_ptr()), a.reps)
+        ref_dual = dual.clone()
+        out["reference_gpu"] = {"ms_per_solve": ms, "niter": it}
+    else:
+        ref_dual = None
+        out["reference_gpu"] = None
+    for name, cluster, prec in (("ours_fp64_cluster", True, "fp64"),
+                                ("ours_fp64_passes", False, "fp64"),
+                                ("ours_mixed_cluster", True, "mixed")):
+        cg.set_bcd_cluster_path(cluster)
+        Mx = Md if prec == "fp64" else Md.float()
+        ms, res = _time(lambda: _solvers._bcd_device(Mx, ad, bd, eta, 1e-8, 100000, None, prec),
+                        a.reps)
+        entry = {"ms_per_solve": ms, "niter": res[0]}
+        if ref_dual is not None and prec == "fp64":
+            d = (res[2] - ref_dual).abs().max().item()
+            entry["max_dual_diff_vs_reference"] = d
+        out[name] = entry
+    cg.set_bcd_cluster_path(True)
+    if out["reference_gpu"]:
+        out["speedup_fp64_cluster"] = out["reference_gpu"]["ms_per_solve"] / \
+            out["ours_fp64_cluster"]["ms_per_solve"]
+    return out
 
 
 def case_splr(a):
@@ -122,6 +176,18 @@ def case_backward(a):
             "peak_GBps": peak, "peak_kind": kind, "frac": gbs / peak}
 
 
+def dual_objective(M64, a, b, dual, eta, rows_per_chunk=1024):
+    """f = eta * sum(T) - <alpha, a> - <beta, b> in FP64 (row chunks), the
+    dual objective the SPLR solver minimises."""
+    n, m = M64.shape
+    al, be = dual[:n].double(), dual[n:].double()
+    tot = 0.0
+    for i0 in range(0, n, rows_per_chunk):
+        i1 = min(n, i0 + rows_per_chunk)
+        tot += float(torch.exp((al[i0:i1, None] + be[None, :] - M64[i0:i1]) / eta).sum())
+    return eta * tot - float((al * a).sum()) - float((be * b).sum())
+
+
 def fp64_marginal_errors(M, a, b, dual, eta, rows_per_chunk=1024):
     """||T 1 - a||_2 and ||T^T 1 - b||_2 of T = exp((alpha_i + beta_j - M_ij) / eta),
     evaluated in FP64 in row chunks."""
@@ -153,15 +219,31 @@ def case_precision(a):
     e1.record()
     torch.cuda.synchronize()
     niter, dual = (out[0], out[2]) if a.algo == "bcd" else (out["niter"], out["dual"])
+    seconds = e0.elapsed_time(e1) / 1e3
     row_err, col_err = fp64_marginal_errors(M, am, bm, dual, eta)
-    return {"case": "precision", "algo": a.algo, "n": a.n, "m": a.n, "eta": eta,
-            "M_dtype": "float32", "iterations": int(niter), "max_iter": a.max_iter,
-            "seconds": e0.elapsed_time(e1) / 1e3, "fp64_row_err": row_err,
-            "fp64_col_err": col_err, "tol": a.tol}
+    res = {"case": "precision", "algo": a.algo, "n": a.n, "m": a.n, "eta": eta,
+           "M_dtype": "float32", "iterations": int(niter), "max_iter": a.max_iter,
+           "seconds": seconds, "fp64_row_err": row_err, "fp64_col_err": col_err, "tol": a.tol}
+    if a.fp64_reference:
+        # objective error against the plain FP64 solve of the same FP32-valued
+        # M (upcast exactly): the FP64 path is the one held to the oracle
+        M64 = M.double()
+        if a.algo == "bcd":
+            _, _, ref = _solvers._bcd_device(M64, am, bm, eta, a.tol, a.max_iter, None, "fp64",
+                                             want_plan=False)
+        else:
+            ref = _solvers._splr_device(M64, am, bm, eta, a.tol, a.max_iter, 0, None, "fp64",
+                                        0.01, 1e-3, 30, 3, want_plan=False)["dual"]
+        f_mixed = dual_objective(M64, am, bm, dual, eta)
+        f_ref = dual_objective(M64, am, bm, ref, eta)
+        del M64
+        res["objective_fp64_ref"] = f_ref
+        res["rel_objective_err"] = abs(f_mixed - f_ref) / abs(f_ref)
+    return res
 
 
 def case_points(a):
-    from .points import cost_from_points, sinkhorn_bcd_points
+    from curegot_backward_b200.points import cost_from_points, sinkhorn_bcd_points
     dev = torch.device("cuda", 0)
     g = torch.Generator(device=dev).manual_seed(a.seed)
     X = torch.rand(a.n, a.d, generator=g, device=dev).bfloat16()
@@ -224,7 +306,8 @@ def case_batch(a):
 
 def main(argv=None):
     p = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    p.add_argument("case", choices=["bcd", "splr", "backward", "precision", "points", "batch"])
+    p.add_argument("case", choices=["bcd", "splr", "backward", "precision", "points", "batch",
+                                    "c0"])
     p.add_argument("--n", type=int, default=8192)
     p.add_argument("--m", type=int, default=8192)
     p.add_argument("--d", type=int, default=16)
@@ -234,6 +317,8 @@ def main(argv=None):
     p.add_argument("--path", default="auto", choices=["auto", "multi"],
                    help="bcd: auto = cluster-resident solver when the problem fits")
     p.add_argument("--density", type=float, default=None, help="splr: density_max kwarg")
+    p.add_argument("--staging", default="on", choices=["on", "off"],
+                   help="bcd: shared-memory staging of the passes")
     p.add_argument("--solver", default=None, choices=[None, "auto", "dense", "peel", "sparse"])
     p.add_argument("--tol", type=float, default=1e-8)
     p.add_argument("--precond", default="diag", choices=["none", "diag", "splr"])
@@ -241,11 +326,15 @@ def main(argv=None):
     p.add_argument("--seed", type=int, default=7)
     p.add_argument("--algo", default="splr", choices=["bcd", "splr"], help="precision case")
     p.add_argument("--max-iter", type=int, default=100000, help="precision case")
+    p.add_argument("--fp64-reference", action="store_true",
+                   help="precision case: also solve in plain FP64 and report the relative "
+                        "objective error of the mixed solution")
     p.add_argument("--compare", action="store_true", help="points: also time the stored cost")
     p.add_argument("--batch", type=int, default=16, help="batch case: problems per batch")
     a = p.parse_args(argv)
     res = {"bcd": case_bcd, "splr": case_splr, "backward": case_backward,
-           "precision": case_precision, "points": case_points, "batch": case_batch}[a.case](a)
+           "precision": case_precision, "points": case_points, "batch": case_batch,
+           "c0": case_c0}[a.case](a)
     print(json.dumps(res), flush=True)
 
 

@@ -12,8 +12,14 @@ row pointers with a SHA-256 of its column indices.
 
 ``backward_c3_2048x2560.npz`` -- differentiation configuration, n = 2048,
 m = 2560: X, Y ~ U[0, 1]^{32}, M_ij = mean over the 32 features of
-(x_i - y_j)^2, uniform marginals, eta = 0.05, tol = 1e-10, loss = sum(T^2)
-so G = dL/dT = 2T.  The forward is the oracle's SPLR; the backward is the
+(x_i - y_j)^2, uniform marginals, eta = 0.05, loss = sum(T^2) so
+G = dL/dT = 2T, forward tol = 1e-9.  (At tol = 1e-10 the SPLR iteration of
+the reference does not converge on this problem: its first Newton step
+reaches ||g|| = 7.8e-10, and the oracle then ran to its 2000-iteration cap,
+because below that the Wolfe line search compares objective decreases at
+the FP64 resolution of f ~ 0.67.  1e-9 is the tightest tolerance reached;
+the reference's own finite-difference harness runs at 1e-8 for the same
+reason, validate_stage4_autograd.py:314-330.)  The forward is the oracle's SPLR; the backward is the
 reference's own curegot/_backward_core.py and curegot/backward.py, loaded
 unmodified from the reference checkout and run on CPU torch, with its
 diagonal preconditioner D_A^{-1} taken from the oracle's context CSR (the
@@ -45,6 +51,7 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 C1_SEED, C3_SEED = 101, 303
+C3_TOL = 1e-9
 FD_SEED, FD_ENTRIES = 7, 64
 
 
@@ -143,7 +150,7 @@ def make_c3():
     M, a, b, eta = c3_problem()
     n, m = M.shape
     t = time.time()
-    r = oracle.splr(M, a, b, eta, tol=1e-10, max_iter=2000, want_plan=True)
+    r = oracle.splr(M, a, b, eta, tol=C3_TOL, max_iter=2000, want_plan=True)
     print(f"c3: oracle SPLR niter {r['niter']} in {time.time() - t:.0f} s", flush=True)
     T = torch.from_numpy(r["plan"])
     G = 2.0 * T
@@ -155,8 +162,10 @@ def make_c3():
           f"{time.time() - t:.0f} s", flush=True)
     grad = out["grad"].numpy()
     ent = fd_entries(n, m)
+    assert r["converged"], "the C3 forward must converge for the fixture"
     np.savez_compressed(os.path.join(HERE, "backward_c3_2048x2560.npz"), M_sha=sha(M), eta=eta,
-                        tol=1e-10, niter=r["niter"], converged=r["converged"], dual=r["dual"],
+                        tol=C3_TOL, niter=r["niter"], converged=r["converged"], dual=r["dual"],
+                        trace=r["trace"],
                         lam=out["lambda"].numpy(), pcg_iterations=out["iterations"],
                         fd_entries=ent, grad_at_entries=grad[ent[:, 0], ent[:, 1]],
                         grad_sum=grad.sum(), grad_abs_sum=np.abs(grad).sum(),

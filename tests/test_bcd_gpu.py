@@ -199,3 +199,33 @@ def test_cluster_path_warm_start_and_truncation(cuda_dev, bcd_path):
     ow = oracle.bcd(M, a, b, 0.02, tol=1e-9, max_iter=5000, x0=full["dual"])
     assert warm["niter"] == ow["niter"]
     assert np.abs(warm["plan"] - ow["plan"]).max() <= 1e-12
+
+
+@pytest.mark.parametrize("precision,n,m", [("fp64", 1500, 4096), ("mixed", 2300, 8192),
+                                           ("mixed", 3000, 2052), ("fp64", 700, 5003)])
+def test_staged_passes_are_bitwise_the_unstaged_ones(cuda_dev, precision, n, m):
+    """The shared-memory staging of the passes changes the memory pipeline
+    only: duals and iteration counts are bitwise those of the register
+    path (m = 5003 is not a multiple of the vector width: both take the
+    scalar path)."""
+    import torch
+    from curegot_backward_b200 import _solvers
+    g = torch.Generator(device=cuda_dev).manual_seed(n + m)
+    X = torch.randn(n, 8, generator=g, device=cuda_dev, dtype=torch.float64)
+    Y = torch.randn(m, 8, generator=g, device=cuda_dev, dtype=torch.float64)
+    M = torch.cdist(X, Y) ** 2
+    M = M / M.max()
+    if precision == "mixed":
+        M = M.float()
+    a = torch.full((n,), 1.0 / n, dtype=torch.float64, device=cuda_dev)
+    b = torch.full((m,), 1.0 / m, dtype=torch.float64, device=cuda_dev)
+    out = {}
+    try:
+        for on in (True, False):
+            cg.set_bcd_staging(on)
+            out[on] = _solvers._bcd_device(M, a, b, 0.02, 1e-8, 3000, None, precision,
+                                           want_plan=False)
+    finally:
+        cg.set_bcd_staging(True)
+    assert out[True][0] == out[False][0]
+    assert torch.equal(out[True][2], out[False][2])

@@ -12,7 +12,7 @@ import torch
 
 import oracle
 from curegot_backward_b200 import _solvers, synthetic
-from curegot_backward_b200.profile_cases import fp64_marginal_errors
+from profile_cases import fp64_marginal_errors
 
 pytestmark = pytest.mark.gpu
 
