@@ -115,6 +115,8 @@ SIGNATURES = {
                            c_double, c_int, c_double, c_int, c_int_p, c_void_p, c_int_p,
                            c_void_p],
     "cg_points_set_wait_limit": [ctypes.c_longlong],
+    "cg_points_cost_stats_bf16": [c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_void_p,
+                                  c_void_p],
     "cg_bcd_mixed": [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_double, c_int,
                      c_int, c_int_p, c_void_p, c_void_p, c_void_p],
     "cg_transport_plan_f64": [c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_int, c_int,
@@ -133,6 +135,9 @@ SIGNATURES = {
     "cg_ctx_destroy": [c_void_p],
     "cg_backward_f64": [c_void_p, c_void_p, c_void_p, c_double, c_int, c_double, c_int, c_int,
                         c_int, c_void_p, c_void_p, c_int_p, c_int_p, c_void_p],
+    "cg_backward_batch_f64": [c_void_p, c_void_p, c_void_p, c_double, c_int, c_double, c_int,
+                              c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                              c_void_p],
     "cg_t_values_f64": [c_void_p, c_void_p, c_void_p, c_int, c_int, c_double, c_void_p,
                         c_void_p, c_void_p],
     "cg_test_t_sparsify_f64": [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_double,

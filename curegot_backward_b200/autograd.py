@@ -25,7 +25,7 @@ import torch
 from torch.autograd.function import once_differentiable
 
 from . import _solvers
-from .backward import _VALID_PRECONDITIONERS, solve_backward
+from .backward import _VALID_PRECONDITIONERS, solve_backward, solve_backward_batch
 
 __all__ = ["splr_ot", "splr_ot_with_info", "splr_ot_batch", "SPLROT", "SPLROTFunction"]
 
@@ -186,16 +186,112 @@ def _worker_streams(dev, k):
         return lst[:k]
 
 
-def splr_ot_batch(M, a, b, *, eta, **kwargs):
+def _batch_forward(M, a, b, eta, tol, max_iter, density, cand):
+    """Native forwards of the B problems: concurrent on worker streams when
+    the problems are small, one after another otherwise.  Returns the plans
+    and backward contexts; raises on non-convergence like splr_ot."""
+    B = M.shape[0]
+    W = min(B, _BATCH_WORKERS)
+
+    def one(i):
+        out = _forward_native(M[i], a[i], b[i], eta, tol, max_iter, density, cand)
+        if not bool(out["converged"]):
+            raise RuntimeError(f"splr_ot_batch: forward solver did not converge for problem {i} "
+                               f"(niter={int(out['niter'])}, max_iter={max_iter}, tol={tol}); "
+                               "relax tol or increase max_iter")
+        return out["plan"], out["context"]
+
+    if W <= 1 or M.shape[1] * M.shape[2] > _BATCH_MAX_ELEMS:
+        return [one(i) for i in range(B)]
+    dev = M.device
+    main = torch.cuda.current_stream(dev)
+    ready = main.record_event()  # inputs (and anything queued before) are done
+    free = queue.Queue()
+    for st in _worker_streams(dev, W):
+        free.put(st)
+
+    def solve(i):
+        st = free.get()
+        try:
+            with torch.cuda.device(dev), torch.cuda.stream(st):
+                st.wait_event(ready)
+                P, c = one(i)
+                done = st.record_event()
+            return P, c, done
+        finally:
+            free.put(st)
+
+    with ThreadPoolExecutor(max_workers=W) as ex:
+        results = [f.result() for f in [ex.submit(solve, i) for i in range(B)]]
+    out = []
+    for P, c, done in results:
+        main.wait_event(done)
+        P.record_stream(main)  # the plan is consumed on the caller's stream
+        out.append((P, c))
+    return out
+
+
+class SPLROTBatchFunction(torch.autograd.Function):
+    """[B, n, m] forward: B native SPLR solves keeping their contexts.
+    Backward: one batched native PCG over the B problems (diagonal or no
+    preconditioner: cg_backward_batch_f64, every PCG iteration of all
+    unfinished problems in one launch); the "splr" preconditioner runs the
+    per-problem backward."""
+
+    @staticmethod
+    def forward(ctx, M, a, b, eta, tol, max_iter, density, candidate_sinkhorn_iter,
+                backward_preconditioner, backward_tol, backward_max_iter):
+        res = _batch_forward(M, a, b, eta, tol, max_iter, density, candidate_sinkhorn_iter)
+        T = torch.stack([P for P, _ in res])
+        ctx.save_for_backward(T)
+        ctx.backward_contexts = [c for _, c in res]
+        ctx.eta = eta
+        ctx.backward_preconditioner = backward_preconditioner
+        ctx.backward_tol = backward_tol
+        ctx.backward_max_iter = backward_max_iter
+        return T
+
+    @staticmethod
+    @once_differentiable
+    def backward(ctx, grad_output):
+        (T,) = ctx.saved_tensors
+        G = grad_output if grad_output.is_contiguous() else grad_output.contiguous()
+        pre = ctx.backward_preconditioner
+        if pre == "splr":
+            grads = []
+            for i, c in enumerate(ctx.backward_contexts):
+                r = solve_backward(T[i], G[i], c, ctx.eta, preconditioner=pre,
+                                   tol=ctx.backward_tol, max_iter=ctx.backward_max_iter)
+                if not r["converged"]:
+                    raise RuntimeError(f"splr_ot_batch: backward PCG did not converge for "
+                                       f"problem {i} (iterations={r['iterations']})")
+                grads.append(r["grad"])
+            grad = torch.stack(grads)
+        else:
+            res = solve_backward_batch(T, G, ctx.backward_contexts, ctx.eta, preconditioner=pre,
+                                       tol=ctx.backward_tol, max_iter=ctx.backward_max_iter)
+            bad = [i for i, ok in enumerate(res["converged"]) if not ok]
+            if bad:
+                raise RuntimeError(f"splr_ot_batch: backward PCG did not converge for problems "
+                                   f"{bad} (max_iter={ctx.backward_max_iter}, "
+                                   f"tol={ctx.backward_tol}, preconditioner='{pre}')")
+            grad = res["grad"]
+        return (grad, None, None, None, None, None, None, None, None, None, None)
+
+
+def splr_ot_batch(M, a, b, *, eta, tol=1e-6, max_iter=1000, density=None,
+                  candidate_sinkhorn_iter=3, backward_preconditioner="diag", backward_tol=1e-12,
+                  backward_max_iter=2000):
     """[B, n, m] costs, [B, n] and [B, m] marginals -> [B, n, m] plans;
     gradients flow to M.
 
     The reference (curegot/autograd.py:340-367) solves the B problems one
-    after another.  Here, for problems of at most 2^21 cost entries, up to 8
-    solves run at once, each on its own worker thread and CUDA stream; every
-    solve is the same native call as splr_ot on the same inputs, so plans
-    and gradients are bitwise those of the sequential loop.  Each problem's
-    backward runs on its forward stream."""
+    after another and runs B backward solves.  Here, for problems of at most
+    2^21 cost entries, up to 8 forward solves run at once, each on its own
+    worker thread and CUDA stream (the same native call as splr_ot, so the
+    plans are bitwise those of the sequential loop), and the backward is one
+    batched native PCG over the B problems whose per-problem values are those
+    of solve_backward."""
     if M.dim() != 3:
         raise ValueError(f"splr_ot_batch: M must be [B, n, m], got shape {tuple(M.shape)}")
     B = M.shape[0]
@@ -203,35 +299,24 @@ def splr_ot_batch(M, a, b, *, eta, **kwargs):
         raise ValueError(f"splr_ot_batch: a must be [B, n], got shape {tuple(a.shape)}")
     if tuple(b.shape) != (B, M.shape[2]):
         raise ValueError(f"splr_ot_batch: b must be [B, m], got shape {tuple(b.shape)}")
-    W = min(B, _BATCH_WORKERS)
-    if (W <= 1 or not (isinstance(M, torch.Tensor) and M.is_cuda)
-            or M.shape[1] * M.shape[2] > _BATCH_MAX_ELEMS):
-        return torch.stack([splr_ot(M[i], a[i], b[i], eta=eta, **kwargs) for i in range(B)])
-    dev = M.device
-    main = torch.cuda.current_stream(dev)
-    ready = main.record_event()  # inputs (and anything queued before) are done
-    free = queue.Queue()
-    for st in _worker_streams(dev, W):
-        free.put(st)
-    grad_on = torch.is_grad_enabled()
-
-    def solve(i):
-        st = free.get()
-        try:
-            with torch.cuda.device(dev), torch.cuda.stream(st), torch.set_grad_enabled(grad_on):
-                st.wait_event(ready)
-                P = splr_ot(M[i], a[i], b[i], eta=eta, **kwargs)
-                done = st.record_event()
-            return P, done
-        finally:
-            free.put(st)
-
-    with ThreadPoolExecutor(max_workers=W) as ex:
-        results = [f.result() for f in [ex.submit(solve, i) for i in range(B)]]
-    for P, done in results:
-        main.wait_event(done)
-        P.record_stream(main)  # the plan is consumed on the caller's stream
-    return torch.stack([P for P, _ in results])
+    if torch.is_autocast_enabled():
+        raise RuntimeError("splr_ot_batch: AMP/autocast is unsupported (float64 solver); "
+                           "disable autocast for this call")
+    if B == 0:
+        raise ValueError("splr_ot_batch: empty batch")
+    _check_inputs(M[0], a[0], b[0])
+    _validate_scalars(eta, tol, max_iter, density, candidate_sinkhorn_iter, backward_tol,
+                      backward_max_iter)
+    if a.requires_grad or b.requires_grad:
+        raise NotImplementedError("splr_ot_batch: gradients w.r.t. a/b are not supported "
+                                  "(only dL/dM)")
+    if backward_preconditioner not in _VALID_PRECONDITIONERS:
+        raise ValueError(f"splr_ot_batch: invalid backward_preconditioner "
+                         f"'{backward_preconditioner}'; expected one of: "
+                         f"{' | '.join(_VALID_PRECONDITIONERS)}")
+    return SPLROTBatchFunction.apply(M, a, b, float(eta), float(tol), int(max_iter), density,
+                                     int(candidate_sinkhorn_iter), backward_preconditioner,
+                                     float(backward_tol), int(backward_max_iter))
 
 
 class SPLROT(torch.nn.Module):

@@ -17,7 +17,7 @@ import torch
 
 from . import _native
 
-__all__ = ["solve_backward", "select_preconditioner"]
+__all__ = ["solve_backward", "solve_backward_batch", "select_preconditioner"]
 
 _VALID_PRECONDITIONERS = ("diag", "splr", "none")
 _MODE = {"none": _native.CG_PRECOND_NONE, "diag": _native.CG_PRECOND_DIAG,
@@ -72,3 +72,42 @@ def solve_backward(T, G, ctx, eta, *, preconditioner="diag", tol=1e-12, max_iter
                      torch.cuda.current_stream(dev).cuda_stream)
     return {"lambda": lam, "grad": grad, "iterations": int(iters.value),
             "converged": bool(conv.value), "preconditioner": preconditioner}
+
+
+def solve_backward_batch(T, G, ctxs, eta, *, preconditioner="diag", tol=1e-12, max_iter=2000):
+    """solve_backward for B problems of one shape in one native call
+    (cg_backward_batch_f64): T, G [B, n, m]; ctxs: the B backward contexts
+    (may be None with preconditioner="none").  Returns ``lambda`` [B, n+m-1],
+    ``grad`` [B, n, m], and per-problem ``iterations`` / ``converged`` lists;
+    each problem's values are those of solve_backward.  The "splr"
+    preconditioner is not batched."""
+    if T.dim() != 3 or G.shape != T.shape:
+        raise ValueError("T and G must be [B, n, m] tensors of one shape")
+    if preconditioner not in ("diag", "none"):
+        raise ValueError("solve_backward_batch: preconditioner must be 'diag' or 'none'")
+    if not T.is_cuda:
+        raise RuntimeError("solve_backward_batch: T must be a CUDA tensor (no CPU fallback)")
+    B, n, m = (int(x) for x in T.shape)
+    if preconditioner == "diag" and ctxs is None:
+        raise ValueError("solve_backward_batch: preconditioner 'diag' needs the contexts")
+    if ctxs is not None and len(ctxs) != B:
+        raise ValueError("solve_backward_batch: one context per problem")
+    modes = [select_preconditioner(c, preconditioner) for c in ctxs] if ctxs is not None else \
+        [select_preconditioner(None, preconditioner)]
+    mode = modes[0]
+    dev = T.device
+    Td = T.detach().to(dtype=torch.float64).contiguous()
+    Gd = G.detach().to(device=dev, dtype=torch.float64).contiguous()
+    lam = torch.empty((B, n + m - 1), dtype=torch.float64, device=dev)
+    grad = torch.empty((B, n, m), dtype=torch.float64, device=dev)
+    iters = (ctypes.c_int * B)()
+    conv = (ctypes.c_int * B)()
+    handles = None
+    if ctxs is not None and mode != 0:
+        handles = (ctypes.c_void_p * B)(*[c._handle.value for c in ctxs])
+    with torch.cuda.device(dev):
+        _native.call("cg_backward_batch_f64", Td.data_ptr(), Gd.data_ptr(), handles, float(eta),
+                     mode, float(tol), int(max_iter), B, n, m, lam.data_ptr(), grad.data_ptr(),
+                     iters, conv, torch.cuda.current_stream(dev).cuda_stream)
+    return {"lambda": lam, "grad": grad, "iterations": list(iters),
+            "converged": [bool(x) for x in conv], "preconditioner": preconditioner}

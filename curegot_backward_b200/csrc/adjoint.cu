@@ -17,6 +17,7 @@
 // deterministic, no atomics on values.
 #include <algorithm>
 #include <cmath>
+#include <vector>
 
 #include "splr.cuh"
 #include "tpass.cuh"
@@ -124,14 +125,15 @@ __device__ void pcg_update(const AdjArgs& A, bool part2, double* red) {
 
 // mode 0: RHS pass (row/col sums of T and of G*T, then PCG init)
 // mode 1: Q p pass (then the PCG update)
+// cta: this CTA's index within the problem's tile grid.
 template <int MODE>
-__global__ void __launch_bounds__(kThreads, 3) adj_pass_kernel(const AdjArgs A, int fused) {
+__device__ __forceinline__ void adj_pass_body(const AdjArgs& A, int fused, int cta) {
   __shared__ double sm_col[2][kWarps][kTStrip];
   __shared__ double red[kWarps];
   const int n = A.n, m = A.m;
   if (MODE == 1 && ldcg(&A.st->done)) return;
-  const int strip = blockIdx.x % A.strips;
-  const int split = blockIdx.x / A.strips;
+  const int strip = cta % A.strips;
+  const int split = cta / A.strips;
   const int rows_per = (n + A.splits - 1) / A.splits;
   const int r0 = split * rows_per, r1 = min(n, r0 + rows_per);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -317,6 +319,20 @@ __global__ void __launch_bounds__(kThreads, 3) adj_pass_kernel(const AdjArgs A, 
   }
 }
 
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 3) adj_pass_kernel(const AdjArgs A, int fused) {
+  adj_pass_body<MODE>(A, fused, (int)blockIdx.x);
+}
+
+// B problems of one shape in one launch: CTAs [b * per, (b + 1) * per) are
+// problem b's tile grid.  Each problem's arithmetic is adj_pass_kernel's.
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 3) adj_pass_batch_kernel(const AdjArgs* __restrict__ probs,
+                                                                     int per, int fused) {
+  const int b = blockIdx.x / per;
+  adj_pass_body<MODE>(probs[b], fused, (int)blockIdx.x - b * per);
+}
+
 // Second half of a PCG step when the preconditioner runs outside the pass.
 __global__ void __launch_bounds__(1024) pcg_update2_kernel(double* r, double* z, double* p,
                                                            int H, PcgState* st) {
@@ -376,15 +392,35 @@ __global__ void assemble_grad_kernel(const double* __restrict__ T, const double*
   }
 }
 
-__global__ void pcg_state_init(PcgState* st, int max_iter, int precond, double tol) {
-  st->k = 0;
-  st->done = 0;
-  st->converged = 0;
-  st->breakdown = 0;
-  st->max_iter = max_iter;
-  st->precond = precond;
-  st->allzero = 0;
-  st->tol = tol;
+__global__ void pcg_state_init(PcgState* st, int max_iter, int precond, double tol, int count) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < count; b += gridDim.x * blockDim.x) {
+    st[b].k = 0;
+    st[b].done = 0;
+    st[b].converged = 0;
+    st[b].breakdown = 0;
+    st[b].max_iter = max_iter;
+    st[b].precond = precond;
+    st[b].allzero = 0;
+    st[b].tol = tol;
+  }
+}
+
+// dL/dM of B problems (T, G, grad: [B, n, m]; lam: [B, n + m - 1]).
+__global__ void assemble_grad_batch_kernel(const double* __restrict__ T,
+                                           const double* __restrict__ G,
+                                           const double* __restrict__ lam, int B, int n, int m,
+                                           double inv_eta, double* __restrict__ grad) {
+  const size_t nm = (size_t)n * m, total = nm * B;
+  const int H = n + m - 1;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const size_t b = q / nm, e = q - b * nm;
+    const int i = (int)(e / m);
+    const int j = (int)(e - (size_t)i * m);
+    const double* lb_ = lam + b * H;
+    const double lb = (j < m - 1) ? lb_[n + j] : 0.0;
+    grad[q] = (T[q] * (lb_[i] + lb - G[q])) * inv_eta;
+  }
 }
 
 }  // namespace
@@ -443,7 +479,7 @@ int backward_solve(const double* T, const double* G, cg_ctx_s* ctx, double eta, 
   A.scal = ws.at<double>(o_sc);
   A.counters = ws.at<unsigned int>(o_cnt);
   CG_TRY_CUDA(cudaMemsetAsync(A.counters, 0, (splits + strips + 1) * sizeof(unsigned int), st));
-  { pcg_state_init<<<1, 1, 0, st>>>(A.st, max_iter, precond, tol); cg::count_launch(); }
+  { pcg_state_init<<<1, 32, 0, st>>>(A.st, max_iter, precond, tol, 1); cg::count_launch(); }
   const int grid = strips * splits;
   const bool splr = (precond == CG_PRECOND_SPLR);
   if (splr) {
@@ -494,7 +530,142 @@ int backward_solve(const double* T, const double* G, cg_ctx_s* ctx, double eta, 
   return CG_OK;
 }
 
+// B problems of one shape with the diagonal preconditioner (or none): every
+// PCG iteration of all unfinished problems is one launch, and the host reads
+// the B states once per chunk of iterations.  Per problem, the values are
+// those of backward_solve.
+int backward_solve_batch(const double* T, const double* G, cg_ctx_s* const* ctxs, double eta,
+                         int precond, double tol, int max_iter, int B, int n, int m,
+                         double* lambda, double* grad, int* iterations, int* converged,
+                         cudaStream_t st) {
+  if (!T || !G || !lambda || B <= 0 || n <= 0 || m <= 0 || !(eta > 0.0) || max_iter <= 0 ||
+      (precond != CG_PRECOND_NONE && precond != CG_PRECOND_DIAG)) {
+    set_last_error("cg_backward_batch: invalid argument (precond must be NONE or DIAG)", __FILE__,
+                   __LINE__);
+    return CG_ERR_INVALID_ARG;
+  }
+  const int H = n + m - 1;
+  if (precond == CG_PRECOND_DIAG) {
+    if (!ctxs) {
+      set_last_error("cg_backward_batch: DIAG needs one backward context per problem", __FILE__,
+                     __LINE__);
+      return CG_ERR_INVALID_CONTEXT;
+    }
+    for (int b = 0; b < B; ++b) {
+      cg_ctx_s* c = ctxs[b];
+      if (!c || !c->valid) {
+        set_last_error("cg_backward_batch: invalid backward context", __FILE__, __LINE__);
+        return CG_ERR_INVALID_CONTEXT;
+      }
+      if (c->H != H) {
+        set_last_error("cg_backward_batch: context dimension mismatch", __FILE__, __LINE__);
+        return CG_ERR_INVALID_ARG;
+      }
+      CG_TRY(ctx_setup_diag(c, st));
+    }
+  }
+  const int sms = sm_count_current();
+  int strips = 1, splits = 1;
+  tpass_geometry(n, m, sms, strips, splits);
+  const int per = strips * splits;
+  const size_t nc = (size_t)splits + strips + 1;
+  Workspace ws(st);
+  const size_t o_rows = ws.reserve<double>((size_t)B * n), o_cols = ws.reserve<double>((size_t)B * m);
+  const size_t o_r = ws.reserve<double>((size_t)B * H), o_z = ws.reserve<double>((size_t)B * H);
+  const size_t o_p = ws.reserve<double>((size_t)B * H), o_w = ws.reserve<double>((size_t)B * H);
+  const size_t o_rp = ws.reserve<double>((size_t)B * 2 * strips * n);
+  const size_t o_cp = ws.reserve<double>((size_t)B * 2 * splits * m);
+  const size_t o_sc = ws.reserve<double>((size_t)B * 2 * (splits + strips));
+  const size_t o_cnt = ws.reserve<unsigned int>((size_t)B * nc);
+  const size_t o_st = ws.reserve<PcgState>(B);
+  const size_t o_args = ws.reserve<AdjArgs>(B);
+  CG_TRY(ws.allocate());
+  std::vector<AdjArgs> hA(B);
+  PcgState* dst = ws.at<PcgState>(o_st);
+  for (int b = 0; b < B; ++b) {
+    AdjArgs& A = hA[b];
+    A = AdjArgs{};
+    A.T = T + (size_t)b * n * m;
+    A.G = G + (size_t)b * n * m;
+    A.n = n;
+    A.m = m;
+    A.rows = ws.at<double>(o_rows) + (size_t)b * n;
+    A.cols = ws.at<double>(o_cols) + (size_t)b * m;
+    A.x = lambda + (size_t)b * H;
+    A.r = ws.at<double>(o_r) + (size_t)b * H;
+    A.z = ws.at<double>(o_z) + (size_t)b * H;
+    A.p = ws.at<double>(o_p) + (size_t)b * H;
+    A.w = ws.at<double>(o_w) + (size_t)b * H;
+    A.inv_diag = (precond == CG_PRECOND_DIAG) ? ctxs[b]->inv_diag : nullptr;
+    A.st = dst + b;
+    A.strips = strips;
+    A.splits = splits;
+    A.rowpart = ws.at<double>(o_rp) + (size_t)b * 2 * strips * n;
+    A.colpart = ws.at<double>(o_cp) + (size_t)b * 2 * splits * m;
+    A.scal = ws.at<double>(o_sc) + (size_t)b * 2 * (splits + strips);
+    A.counters = ws.at<unsigned int>(o_cnt) + (size_t)b * nc;
+  }
+  AdjArgs* dA = ws.at<AdjArgs>(o_args);
+  CG_TRY_CUDA(cudaMemcpyAsync(dA, hA.data(), B * sizeof(AdjArgs), cudaMemcpyHostToDevice, st));
+  CG_TRY_CUDA(cudaMemsetAsync(ws.at<unsigned int>(o_cnt), 0, B * nc * sizeof(unsigned int), st));
+  { pcg_state_init<<<std::max(1, (B + 127) / 128), 128, 0, st>>>(dst, max_iter, precond, tol, B); cg::count_launch(); }
+  { adj_pass_batch_kernel<0><<<B * per, kThreads, 0, st>>>(dA, per, 0); cg::count_launch(); }
+  CG_TRY_CUDA(cudaGetLastError());
+  std::vector<PcgState> hs(B);
+  auto all_done = [&]() {
+    for (const PcgState& x : hs)
+      if (!x.done) return false;
+    return true;
+  };
+  // B states are read through a pinned bounce buffer in pieces of 4 KB
+  auto read_states = [&]() -> int {
+    const int per_read = (int)(4096 / sizeof(PcgState));
+    for (int b0 = 0; b0 < B; b0 += per_read) {
+      const int cnt = std::min(per_read, B - b0);
+      CG_TRY(read_device(hs.data() + b0, dst + b0, cnt * sizeof(PcgState), st));
+    }
+    return CG_OK;
+  };
+  CG_TRY(read_states());
+  int chunk = 4;
+  while (!all_done()) {
+    for (int c = 0; c < chunk; ++c)
+      { adj_pass_batch_kernel<1><<<B * per, kThreads, 0, st>>>(dA, per, 1); cg::count_launch(); }
+    CG_TRY_CUDA(cudaGetLastError());
+    CG_TRY(read_states());
+    chunk = std::min(chunk * 2, 64);
+  }
+  int broke = -1;
+  for (int b = 0; b < B; ++b) {
+    if (iterations) iterations[b] = hs[b].allzero ? 0 : (hs[b].converged ? hs[b].k : max_iter);
+    if (converged) converged[b] = hs[b].converged;
+    if (hs[b].breakdown && broke < 0) broke = b;
+  }
+  if (grad) {
+    const size_t total = (size_t)B * n * m;
+    const int blocks = (int)std::max<size_t>(1, std::min<size_t>((total + 255) / 256, sms * 16));
+    { assemble_grad_batch_kernel<<<blocks, 256, 0, st>>>(T, G, lambda, B, n, m, 1.0 / eta, grad); cg::count_launch(); }
+    CG_TRY_CUDA(cudaGetLastError());
+  }
+  ws.release();
+  if (broke >= 0) {
+    set_last_error("PCG breakdown: p^T A p <= 0 (matrix not SPD?) in a problem of the batch",
+                   __FILE__, __LINE__);
+    return CG_ERR_NOT_SPD;
+  }
+  return CG_OK;
+}
+
 }  // namespace cg
+
+extern "C" int cg_backward_batch_f64(const double* T, const double* G, cg_ctx* const* ctxs,
+                                     double eta, int precond, double tol, int max_iter, int B,
+                                     int n, int m, double* lambda, double* grad, int* iterations,
+                                     int* converged, cudaStream_t stream) {
+  return cg::backward_solve_batch(T, G, reinterpret_cast<cg_ctx_s* const*>(ctxs), eta, precond,
+                                  tol, max_iter, B, n, m, lambda, grad, iterations, converged,
+                                  stream);
+}
 
 extern "C" int cg_backward_f64(const double* T, const double* G, cg_ctx* ctx, double eta,
                                int precond, double tol, int max_iter, int n, int m,

@@ -39,6 +39,7 @@
 // and the same K order, so row and column passes see identical M_ij.
 #include <algorithm>
 #include <atomic>
+#include <cstring>
 #include <cmath>
 #include <cstdint>
 
@@ -304,6 +305,131 @@ __global__ void __launch_bounds__(kPtsThreads) pts_cost_kernel(
   pts_teardown(sh);
 }
 
+// Statistics of the unscaled cost c_ij = max(0, |x_i|^2 + |y_j|^2 - 2 x_i . y_j)
+// (the FP32 values the cost tiles hold at scale 1), for the /max and /median
+// normalisers: one pass per radix level over the recomputed tiles.  The keys
+// are the FP32 bit patterns (c >= 0, sign cleared), which order like the
+// values.  Level 0 also takes the maximum; level L histograms the digit
+// (12, 12, 8 bits from the top) of the keys whose higher digits equal the
+// prefix found so far (sel[0]).
+constexpr int kStatBins = 4096;
+struct StatSel {
+  unsigned long long krem;  // rank (1-based) still to find inside the prefix
+  unsigned int prefix;      // digits found so far
+  unsigned int maxbits;     // maximum key (level 0)
+};
+__device__ __forceinline__ int stat_shift(int level) { return level == 0 ? 20 : (level == 1 ? 8 : 0); }
+__device__ __forceinline__ int stat_width(int level) { return level == 2 ? 8 : 12; }
+
+__global__ void __launch_bounds__(kPtsThreads) pts_stats_kernel(
+    const uint16_t* __restrict__ P, const uint16_t* __restrict__ Q, const float* __restrict__ nP,
+    const float* __restrict__ nQ, int rows, int cols, int D, int level,
+    const StatSel* __restrict__ sel, unsigned long long* __restrict__ hist,
+    unsigned int* __restrict__ maxbits, int* __restrict__ error, long first_wait) {
+  extern __shared__ __align__(1024) char smem[];
+  __shared__ PtsShared sh;
+  __shared__ unsigned int shist[kStatBins];
+  __shared__ unsigned int smax;
+  char* tA = smem;
+  char* tB = smem + kTileBytesMax;
+  for (int b = threadIdx.x; b < kStatBins; b += blockDim.x) shist[b] = 0u;
+  if (threadIdx.x == 0) smax = 0u;
+  pts_setup(sh);  // ends with a block barrier
+  const int r0 = blockIdx.x * kPtsTile, c0 = blockIdx.y * kPtsTile;
+  stage_tile(P, rows, D, r0, tA);
+  stage_tile(Q, cols, D, c0, tB);
+  uint32_t phase = 0;
+  const bool ok = pts_tile_mma(sh, tA, tB, D, phase, first_wait);
+  const int sh_lo = stat_shift(level), width = stat_width(level);
+  const unsigned int prefix = (level == 0) ? 0u : sel->prefix;
+  const int sh_hi = sh_lo + width;
+  if (!ok) {
+    if (threadIdx.x == 0) atomicExch(error, 1);
+  } else {
+    const int warp = threadIdx.x >> 5;
+    const int r = r0 + threadIdx.x;
+    const float nr = r < rows ? nP[r] : 0.0f;
+    const int lane = threadIdx.x & 31;
+    unsigned int mymax = 0u;
+#pragma unroll 1
+    for (int cb = 0; cb < kPtsTile; cb += 32) {
+      float v[32];
+      tmem_ld32(sh.tmem + (static_cast<uint32_t>(warp * 32) << 16) + cb, v);
+#pragma unroll 4
+      for (int q = 0; q < 32; ++q) {
+        const int c = c0 + cb + q;
+        int bin = -1;
+        if (r < rows && c < cols) {
+          const unsigned int key = __float_as_uint(pts_cost(v[q], nr, nQ[c], 1.0f)) & 0x7FFFFFFFu;
+          if (level == 0) mymax = max(mymax, key);
+          if (level == 0 || (key >> sh_hi) == prefix)
+            bin = (int)((key >> sh_lo) & ((1u << width) - 1u));
+        }
+        // warp-aggregated increment: one shared atomic per distinct bin
+        const unsigned int act = __ballot_sync(0xffffffffu, bin >= 0);
+        if (bin >= 0) {
+          const unsigned int peers = __match_any_sync(act, bin);
+          if ((__ffs(peers) - 1) == lane) atomicAdd(&shist[bin], (unsigned)__popc(peers));
+        }
+      }
+    }
+    if (level == 0) atomicMax(&smax, mymax);
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < kStatBins; b += blockDim.x)
+    if (shist[b]) atomicAdd(&hist[b], (unsigned long long)shist[b]);
+  if (level == 0 && threadIdx.x == 0) atomicMax(maxbits, smax);
+  pts_teardown(sh);
+}
+
+// One CTA of 1024 threads: the bin (ascending) holding the krem-th smallest
+// key of this level; extends the prefix and clears the histogram.
+__global__ void __launch_bounds__(1024) pts_stats_select_kernel(StatSel* sel,
+                                                                 unsigned long long* hist,
+                                                                 int level) {
+  __shared__ unsigned long long part[1024];
+  __shared__ int sh_b;
+  __shared__ unsigned long long sh_below;
+  const int t = threadIdx.x;
+  const int nb = 1 << stat_width(level);
+  unsigned long long c[4], mine = 0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int b = 4 * t + q;
+    c[q] = (b < nb) ? hist[b] : 0ull;
+    mine += c[q];
+  }
+  part[t] = mine;
+  if (t == 0) sh_b = -1;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {  // inclusive prefix scan
+    const unsigned long long v = (t >= off) ? part[t - off] : 0ull;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  const unsigned long long krem = sel->krem;
+  const unsigned long long before = (t > 0) ? part[t - 1] : 0ull;
+  if (before < krem && part[t] >= krem) {
+    unsigned long long below = before;
+    for (int q = 0; q < 4; ++q) {
+      if (below + c[q] >= krem) {
+        sh_b = 4 * t + q;
+        sh_below = below;
+        break;
+      }
+      below += c[q];
+    }
+  }
+  __syncthreads();
+  if (t == 0 && sh_b >= 0) {
+    sel->krem = krem - sh_below;
+    sel->prefix = (level == 0 ? 0u : (sel->prefix << stat_width(level))) | (unsigned int)sh_b;
+  }
+  __syncthreads();
+  for (int b = t; b < kStatBins; b += blockDim.x) hist[b] = 0ull;
+}
+
 // Partial LSE over the column tiles [t0, t1) for the 128 rows of tile
 // blockIdx.x: part[(split * rows_pad + r) * 2 + {0, 1}] = (max, sum) in base 2
 // of xs_j - s2 M_rj, xs the other side's scaled duals.  The state's
@@ -544,6 +670,8 @@ int pts_attrs() {
                                    kPtsSmemLaunch));
   CG_TRY_CUDA(cudaFuncSetAttribute(pts_lse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    kPtsSmemLaunch));
+  CG_TRY_CUDA(cudaFuncSetAttribute(pts_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   kPtsSmemLaunch));
   done_dev = dev;
   return CG_OK;
 }
@@ -711,4 +839,79 @@ extern "C" int cg_bcd_points_bf16(const uint16_t* X, const uint16_t* Y, int n, i
 extern "C" int cg_points_set_wait_limit(long long polls) {
   cg::g_pts_first_wait.store(polls < 0 ? cg::kPtsSpinLimit : (long)polls);
   return CG_OK;
+}
+
+extern "C" int cg_points_cost_stats_bf16(const uint16_t* X, const uint16_t* Y, int n, int m,
+                                         int d, double* max_out, double* median_out,
+                                         cudaStream_t stream) {
+  CG_TRY(check_points_args(n, m, d, 1.0));
+  if (!X || !Y || !max_out || !median_out) {
+    set_last_error("points: null pointer", __FILE__, __LINE__);
+    return CG_ERR_INVALID_ARG;
+  }
+  CG_TRY(pts_attrs());
+  const int D = pad_dim(d);
+  Workspace W(stream);
+  const size_t oXp = W.reserve<uint16_t>((size_t)n * D), oYp = W.reserve<uint16_t>((size_t)m * D);
+  const size_t onX = W.reserve<float>(n), onY = W.reserve<float>(m);
+  const size_t ohist = W.reserve<unsigned long long>(kStatBins);
+  const size_t osel = W.reserve<StatSel>(1);
+  const size_t omax = W.reserve<unsigned int>(1);
+  const size_t oerr = W.reserve<int>(1);
+  CG_TRY(W.allocate());
+  uint16_t* Xp = W.at<uint16_t>(oXp);
+  uint16_t* Yp = W.at<uint16_t>(oYp);
+  float* nX = W.at<float>(onX);
+  float* nY = W.at<float>(onY);
+  unsigned long long* hist = W.at<unsigned long long>(ohist);
+  StatSel* sel = W.at<StatSel>(osel);
+  unsigned int* maxbits = W.at<unsigned int>(omax);
+  int* err = W.at<int>(oerr);
+  const long first_wait = g_pts_first_wait.load();
+  int rc = CG_OK;
+  do {
+    // lower median: the ceil(N / 2)-th smallest of the N = n m values
+    StatSel hs{};
+    hs.krem = ((unsigned long long)n * (unsigned long long)m + 1ull) / 2ull;
+    if ((rc = status_from_cuda(cudaMemcpyAsync(sel, &hs, sizeof(StatSel), cudaMemcpyHostToDevice,
+                                               stream))) != CG_OK)
+      break;
+    if ((rc = status_from_cuda(cudaMemsetAsync(hist, 0, kStatBins * sizeof(unsigned long long),
+                                               stream))) != CG_OK)
+      break;
+    if ((rc = status_from_cuda(cudaMemsetAsync(maxbits, 0, sizeof(unsigned int), stream))) != CG_OK)
+      break;
+    if ((rc = status_from_cuda(cudaMemsetAsync(err, 0, sizeof(int), stream))) != CG_OK) break;
+    { pts_pad_kernel<<<(n + 255) / 256, 256, 0, stream>>>(X, n, d, D, Xp, nX); count_launch(); }
+    { pts_pad_kernel<<<(m + 255) / 256, 256, 0, stream>>>(Y, m, d, D, Yp, nY); count_launch(); }
+    dim3 grid((n + kPtsTile - 1) / kPtsTile, (m + kPtsTile - 1) / kPtsTile);
+    for (int level = 0; level < 3; ++level) {
+      { pts_stats_kernel<<<grid, kPtsThreads, kPtsSmemLaunch, stream>>>(
+          Xp, Yp, nX, nY, n, m, D, level, sel, hist, maxbits, err, first_wait); count_launch(); }
+      { pts_stats_select_kernel<<<1, 1024, 0, stream>>>(sel, hist, level); count_launch(); }
+    }
+    if ((rc = status_from_cuda(cudaGetLastError())) != CG_OK) break;
+    struct {
+      StatSel s;
+      unsigned int mx;
+      int err;
+    } out{};
+    const ReadSpan spans[3] = {{&out.s, sel, sizeof(StatSel)},
+                               {&out.mx, maxbits, sizeof(unsigned int)},
+                               {&out.err, err, sizeof(int)}};
+    if ((rc = read_device_spans(spans, 3, stream)) != CG_OK) break;
+    if (out.err) {
+      set_last_error("points: tensor-core completion wait timed out", __FILE__, __LINE__);
+      rc = CG_ERR_TIMEOUT;
+      break;
+    }
+    float fmx, fmed;
+    const unsigned int mb = out.mx, kb = out.s.prefix;
+    std::memcpy(&fmx, &mb, sizeof(float));
+    std::memcpy(&fmed, &kb, sizeof(float));
+    *max_out = fmx;
+    *median_out = fmed;
+  } while (false);
+  W.release();
+  return rc;
 }

@@ -79,3 +79,17 @@ def sinkhorn_bcd_points(X, Y, a, b, reg, tol=1e-8, max_iter=100000, scale=None,
                      b.data_ptr(), float(reg), int(max_iter), float(tol), mode,
                      ctypes.byref(niter), dual.data_ptr(), ctypes.byref(fast), _stream(dev))
     return {"niter": niter.value, "dual": dual, "fast_iters": fast.value}
+
+
+def cost_normalisers(X, Y):
+    """(max, lower median) of the unscaled cost c_ij = max(0, |x_i|^2 + |y_j|^2
+    - 2 x_i . y_j) as the tensor-core tiles compute it, without storing it.
+    ``sinkhorn_bcd_points(..., scale=1 / max)`` is the "M / max" cost;
+    ``scale=1 / median`` the "M / median" one."""
+    X, Y, n, m, d = _check_points(X, Y)
+    mx = ctypes.c_double(0.0)
+    md = ctypes.c_double(0.0)
+    with torch.cuda.device(X.device):
+        _native.call("cg_points_cost_stats_bf16", X.data_ptr(), Y.data_ptr(), n, m, d,
+                     ctypes.byref(mx), ctypes.byref(md), _stream(X.device))
+    return mx.value, md.value

@@ -249,6 +249,20 @@ int cg_backward_f64(const double* T, const double* G, cg_ctx* ctx, double eta, i
                     double tol, int max_iter, int n, int m, double* lambda, double* grad,
                     int* iterations, int* converged, cudaStream_t stream);
 
+/*
+ * The same backward for B problems of one shape in one call: T, G, grad are
+ * [B, n, m] (contiguous), lambda [B, n + m - 1], iterations / converged host
+ * [B]; ctxs: B contexts (CG_PRECOND_DIAG) or NULL (CG_PRECOND_NONE; the SPLR
+ * preconditioner is not batched).  One launch per PCG iteration covers every
+ * unfinished problem and the host reads the B states once per chunk of
+ * iterations; each problem's values are those of cg_backward_f64.  Replaces
+ * the per-problem backward of splr_ot_batch (curegot/autograd.py:340-367).
+ */
+int cg_backward_batch_f64(const double* T, const double* G, cg_ctx* const* ctxs, double eta,
+                          int precond, double tol, int max_iter, int B, int n, int m,
+                          double* lambda, double* grad, int* iterations, int* converged,
+                          cudaStream_t stream);
+
 /* ------------------------------------------------------------------------ */
 /* Continuous-batching serving engine (no reference counterpart: the         */
 /* reference solves one problem per blocking call and batches only with a    */
@@ -370,7 +384,19 @@ int cg_bcd_points_bf16(const uint16_t* X, const uint16_t* Y, int n, int m, int d
                        double cost_scale, const double* a, const double* b, double reg,
                        int max_iter, double tol, int precision, int* niter, double* dual,
                        int* fast_iters, cudaStream_t stream);
-/* Poll limit of the first wait for each tile's tensor-core MMAs in the two
+/*
+ * Normalisers of the cost on the tensor-core tiles, without storing it:
+ * *max_out = the largest and *median_out = the lower median (the
+ * ceil(nm/2)-th smallest) of c_ij = max(0, |x_i|^2 + |y_j|^2 - 2 x_i . y_j),
+ * the FP32 values cg_points_cost_bf16 writes at cost_scale 1.  Three passes
+ * recompute the tiles and histogram the FP32 bit patterns digit by digit
+ * (12, 12, 8 bits); the maximum comes with the first.  The configurations'
+ * "M / max" and "M / median" are cost_scale = 1 / max or 1 / median.
+ * Outputs are host doubles (exactly the FP32 values).
+ */
+int cg_points_cost_stats_bf16(const uint16_t* X, const uint16_t* Y, int n, int m, int d,
+                              double* max_out, double* median_out, cudaStream_t stream);
+/* Poll limit of the first wait for each tile's tensor-core MMAs in the
  * functions above (process-wide; polls < 0 restores the default of 2^24).
  * When a wait gives up, the kernel waits once more at the full limit for the
  * MMAs to drain, frees its tensor memory and flags the error: the call

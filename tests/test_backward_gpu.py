@@ -144,3 +144,28 @@ def test_batch_concurrent_matches_sequential(B):
     with torch.no_grad():
         Tn = cg.torch.splr_ot_batch(M, a, b, eta=0.05, tol=1e-8)
     assert Tn.grad_fn is None and torch.equal(Tn, Ts.detach())
+
+
+@pytest.mark.parametrize("precond", ["diag", "none"])
+def test_batched_adjoint_matches_per_problem(precond):
+    """cg_backward_batch_f64 (one launch per PCG iteration over all problems)
+    gives each problem exactly the lambda, gradient and iteration count of
+    cg_backward_f64."""
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device=dev).manual_seed(7)
+    B, n, m, eta = 5, 90, 70, 0.05
+    X = torch.rand(B, n, 8, generator=g, device=dev, dtype=torch.float64)
+    Y = torch.rand(B, m, 8, generator=g, device=dev, dtype=torch.float64)
+    M = ((X[:, :, None, :] - Y[:, None, :, :]) ** 2).mean(-1)
+    a = torch.full((n,), 1.0 / n, dtype=torch.float64, device=dev)
+    b = torch.full((m,), 1.0 / m, dtype=torch.float64, device=dev)
+    outs = [cg.torch.sinkhorn_splr_bwd(M[i], a, b, eta, 1e-9, 500, 0) for i in range(B)]
+    T = torch.stack([o["plan"] for o in outs])
+    G = torch.randn(B, n, m, generator=g, device=dev, dtype=torch.float64)
+    ctxs = [o["context"] for o in outs]
+    res = cg.backward.solve_backward_batch(T, G, ctxs, eta, preconditioner=precond)
+    for i in range(B):
+        one = cg.torch.solve_backward(T[i], G[i], ctxs[i], eta, preconditioner=precond)
+        assert torch.equal(res["lambda"][i], one["lambda"])
+        assert torch.equal(res["grad"][i], one["grad"])
+        assert res["iterations"][i] == one["iterations"] and res["converged"][i]

@@ -97,3 +97,19 @@ def test_invalid_arguments():
     Z = torch.zeros(4, 65, dtype=torch.bfloat16, device="cuda")
     with pytest.raises(ValueError):
         cost_from_points(Z, Z)
+
+
+@pytest.mark.parametrize("n,m,d", [(300, 260, 32), (1000, 777, 8), (129, 4000, 16)])
+def test_cost_normalisers_on_the_tiles(cuda_dev, n, m, d):
+    """max and lower median of the unscaled cost, computed on the tensor-core
+    tiles by radix histograms, equal torch's max / kthvalue of the same FP32
+    values written out by cost_from_points (scale 1)."""
+    from curegot_backward_b200 import points
+    g = torch.Generator(device=cuda_dev).manual_seed(n * 7 + m)
+    X = torch.randn(n, d, generator=g, device=cuda_dev).to(torch.bfloat16)
+    Y = torch.randn(m, d, generator=g, device=cuda_dev).to(torch.bfloat16)
+    mx, med = points.cost_normalisers(X, Y)
+    C = points.cost_from_points(X, Y, scale=1.0).flatten()
+    assert mx == float(C.max())
+    k = (C.numel() + 1) // 2
+    assert med == float(torch.kthvalue(C.cpu(), k).values)
