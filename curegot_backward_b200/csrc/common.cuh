@@ -70,6 +70,9 @@ struct ReadSpan {
   size_t bytes;
 };
 int read_device_spans(const ReadSpan* spans, int count, cudaStream_t st);
+// Any size: through a thread-local pinned buffer that grows as needed (kept
+// for the thread's lifetime), then host_wait on the stream.
+int read_device_bulk(void* host, const void* dev, size_t bytes, cudaStream_t st);
 int read_device(void* host1, const void* dev1, size_t bytes1, cudaStream_t st,
                 void* host2 = nullptr, const void* dev2 = nullptr, size_t bytes2 = 0);
 

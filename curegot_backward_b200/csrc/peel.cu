@@ -511,13 +511,13 @@ int peel_plan(PeelFactor& P, const SpHess& A, cudaStream_t st, bool no_peel) {
   P.n = n;
   P.m = m;
   P.H = H;
+  // pattern to the host through pinned memory (pageable copies serialise
+  // with the other streams' work)
   std::vector<int> rp(H + 1);
-  CG_TRY_CUDA(cudaMemcpyAsync(rp.data(), A.rowptr, (H + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
-  CG_TRY_CUDA(cudaStreamSynchronize(st));
+  CG_TRY(read_device_bulk(rp.data(), A.rowptr, (H + 1) * sizeof(int), st));
   const int nl = rp[H];
   std::vector<int> cl(std::max(nl, 1));
-  CG_TRY_CUDA(cudaMemcpyAsync(cl.data(), A.col, (size_t)nl * sizeof(int), cudaMemcpyDeviceToHost, st));
-  CG_TRY_CUDA(cudaStreamSynchronize(st));
+  CG_TRY(read_device_bulk(cl.data(), A.col, (size_t)nl * sizeof(int), st));
 
   // diagonal positions and the bipartite adjacency (neighbour, value index)
   std::vector<int> diagq(H);

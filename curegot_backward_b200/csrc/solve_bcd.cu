@@ -140,6 +140,30 @@ int read_device_spans(const ReadSpan* spans, int count, cudaStream_t st) {
   return CG_OK;
 }
 
+int read_device_bulk(void* host, const void* dev, size_t bytes, cudaStream_t st) {
+  struct Pinned {
+    void* p = nullptr;
+    size_t cap = 0;
+    ~Pinned() {
+      if (p) cudaFreeHost(p);
+    }
+  };
+  thread_local Pinned buf;
+  if (bytes == 0) return CG_OK;
+  if (bytes > buf.cap) {
+    if (buf.p) cudaFreeHost(buf.p);
+    buf.p = nullptr;
+    buf.cap = 0;
+    const size_t cap = std::max(bytes, (size_t)1 << 20);
+    CG_TRY_CUDA(cudaHostAlloc(&buf.p, cap, cudaHostAllocDefault));
+    buf.cap = cap;
+  }
+  CG_TRY_CUDA(cudaMemcpyAsync(buf.p, dev, bytes, cudaMemcpyDeviceToHost, st));
+  CG_TRY(host_wait(st));
+  std::memcpy(host, buf.p, bytes);
+  return CG_OK;
+}
+
 int read_device(void* host1, const void* dev1, size_t bytes1, cudaStream_t st, void* host2,
                 const void* dev2, size_t bytes2) {
   const ReadSpan spans[2] = {{host1, dev1, bytes1}, {host2, dev2, bytes2}};

@@ -165,12 +165,10 @@ int spchol_order(SparseChol& C, const SpHess& A, double flop_budget, cudaStream_
   C.analyzed = false;
   // lower pattern -> host
   std::vector<int> rp(H + 1);
-  CG_TRY_CUDA(cudaMemcpyAsync(rp.data(), A.rowptr, (H + 1) * sizeof(int), cudaMemcpyDeviceToHost, st));
-  CG_TRY_CUDA(cudaStreamSynchronize(st));
+  CG_TRY(read_device_bulk(rp.data(), A.rowptr, (H + 1) * sizeof(int), st));
   const int nl = rp[H];
   std::vector<int> cl(std::max(nl, 1));
-  CG_TRY_CUDA(cudaMemcpyAsync(cl.data(), A.col, (size_t)nl * sizeof(int), cudaMemcpyDeviceToHost, st));
-  CG_TRY_CUDA(cudaStreamSynchronize(st));
+  CG_TRY(read_device_bulk(cl.data(), A.col, (size_t)nl * sizeof(int), st));
   // full symmetric pattern + value map; rows are filled in increasing row
   // order of the lower view, so every row of the full pattern comes out with
   // ascending columns (upper part first from earlier rows, then the lower)
