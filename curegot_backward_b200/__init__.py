@@ -73,9 +73,10 @@ def set_bcd_cluster_path(enabled: bool = True) -> None:
 
 
 def set_bcd_staging(enabled: bool = True) -> None:
-    """Enable (default) or disable the shared-memory staging of the Sinkhorn
+    """Enable or disable (default) the shared-memory staging of the Sinkhorn
     passes: long rows and column strips stream through per-warp rings filled
-    by bulk asynchronous copies.  Results are bitwise the same either way."""
+    by bulk asynchronous copies.  Results are bitwise the same either way; on
+    B200 the register path measured faster, so staging is off by default."""
     _native.call("cg_bcd_set_staging", 1 if enabled else 0)
 
 

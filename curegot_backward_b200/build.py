@@ -33,7 +33,9 @@ def _nvcc() -> str:
 
 
 def _flags(extra=()):
-    return [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+    # C++20: the SPLR solve is a coroutine (csrc/task.cuh)
+    return [*ARCH, "-O3", "-lineinfo", "-std=c++20", "-Xcompiler", "-fPIC",
+            "-Xcompiler", "-Wno-subobject-linkage",
             "-I", INCLUDE, "-I", CSRC, *extra]
 
 

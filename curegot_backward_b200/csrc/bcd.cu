@@ -52,11 +52,15 @@ struct RowU {
 
 // One warp's segment [c0, c1) of row `row`: LSE over j of (betas_j - s2*M_ij).
 // Full chunks run predicate-free with the next chunk's M vectors prefetched.
-template <typename TM, bool FAST>
+// CHECK (first pass of a solve): a NaN exponent (NaN in M or the duals) makes
+// the row's sum NaN.  Without it a NaN entry would drop out of the sum like
+// an infinite cost: the exponent clamp of the exponential ignores NaN.
+template <typename TM, bool FAST, bool CHECK>
 __device__ __forceinline__ void row_segment(const TM* __restrict__ Mrow,
                                             const double* __restrict__ betas, double s2, int c0,
                                             int c1, int lane, bool vec_ok, const double* tab,
                                             double& mx, double& s) {
+  bool bad = false;
   constexpr int VN = Vec<TM>::N;
   if (vec_ok) {
     constexpr int U = RowU<TM>::U;
@@ -85,6 +89,9 @@ __device__ __forceinline__ void row_segment(const TM* __restrict__ Mrow,
 #pragma unroll
         for (int k = 0; k < VN; ++k) d[u * VN + k] = fma(-Raw<TM>::get(cur[u], k), s2, bv[k]);
       }
+      if (CHECK)
+#pragma unroll
+        for (int q = 0; q < U * VN; ++q) bad |= (d[q] != d[q]);
       lse_chunk_full<FAST, U * VN>(d, mx, s, tab);
     }
     // tail (vectors that are in range, then nothing: c1 is a multiple of VN)
@@ -99,6 +106,9 @@ __device__ __forceinline__ void row_segment(const TM* __restrict__ Mrow,
         ok[k] = true;
         d[k] = fma(-mv[k], s2, bv[k]);
       }
+      if (CHECK)
+#pragma unroll
+        for (int q = 0; q < VN; ++q) bad |= (d[q] != d[q]);
       lse_chunk<FAST, VN>(d, ok, mx, s, tab);
     }
   } else {
@@ -111,9 +121,13 @@ __device__ __forceinline__ void row_segment(const TM* __restrict__ Mrow,
         ok[u] = j < c1;
         d[u] = ok[u] ? fma(-ld1(Mrow + j), s2, betas[j]) : kNegInf;
       }
+      if (CHECK)
+#pragma unroll
+        for (int q = 0; q < kUnroll; ++q) bad |= (ok[q] && d[q] != d[q]);
       lse_chunk<FAST, kUnroll>(d, ok, mx, s, tab);
     }
   }
+  if (CHECK && bad) s = __longlong_as_double(0x7ff8000000000000LL);
 }
 
 // row_segment for rows whose 16-byte vectors are aligned (vec_ok) and long
@@ -123,11 +137,12 @@ __device__ __forceinline__ void row_segment(const TM* __restrict__ Mrow,
 // span is processed exactly like row_segment's loop body -- same grouping,
 // same order, bitwise the same (mx, s).  The tail (< one span) is read as in
 // row_segment.  A ring wait that gives up leaves ring.failed set.
-template <typename TM, bool FAST>
+template <typename TM, bool FAST, bool CHECK>
 __device__ __forceinline__ void row_segment_staged(const TM* __restrict__ Mrow,
                                                    const double* __restrict__ betas, double s2,
                                                    int c0, int c1, int lane, const double* tab,
                                                    WarpRing& ring, double& mx, double& s) {
+  bool bad = false;
   constexpr int VN = Vec<TM>::N;
   constexpr int U = RowU<TM>::U;
   constexpr int step = 32 * VN;
@@ -168,6 +183,9 @@ __device__ __forceinline__ void row_segment_staged(const TM* __restrict__ Mrow,
 #pragma unroll
         for (int kk = 0; kk < VN; ++kk) d[u * VN + kk] = fma(-Raw<TM>::get(v, kk), s2, bv[kk]);
       }
+      if (CHECK)
+#pragma unroll
+        for (int q = 0; q < U * VN; ++q) bad |= (d[q] != d[q]);
       lse_chunk_full<FAST, U * VN>(d, mx, s, tab);
     }
     ring.consumed++;
@@ -191,8 +209,12 @@ __device__ __forceinline__ void row_segment_staged(const TM* __restrict__ Mrow,
       ok[k] = true;
       d[k] = fma(-mv[k], s2, bv[k]);
     }
+    if (CHECK)
+#pragma unroll
+      for (int q = 0; q < VN; ++q) bad |= (d[q] != d[q]);
     lse_chunk<FAST, VN>(d, ok, mx, s, tab);
   }
+  if (CHECK && bad) s = __longlong_as_double(0x7ff8000000000000LL);
 }
 
 // CTA-wide Chan combine; thread 0 ends with the total.  sh: 3 * kThreads.
@@ -288,15 +310,23 @@ __device__ __forceinline__ void row_block(const BcdProb* __restrict__ probs,
     const TM* __restrict__ Mrow = M + (size_t)row * m;
     // stream through the ring when the segment holds at least two chunks
     const bool use_ring = staged && vec_ok && (c1 - c0) * (int)sizeof(TM) >= 2 * kRingBytes;
+    const bool first = (t == 0);  // the first pass also flags NaN exponents
     if (use_ring) {
-      if (fast)
-        row_segment_staged<TM, true>(Mrow, betas, s2, c0, c1, lane, tab, ring, mx, s);
+      if (first && fast)
+        row_segment_staged<TM, true, true>(Mrow, betas, s2, c0, c1, lane, tab, ring, mx, s);
+      else if (first)
+        row_segment_staged<TM, false, true>(Mrow, betas, s2, c0, c1, lane, tab, ring, mx, s);
+      else if (fast)
+        row_segment_staged<TM, true, false>(Mrow, betas, s2, c0, c1, lane, tab, ring, mx, s);
       else
-        row_segment_staged<TM, false>(Mrow, betas, s2, c0, c1, lane, tab, ring, mx, s);
+        row_segment_staged<TM, false, false>(Mrow, betas, s2, c0, c1, lane, tab, ring, mx, s);
+    } else if (first) {
+      if (fast) row_segment<TM, true, true>(Mrow, betas, s2, c0, c1, lane, vec_ok, tab, mx, s);
+      else row_segment<TM, false, true>(Mrow, betas, s2, c0, c1, lane, vec_ok, tab, mx, s);
     } else if (fast) {
-      row_segment<TM, true>(Mrow, betas, s2, c0, c1, lane, vec_ok, tab, mx, s);
+      row_segment<TM, true, false>(Mrow, betas, s2, c0, c1, lane, vec_ok, tab, mx, s);
     } else {
-      row_segment<TM, false>(Mrow, betas, s2, c0, c1, lane, vec_ok, tab, mx, s);
+      row_segment<TM, false, false>(Mrow, betas, s2, c0, c1, lane, vec_ok, tab, mx, s);
     }
   }
   if (ring.failed && lane == 0) {
@@ -796,7 +826,7 @@ __global__ void plan_kernel(const TM* __restrict__ M, const double* __restrict__
 
 namespace {
 constexpr int kRingDynBytes = kWarps * kRingStages * kRingBytes;
-std::atomic<int> g_staged{1};
+std::atomic<int> g_staged{0};
 std::once_flag g_ring_attr_once;
 
 // Opt the pass kernels into kRingDynBytes of dynamic shared memory (once per

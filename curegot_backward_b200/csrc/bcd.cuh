@@ -68,7 +68,7 @@ void launch_plan(const TM* M, const double* alpha, const double* beta, double* P
                  double inv_eta, int n, int m, cudaStream_t stream);
 
 // Pass kernels stream long rows / column strips through shared-memory rings
-// filled by bulk copies (process-wide; default on).  Off: every pass reads M
+// filled by bulk copies (process-wide; default off, measured slower on B200).  Off: every pass reads M
 // with vector loads straight into registers.  Same results either way.
 void bcd_set_staging(bool on);
 

@@ -214,12 +214,20 @@ __global__ void __launch_bounds__(kCT, 1) bcd_cluster_kernel(const ClusterProb* 
 
   // ---- set-up: band of M, marginal logs, initial duals, control ----------
   load_exp2_table(tab);
+  bool nan_seen = false;
   for (size_t e = tid; e < (size_t)nrr * m; e += kCT) {
     const int i = (int)(e / m), j = (int)(e - (size_t)i * m);
-    Mb[(size_t)i * L.ldm + j] = Mg[(size_t)(r0 + i) * m + j];
+    const TM v = Mg[(size_t)(r0 + i) * m + j];
+    nan_seen |= (v != v);
+    Mb[(size_t)i * L.ldm + j] = v;
   }
+  // A NaN cost must not drop out of the sums like an infinite one (the
+  // exponent clamp ignores NaN): the band's rows get a NaN log-marginal, so
+  // the first iterate difference is NaN and every rank stops with
+  // `nonfinite` on the same gathered values.
+  nan_seen = __syncthreads_or(nan_seen) != 0;
   for (int i = tid; i < nrr; i += kCT) {
-    loga[i] = log(P.a[r0 + i]);
+    loga[i] = nan_seen ? __longlong_as_double(0x7ff8000000000000LL) : log(P.a[r0 + i]);
     const double v = P.x0 ? P.x0[r0 + i] : 0.0;
     alpha[i] = v;
     alphas[i] = v * s2;

@@ -37,6 +37,7 @@
 
 #include "bcd.cuh"
 #include "splr.cuh"
+#include "task.cuh"
 
 namespace cg {
 namespace {
@@ -47,6 +48,9 @@ double now_s() {
 }
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// SPLR solves multiplexed by one scheduler thread.
+constexpr int kSplrSlotsPerThread = 8;
 
 // Sinkhorn requests with at most this many bytes of M share the small batch.
 constexpr size_t kSmallBatchBytes = size_t(8) << 20;
@@ -573,15 +577,109 @@ void bcd_loop(cg_engine_s* E, int cls) {
   cudaStreamDestroy(st);
 }
 
-void splr_loop(cg_engine_s* E) {
+// One SPLR request in flight on a scheduler thread: its stream, its
+// resumable solve (splr_task) and the buffers the engine owns for it.
+struct SplrJob {
+  Req* q = nullptr;
+  cudaStream_t st = nullptr;
+  TaskIO io;
+  SolveTask task;
+  void* blk = nullptr;
+  double* ddual = nullptr;
+  int niter = 0, conv = 0;
+  bool finishing = false;  // final copy posted; waiting for its event
+};
+
+// SPLR scheduler: up to `slots` solves in flight, each a coroutine on its own
+// high-priority stream.  The thread starts admitted requests, then resumes
+// whichever solve's posted device read has landed (cudaEventQuery, no
+// blocking), so many solves share one host thread and their kernels overlap
+// on the device.  Decisions inside every solve are those of cg_splr_mixed /
+// cg_splr_f64 (the same coroutine, driven to completion there).
+void splr_loop(cg_engine_s* E, int slots) {
   cudaSetDevice(E->device);
   host_wait_yield(true);
-  cudaStream_t st;
   int prio_lo = 0, prio_hi = 0;
   cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
-  cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio_hi);
+  std::vector<cudaStream_t> streams(slots);
+  for (auto& s : streams) cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, prio_hi);
+  std::vector<cudaStream_t> free_streams(streams.rbegin(), streams.rend());
+  std::vector<SplrJob*> jobs;
+
+  auto start = [&](SplrJob* j) -> int {
+    const cg_request_t& r = j->q->r;
+    const int n = r.n, m = r.m;
+    const size_t es = r.m_f32 ? 4 : 8;
+    const void* dM = r.M;
+    const double *da = r.a, *db = r.b;
+    const size_t inb = r.host_inputs ? align256((size_t)n * m * es) + align256(8 * (size_t)(n + m)) : 0;
+    CG_TRY(pool_alloc_async(&j->blk, inb + align256(8 * (size_t)(n + m)), j->st));
+    char* p = static_cast<char*>(j->blk);
+    if (r.host_inputs) {
+      CG_TRY_CUDA(cudaMemcpyAsync(p, r.M, (size_t)n * m * es, cudaMemcpyHostToDevice, j->st));
+      dM = p;
+      double* dab = reinterpret_cast<double*>(p + align256((size_t)n * m * es));
+      CG_TRY_CUDA(cudaMemcpyAsync(dab, r.a, 8 * (size_t)n, cudaMemcpyHostToDevice, j->st));
+      CG_TRY_CUDA(cudaMemcpyAsync(dab + n, r.b, 8 * (size_t)m, cudaMemcpyHostToDevice, j->st));
+      da = dab;
+      db = dab + n;
+    }
+    j->ddual = reinterpret_cast<double*>(p + inb);
+    CG_TRY(j->io.init(j->st));
+    // the engine stops on the full marginal error, so every SPLR result
+    // meets tol on rows and on all m columns (the reference's test leaves
+    // the gauge column out)
+    SplrParams prm{r.eta, r.tol, r.max_iter, std::min(10.0 / std::min(n, m), 1.0), 1e-3, 30, 3,
+                   0, 1, &j->q->cancel};
+    if (r.m_f32)
+      j->task = splr_task<float>(&j->io, static_cast<const float*>(dM), da, db, nullptr, n, m,
+                                 prm, nullptr, j->ddual, &j->niter, &j->conv, nullptr, nullptr);
+    else
+      j->task = splr_task<double>(&j->io, static_cast<const double*>(dM), da, db, nullptr, n, m,
+                                  prm, nullptr, j->ddual, &j->niter, &j->conv, nullptr, nullptr);
+    j->task.resume();
+    return CG_OK;
+  };
+  // the solve has returned: status, duals out, release its frame and block
+  auto conclude = [&](SplrJob* j, int rc) {
+    Req* q = j->q;
+    const cg_request_t& r = q->r;
+    q->niter = j->niter;
+    q->converged = j->conv;
+    // the SPLR loop ends early without converging only on a non-finite
+    // objective or gradient norm (the reference's break, sinkhorn_splr.cu:1128)
+    if (rc == CG_OK && !j->conv && j->niter < r.max_iter) {
+      set_last_error("engine: SPLR objective or gradient became non-finite", __FILE__, __LINE__);
+      rc = CG_ERR_NONFINITE;
+    }
+    q->status = rc;
+    j->task = SolveTask();  // frame released: its workspace is freed stream-ordered
+    if (rc == CG_OK && r.dual_out)
+      cudaMemcpyAsync(r.dual_out, j->ddual, 8 * (size_t)(r.n + r.m),
+                      r.host_inputs ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, j->st);
+    if (j->blk) cudaFreeAsync(j->blk, j->st);
+    j->blk = nullptr;
+    if (j->io.ev) {
+      cudaEventRecord(j->io.ev, j->st);
+      j->io.posted = true;
+    }
+    j->finishing = true;
+  };
+  auto retire = [&](SplrJob* j) {
+    j->io.release();
+    free_streams.push_back(j->st);
+    {
+      std::lock_guard<std::mutex> lk(E->mu);
+      E->in_use -= std::min(j->q->footprint, E->in_use);
+      E->active_splr--;
+    }
+    E->cv.notify_all();
+    finish(E, j->q);
+    delete j;
+  };
+
   while (true) {
-    Req* q = nullptr;
+    std::vector<SplrJob*> admitted;
     {
       std::unique_lock<std::mutex> lk(E->mu);
       auto ready = [&](std::deque<Req*>& dq) {
@@ -589,82 +687,56 @@ void splr_loop(cg_engine_s* E) {
         Req* f = dq.front();
         return f->footprint > E->budget || E->in_use + f->footprint <= E->budget;
       };
-      E->cv.wait(lk, [&] { return E->stop || ready(E->splr_q); });
-      if (E->stop) break;
+      if (jobs.empty()) E->cv.wait(lk, [&] { return E->stop || ready(E->splr_q); });
+      if (E->stop && jobs.empty()) break;
       std::deque<Req*>& dq = E->splr_q;
-      if (dq.empty()) continue;
-      q = dq.front();
-      dq.pop_front();
-      if (q->footprint > E->budget) {
-        q->status = CG_ERR_ADMISSION;
-        lk.unlock();
-        finish(E, q);
-        continue;
+      while (!E->stop && (int)(jobs.size() + admitted.size()) < slots && ready(dq)) {
+        Req* q = dq.front();
+        dq.pop_front();
+        if (q->footprint > E->budget) {
+          q->status = CG_ERR_ADMISSION;
+          lk.unlock();
+          finish(E, q);
+          lk.lock();
+          continue;
+        }
+        E->in_use += q->footprint;
+        E->active_splr++;
+        auto* j = new SplrJob();
+        j->q = q;
+        j->st = free_streams.back();
+        free_streams.pop_back();
+        admitted.push_back(j);
       }
-      E->in_use += q->footprint;
-      E->active_splr++;
     }
-    q->t_admit = now_s();
-    const cg_request_t& r = q->r;
-    const int n = r.n, m = r.m;
-    const size_t es = r.m_f32 ? 4 : 8;
-    int rc = CG_OK;
-    void* blk = nullptr;
-    const void* dM = r.M;
-    const double *da = r.a, *db = r.b;
-    double* ddual = nullptr;
-    const size_t inb = r.host_inputs ? align256((size_t)n * m * es) + align256(8 * (size_t)(n + m)) : 0;
-    if (pool_alloc_async(&blk, inb + align256(8 * (size_t)(n + m)), st) != CG_OK) {
-      rc = CG_ERR_OOM;
-    } else {
-      char* p = static_cast<char*>(blk);
-      if (r.host_inputs) {
-        cudaMemcpyAsync(p, r.M, (size_t)n * m * es, cudaMemcpyHostToDevice, st);
-        dM = p;
-        double* dab = reinterpret_cast<double*>(p + align256((size_t)n * m * es));
-        cudaMemcpyAsync(dab, r.a, 8 * (size_t)n, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(dab + n, r.b, 8 * (size_t)m, cudaMemcpyHostToDevice, st);
-        da = dab;
-        db = dab + n;
+    for (SplrJob* j : admitted) {
+      j->q->t_admit = now_s();
+      const int rc = start(j);
+      jobs.push_back(j);
+      if (rc != CG_OK) conclude(j, rc);
+      else if (j->task.done()) conclude(j, j->task.rc());
+    }
+    bool progressed = !admitted.empty();
+    for (size_t k = 0; k < jobs.size();) {
+      SplrJob* j = jobs[k];
+      if (j->finishing) {
+        if (j->io.ready()) {
+          jobs[k] = jobs.back();
+          jobs.pop_back();
+          retire(j);
+          progressed = true;
+          continue;
+        }
+      } else if (j->io.ready()) {
+        j->task.resume();
+        progressed = true;
+        if (j->task.done()) conclude(j, j->task.rc());
       }
-      ddual = reinterpret_cast<double*>(p + inb);
-      // the engine stops on the full marginal error, so every SPLR result
-      // meets tol on rows and on all m columns (the reference's test leaves
-      // the gauge column out)
-      SplrParams prm{r.eta, r.tol, r.max_iter, std::min(10.0 / std::min(n, m), 1.0), 1e-3, 30, 3,
-                     0, 1, &q->cancel};
-      int niter = 0, conv = 0;
-      if (r.m_f32)
-        rc = splr_solve<float>(static_cast<const float*>(dM), da, db, nullptr, n, m, prm, nullptr,
-                               ddual, &niter, &conv, nullptr, nullptr, st);
-      else
-        rc = splr_solve<double>(static_cast<const double*>(dM), da, db, nullptr, n, m, prm,
-                                nullptr, ddual, &niter, &conv, nullptr, nullptr, st);
-      q->niter = niter;
-      q->converged = conv;
-      // the SPLR loop ends early without converging only on a non-finite
-      // objective or gradient norm (the reference's break, sinkhorn_splr.cu:1128)
-      if (rc == CG_OK && !conv && niter < r.max_iter) {
-        set_last_error("engine: SPLR objective or gradient became non-finite", __FILE__,
-                       __LINE__);
-        rc = CG_ERR_NONFINITE;
-      }
-      if (rc == CG_OK && r.dual_out)
-        cudaMemcpyAsync(r.dual_out, ddual, 8 * (size_t)(n + m),
-                        r.host_inputs ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, st);
-      cudaFreeAsync(blk, st);
-      host_wait(st);
+      ++k;
     }
-    q->status = rc;
-    {
-      std::lock_guard<std::mutex> lk(E->mu);
-      E->in_use -= std::min(q->footprint, E->in_use);
-      E->active_splr--;
-    }
-    E->cv.notify_all();
-    finish(E, q);
+    if (!progressed) std::this_thread::yield();
   }
-  cudaStreamDestroy(st);
+  for (auto& s : streams) cudaStreamDestroy(s);
 }
 
 }  // namespace
@@ -683,8 +755,17 @@ int cg_engine_create(size_t budget_bytes, int max_batch, int splr_workers, int c
   E->sms = cg::sm_count_current();
   E->threads.emplace_back(cg::bcd_loop, E, 0);
   E->threads.emplace_back(cg::bcd_loop, E, 1);
+  // splr_workers = SPLR solves in flight, spread over scheduler threads of
+  // at most kSplrSlotsPerThread solves each
   E->n_workers = splr_workers;
-  for (int w = 0; w < splr_workers; ++w) E->threads.emplace_back(cg::splr_loop, E);
+  if (splr_workers > 0) {
+    const int nthreads = std::max(1, (splr_workers + cg::kSplrSlotsPerThread - 1) /
+                                         cg::kSplrSlotsPerThread);
+    for (int w = 0; w < nthreads; ++w) {
+      const int slots = splr_workers / nthreads + (w < splr_workers % nthreads ? 1 : 0);
+      E->threads.emplace_back(cg::splr_loop, E, slots);
+    }
+  }
   *out = reinterpret_cast<cg_engine*>(E);
   return CG_OK;
 }

@@ -11,8 +11,10 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <vector>
 
 #include "bcd.cuh"
+#include "task.cuh"
 #include "workspace.cuh"
 
 namespace cg {
@@ -162,6 +164,102 @@ int read_device_bulk(void* host, const void* dev, size_t bytes, cudaStream_t st)
   CG_TRY(host_wait(st));
   std::memcpy(host, buf.p, bytes);
   return CG_OK;
+}
+
+// Pool of (pinned buffer, event) pairs for resumable solves.
+namespace {
+struct IoSlot {
+  void* pinned;
+  cudaEvent_t ev;
+  int dev;
+};
+std::mutex g_io_mu;
+std::vector<IoSlot> g_io_free;
+}  // namespace
+
+int TaskIO::init(cudaStream_t s) {
+  st = s;
+  err = CG_OK;
+  posted = false;
+  count = 0;
+  int dev = 0;
+  CG_TRY_CUDA(cudaGetDevice(&dev));
+  {
+    std::lock_guard<std::mutex> lk(g_io_mu);
+    for (size_t k = 0; k < g_io_free.size(); ++k)
+      if (g_io_free[k].dev == dev) {
+        pinned = g_io_free[k].pinned;
+        ev = g_io_free[k].ev;
+        g_io_free.erase(g_io_free.begin() + k);
+        return CG_OK;
+      }
+  }
+  CG_TRY_CUDA(cudaHostAlloc(&pinned, kTaskPinnedBytes, cudaHostAllocDefault));
+  const cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    cudaFreeHost(pinned);
+    pinned = nullptr;
+    CG_TRY_CUDA(e);
+  }
+  return CG_OK;
+}
+
+void TaskIO::release() {
+  if (!pinned) return;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_io_mu);
+  g_io_free.push_back({pinned, ev, dev});
+  pinned = nullptr;
+  ev = nullptr;
+}
+
+int TaskIO::wait() {
+  if (!posted) return CG_OK;
+  if (!t_wait_yield) {
+    CG_TRY_CUDA(cudaEventSynchronize(ev));
+    return CG_OK;
+  }
+  while (true) {
+    const cudaError_t q = cudaEventQuery(ev);
+    if (q == cudaSuccess) return CG_OK;
+    if (q != cudaErrorNotReady) CG_TRY_CUDA(q);
+    if (t_wait_yield) std::this_thread::yield();
+  }
+}
+
+TaskIO::Await TaskIO::read_spans(const ReadSpan* sp, int cnt) {
+  size_t total = 0;
+  for (int k = 0; k < cnt; ++k) total += sp[k].bytes;
+  if (cnt > kTaskMaxSpans || total > kTaskPinnedBytes) {
+    set_last_error("task read: too many bytes or spans", __FILE__, __LINE__);
+    err = CG_ERR_INVALID_ARG;
+    return Await{this};
+  }
+  count = cnt;
+  char* pin = static_cast<char*>(pinned);
+  size_t off = 0;
+  for (int k = 0; k < cnt; ++k) {
+    spans[k] = sp[k];
+    if (sp[k].bytes) {
+      const cudaError_t e =
+          cudaMemcpyAsync(pin + off, sp[k].dev, sp[k].bytes, cudaMemcpyDeviceToHost, st);
+      if (e != cudaSuccess) {
+        set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
+        err = status_from_cuda(e);
+        return Await{this};
+      }
+    }
+    off += sp[k].bytes;
+  }
+  const cudaError_t e = cudaEventRecord(ev, st);
+  if (e != cudaSuccess) {
+    set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
+    err = status_from_cuda(e);
+    return Await{this};
+  }
+  posted = true;
+  return Await{this};
 }
 
 int read_device(void* host1, const void* dev1, size_t bytes1, cudaStream_t st, void* host2,

@@ -26,6 +26,7 @@
 
 #include "bcd.cuh"
 #include "splr.cuh"
+#include "task.cuh"
 #include "tpass.cuh"
 #include "workspace.cuh"
 
@@ -237,11 +238,6 @@ __global__ void inv_diag_kernel(const double* val, const int* rowptr, int n, int
   }
 }
 
-template <typename T>
-int read_dev(T* host, const T* dev, cudaStream_t st) {
-  return read_device(host, dev, sizeof(T), st);
-}
-
 // ---------------------------------------------------------------------------
 // Line-search step selection: quadratic_minimizer (x2), cubic_minimizer and
 // step_selection of the reference's src/utils.h:76-230, ported expression for
@@ -396,21 +392,24 @@ static void hblock_carve(void* base, int n, int m, long long kcap, int k, bool b
   hb.err = reinterpret_cast<int*>(take(sizeof(int)));
 }
 
+// The SPLR solve as a resumable task: it suspends at every device read (see
+// task.cuh).  splr_solve drives it to completion on the calling thread; the
+// serving engine drives many at once.  `prm` is copied into the task.
 template <typename TM>
-int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int n, int m,
-                      const SplrParams& prm, const double* x0, double* dual, int* niter_out,
-                      int* converged_out, cg_ctx_s** ctx_out, double* trace,
-                      cudaStream_t st) {
+SolveTask splr_task(TaskIO* io, const TM* M, const double* a, const double* b, double* Pout,
+                    int n, int m, SplrParams prm, const double* x0, double* dual,
+                    int* niter_out, int* converged_out, cg_ctx_s** ctx_out, double* trace) {
+  const cudaStream_t st = io->st;
   const bool f32 = sizeof(TM) == 4;
   const double reg = prm.reg;
   if (!M || !a || !b || n <= 0 || m <= 0 || !(reg > 0.0) || !std::isfinite(reg) ||
       prm.cycle <= 0) {
     set_last_error("cg_splr: invalid argument", __FILE__, __LINE__);
-    return CG_ERR_INVALID_ARG;
+    co_return CG_ERR_INVALID_ARG;
   }
   if ((long long)(n + m) * (n + m) >= (1LL << 31)) {
     set_last_error("cg_splr: n + m too large for 32-bit Hsl indices", __FILE__, __LINE__);
-    return CG_ERR_INVALID_ARG;
+    co_return CG_ERR_INVALID_ARG;
   }
   const int H = n + m - 1;
   const long long Te = (long long)n * (m - 1);
@@ -427,9 +426,9 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
   bool big_alpha = true;
   schur_dims(n, m, k, big_alpha);
   cusolverDnHandle_t sol = nullptr;
-  CG_TRY(solver_handle(&sol));
+  CO_TRY(solver_handle(&sol));
   int lwork = 0;
-  CG_TRY(schur_lwork(sol, k, lwork));
+  CO_TRY(schur_lwork(sol, k, lwork));
 
   // context-capable block: plain cudaMalloc when a context will own it (it
   // may outlive the stream), stream-ordered otherwise (no device-wide sync)
@@ -437,9 +436,9 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
   void* hbase = nullptr;
   const bool owned_by_ctx = (ctx_out != nullptr);
   if (owned_by_ctx) {
-    CG_TRY_CUDA(cudaMalloc(&hbase, hbytes));
+    CO_TRY_CUDA(cudaMalloc(&hbase, hbytes));
   } else {
-    CG_TRY(pool_alloc_async(&hbase, hbytes, st));
+    CO_TRY(pool_alloc_async(&hbase, hbytes, st));
   }
   HBlock hb;
   hblock_carve(hbase, n, m, Kmax, k, big_alpha, lwork, hb);
@@ -510,7 +509,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
   const size_t o_bcnt = ws.reserve<unsigned int>(bcount);
   const size_t o_bst = ws.reserve<BcdState>(1);
   const size_t o_bprob = ws.reserve<BcdProb>(1);
-  CG_TRY(ws.allocate());
+  CO_TRY(ws.allocate());
 
   double* ab = ws.at<double>(o_ab);
   double* logab = ws.at<double>(o_logab);
@@ -553,14 +552,14 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
   cp.st = ws.at<BcdState>(o_bst);
   BcdProb* dcp = ws.at<BcdProb>(o_bprob);
 
-  CG_TRY_CUDA(cudaMemcpyAsync(ab, a, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
-  CG_TRY_CUDA(cudaMemcpyAsync(ab + n, b, m * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  CO_TRY_CUDA(cudaMemcpyAsync(ab, a, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  CO_TRY_CUDA(cudaMemcpyAsync(ab + n, b, m * sizeof(double), cudaMemcpyDeviceToDevice, st));
   { log_kernel<<<grid_for(n + m, 256, 1024), 256, 0, st>>>(ab, logab, n + m); cg::count_launch(); }
-  CG_TRY_CUDA(cudaMemcpyAsync(dcp, &cp, sizeof(BcdProb), cudaMemcpyHostToDevice, st));
-  CG_TRY_CUDA(cudaMemsetAsync(tcnt, 0, (tsplits + tstrips + 1) * sizeof(unsigned int), st));
-  CG_TRY_CUDA(cudaMemsetAsync(gamma_prev, 0, (n + m) * sizeof(double), st));
-  CG_TRY_CUDA(cudaMemsetAsync(grad_prev, 0, H * sizeof(double), st));
-  CG_TRY_CUDA(cudaMemsetAsync(hb.dres, 0, sizeof(DirRes), st));
+  CO_TRY_CUDA(cudaMemcpyAsync(dcp, &cp, sizeof(BcdProb), cudaMemcpyHostToDevice, st));
+  CO_TRY_CUDA(cudaMemsetAsync(tcnt, 0, (tsplits + tstrips + 1) * sizeof(unsigned int), st));
+  CO_TRY_CUDA(cudaMemsetAsync(gamma_prev, 0, (n + m) * sizeof(double), st));
+  CO_TRY_CUDA(cudaMemsetAsync(grad_prev, 0, H * sizeof(double), st));
+  CO_TRY_CUDA(cudaMemsetAsync(hb.dres, 0, sizeof(DirRes), st));
 
   // T-pass launcher
   TPassArgs ta{};
@@ -572,11 +571,14 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
   ta.ab = ab;
   ta.strips = tstrips;
   ta.splits = tsplits;
+  // workspace of the trial-point slots: [K x rowpart | K x colpart | K x scal],
+  // the strides tpass_kernel's slot k uses
   ta.rowpart = tw;
-  ta.colpart = tw + (size_t)tstrips * n;
-  ta.scal = tw + (size_t)tstrips * n + (size_t)tsplits * m;
+  ta.colpart = tw + (size_t)kMaxTrialSteps * tstrips * n;
+  ta.scal = ta.colpart + (size_t)kMaxTrialSteps * tsplits * m;
   ta.counters = tcnt;
-  auto eval_at = [&](double* g, double* gr, double* r, double* c, TResult* out, TResult& host,
+  // plan pass at a given point (not a trial); its TResult lands in `out`
+  auto eval_at = [&](double* g, double* gr, double* r, double* c, TResult* out,
                      const double* dir) -> int {
     TPassArgs x = ta;
     x.gamma = g;
@@ -588,8 +590,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     x.cols = c;
     x.grad = gr;
     x.res = out;
-    CG_TRY(launch_tpass(f32, x, st));
-    return read_dev(&host, out, st);
+    return launch_tpass(f32, x, st);
   };
   // Trial passes.  A pass evaluates `step` in slot 0 and, when spec > 0, a
   // speculative second step in slot 1 (one read of M, the same values as two
@@ -630,20 +631,15 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
       latest[k].valid = true;
     }
   };
-  auto trial = [&](double step, double spec, TResult& host) -> int {
+  // a slot of the latest pass holding `step` (bitwise): no pass needed
+  auto trial_cached = [&](double step, TResult& host) -> bool {
     for (int k = 0; k < kMaxTrialSteps; ++k)
       if (latest[k].valid && latest[k].step == step) {
         host = latest[k].r;
         cur_slot = k;
-        return CG_OK;
+        return true;
       }
-    CG_TRY(trial_launch(step, spec));
-    TResult r2[kMaxTrialSteps];
-    CG_TRY(read_device(r2, res, (spec > 0.0 ? 2 : 1) * sizeof(TResult), st));
-    trial_latch(r2, spec > 0.0 ? 2 : 1);
-    host = r2[0];
-    cur_slot = 0;
-    return CG_OK;
+    return false;
   };
   // Make slot 0 the current point when the last evaluation came from slot 1.
   auto settle_slot = [&]() -> int {
@@ -668,18 +664,19 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
 
   // init_dual (sinkhorn_splr.cu:330-359)
   if (x0) {
-    CG_TRY_CUDA(cudaMemcpyAsync(gamma, x0, (n + m) * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CO_TRY_CUDA(cudaMemcpyAsync(gamma, x0, (n + m) * sizeof(double), cudaMemcpyDeviceToDevice, st));
     { shift_inplace_kernel<<<1, 1024, 0, st>>>(gamma, n, m); cg::count_launch(); }
   } else {
     bcd_sweeps(nullptr, true, 0);
     // alpha in buffer 1, beta = 0
-    CG_TRY_CUDA(cudaMemcpyAsync(gamma, cp.alpha[1], n * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    CG_TRY_CUDA(cudaMemsetAsync(gamma + n, 0, m * sizeof(double), st));
+    CO_TRY_CUDA(cudaMemcpyAsync(gamma, cp.alpha[1], n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CO_TRY_CUDA(cudaMemsetAsync(gamma + n, 0, m * sizeof(double), st));
   }
-  CG_TRY_CUDA(cudaGetLastError());
+  CO_TRY_CUDA(cudaGetLastError());
 
   TResult tr{};
-  CG_TRY(eval_at(gamma, grad, rows, cols, res, tr, nullptr));
+  CO_TRY(eval_at(gamma, grad, rows, cols, res, nullptr));
+  CO_TRY(co_await io->read(&tr, res, sizeof(TResult)));
   double objfn = tr.f, gnorm = tr.gnorm;
   double gfull = tr.gfull;  // full marginal error, for the full_stop test
   const double gnorm_init = gnorm;
@@ -784,7 +781,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     pattern_new = true;
     return sparsify_select_and_build(f32, M, gamma, rows, cols, n, m, s2, sh, Ks, hb.A, sw, st);
   };
-  CG_TRY(dual_sphess(density, shift * reg, false));
+  CO_TRY(dual_sphess(density, shift * reg, false));
 
   // Speculative second trial point in the line search's passes: always for
   // problems whose pass is latency-bound (the second point costs no time),
@@ -799,7 +796,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
   for (int iter = 0; iter < prm.max_iter; ++iter) {
     if (prm.cancel && prm.cancel->load(std::memory_order_relaxed)) {
       set_last_error("cg_splr: cancelled", __FILE__, __LINE__);
-      return CG_ERR_CANCELLED;
+      co_return CG_ERR_CANCELLED;
     }
     if (prm.verbose >= 1)
       printf("iter = %d, objval = %.10g, ||grad|| = %.10g\n", iter, objfn, gnorm);
@@ -821,20 +818,21 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
       bcd_sweeps(gamma + n, false, cand);
       { shift_assemble_kernel<<<grid_for(n + m, 256, 1024), 256, 0, st>>>(
           gamma_bcd, cp.alpha[(cand + 1) & 1], cp.beta[cand & 1], n, m); cg::count_launch(); }
-      CG_TRY(eval_at(gamma_bcd, grad_c, rows_c, cols_c, res_c, trc, nullptr));
+      // its result is read together with the direction's status below
+      CO_TRY(eval_at(gamma_bcd, grad_c, rows_c, cols_c, res_c, nullptr));
     }
 
     // search direction (sinkhorn_splr.cu:538-649); rhs2 = [g, y] was
     // written by lowrank_kernel
     int sp_bad = 0;
     const int nrhs = (iter > 0) ? 2 : 1;
-    CG_TRY(factor_solve_direction(&sp_bad, hb.rhs2, hb.sol2, nrhs));
+    CO_TRY(factor_solve_direction(&sp_bad, hb.rhs2, hb.sol2, nrhs));
     g_last_dir = path;
     // Woodbury correction, scaling, <g, d>, and save_history (first H
     // entries of gamma and g) in one launch
     { woodbury_kernel<<<1, 1024, 0, st>>>(hb.sol2, hb.sol2 + H, grad, hb.rhs2 + H, hb.s, H, reg, 1,
                                         hb.dres, gamma, gamma_prev, grad_prev); cg::count_launch(); }
-    CG_TRY_CUDA(cudaGetLastError());
+    CO_TRY_CUDA(cudaGetLastError());
 
     // The line search's first trial point depends only on the previous step
     // length, so its pass is queued behind the direction solve and read back
@@ -853,7 +851,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
       const double t = std::min(step_max, step + delta_max_spec * (step - I_lo));
       return (t > step) ? t : 0.0;
     };
-    CG_TRY(trial_launch(init_step, spec_after(init_step, 0.0)));
+    CO_TRY(trial_launch(init_step, spec_after(init_step, 0.0)));
     DirRes dr{};
     TResult t_first[kMaxTrialSteps]{};
     int info2[2] = {0, 0};
@@ -862,10 +860,11 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     factor_info_src(&isrc, &ibytes);
     {
       const int nfirst = latest[1].step > 0.0 ? 2 : 1;
-      const ReadSpan spans[3] = {{&dr, hb.dres, sizeof(DirRes)},
+      const ReadSpan spans[4] = {{&dr, hb.dres, sizeof(DirRes)},
                                  {info2, isrc, ibytes},
-                                 {t_first, res, nfirst * sizeof(TResult)}};
-      CG_TRY(read_device_spans(spans, 3, st));
+                                 {t_first, res, nfirst * sizeof(TResult)},
+                                 {&trc, res_c, use_cand ? sizeof(TResult) : 0}};
+      CO_TRY(co_await io->read_spans(spans, 4));
       trial_latch(t_first, nfirst);
       cur_slot = 0;
     }
@@ -873,7 +872,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     if (sp_bad || info2[0] != 0 || info2[1] != 0) {
       set_last_error("direction solve: sparsified Hessian not positive definite", __FILE__,
                      __LINE__);
-      return CG_ERR_NOT_SPD;
+      co_return CG_ERR_NOT_SPD;
     }
     ys = dr.ys;
     yy = dr.yy;
@@ -917,7 +916,16 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
           // the first trial (init_step) comes from the pass queued behind the
           // direction solve; later ones from the latest pass when it holds
           // the step, else from a new pass
-          CG_TRY(trial(step, spec_after(step, I_lo), t));
+          if (!trial_cached(step, t)) {
+            const double sp = spec_after(step, I_lo);
+            const int ns = sp > 0.0 ? 2 : 1;
+            CO_TRY(trial_launch(step, sp));
+            TResult r2[kMaxTrialSteps];
+            CO_TRY(co_await io->read(r2, res, ns * sizeof(TResult)));
+            trial_latch(r2, ns);
+            t = r2[0];
+            cur_slot = 0;
+          }
           ++trials;
           fx = t.f;
           dg = t.dg;
@@ -990,7 +998,12 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     const double gnorm_pre = gnorm;
     if (recompute_fg) {
       TResult t{};
-      CG_TRY(trial(alpha_step, 0.0, t));  // no pass when the latest one holds it
+      if (!trial_cached(alpha_step, t)) {  // no pass when the latest one holds it
+        CO_TRY(trial_launch(alpha_step, 0.0));
+        CO_TRY(co_await io->read(&t, res, sizeof(TResult)));
+        trial_latch(&t, 1);
+        cur_slot = 0;
+      }
       objfn = t.f;
       gnorm = t.gnorm;
       gfull = t.gfull;
@@ -998,16 +1011,17 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
       gnorm = last_trial_gnorm;  // f, g and ||g|| of the last trial are current
       gfull = last_trial_gfull;
     }
-    CG_TRY(settle_slot());
+    CO_TRY(settle_slot());
     speculate = small_problem || trials > 1;
 
     bool cand_accepted = false;
     if (use_cand) {
       if ((trc.f < objfn) && (trc.gnorm < 10 * gnorm)) {
         cand_accepted = true;
-        CG_TRY_CUDA(cudaMemcpyAsync(gamma, gamma_bcd, H * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        CO_TRY_CUDA(cudaMemcpyAsync(gamma, gamma_bcd, H * sizeof(double), cudaMemcpyDeviceToDevice, st));
         TResult t{};
-        CG_TRY(eval_at(gamma, grad, rows, cols, res, t, nullptr));
+        CO_TRY(eval_at(gamma, grad, rows, cols, res, nullptr));
+        CO_TRY(co_await io->read(&t, res, sizeof(TResult)));
         objfn = t.f;
         gnorm = t.gnorm;
         gfull = t.gfull;
@@ -1032,7 +1046,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     const bool stop_after = converged_after || max_iter_reached || invalid_after;
     if (!stop_after) {
       shift = std::min(gnorm, prm.shift_max);
-      CG_TRY(dual_sphess(density, shift * reg, !update));
+      CO_TRY(dual_sphess(density, shift * reg, !update));
     }
     niter = iter + 1;
     if (stop_after) {
@@ -1045,14 +1059,14 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
   if (niter_out) *niter_out = niter;
   if (converged_out) *converged_out = converged ? 1 : 0;
   if (Pout) launch_plan<TM>(M, gamma, gamma + n, Pout, 1.0 / reg, n, m, st);
-  if (dual) CG_TRY_CUDA(cudaMemcpyAsync(dual, gamma, (n + m) * sizeof(double), cudaMemcpyDeviceToDevice, st));
-  CG_TRY_CUDA(cudaGetLastError());
+  if (dual) CO_TRY_CUDA(cudaMemcpyAsync(dual, gamma, (n + m) * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  CO_TRY_CUDA(cudaGetLastError());
 
   if (ctx_out) {
     *ctx_out = nullptr;
     int ctx_sp_bad = 0;
     cg_ctx_s* c = new cg_ctx_s();
-    CG_TRY_CUDA(cudaGetDevice(&c->device));
+    CO_TRY_CUDA(cudaGetDevice(&c->device));
     c->n = n;
     c->m = m;
     c->H = H;
@@ -1068,7 +1082,7 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
         int rc = factor_direction(&ctx_sp_bad);
         if (rc != CG_OK) {
           delete c;
-          return rc;
+          co_return rc;
         }
       }
     } else {
@@ -1088,13 +1102,13 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     c->dres = hb.dres;
     c->err = hb.err;
     int rp = 0;
-    CG_TRY_CUDA(cudaMemcpyAsync(c->point, c->fallback ? gamma : gamma_prev, H * sizeof(double),
+    CO_TRY_CUDA(cudaMemcpyAsync(c->point, c->fallback ? gamma : gamma_prev, H * sizeof(double),
                                 cudaMemcpyDeviceToDevice, st));
     int info2[2] = {0, 0};
     const int* isrc = nullptr;
     size_t ibytes = 0;
     factor_info_src(&isrc, &ibytes);
-    CG_TRY(read_device(&rp, hb.A.rowptr + H, sizeof(int), st, info2, isrc, ibytes));
+    CO_TRY(read_device(&rp, hb.A.rowptr + H, sizeof(int), st, info2, isrc, ibytes));
     const int info = ctx_sp_bad | info2[0] | info2[1];
     c->nnz = rp;
     c->has_point = true;
@@ -1106,9 +1120,31 @@ int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int 
     *ctx_out = c;
   }
   ws.release();
-  return CG_OK;
+  co_return CG_OK;
 }
 
+template <typename TM>
+int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int n, int m,
+               const SplrParams& prm, const double* x0, double* dual, int* niter_out,
+               int* converged_out, cg_ctx_s** ctx_out, double* trace, cudaStream_t st) {
+  TaskIO io;
+  CG_TRY(io.init(st));
+  int rc;
+  {
+    SolveTask t = splr_task<TM>(&io, M, a, b, Pout, n, m, prm, x0, dual, niter_out,
+                                converged_out, ctx_out, trace);
+    rc = drive_task(t, io);
+  }  // the task's frame (workspace, factor blocks) is released here, stream-ordered
+  io.release();
+  return rc;
+}
+
+template SolveTask splr_task<double>(TaskIO*, const double*, const double*, const double*,
+                                     double*, int, int, SplrParams, const double*, double*, int*,
+                                     int*, cg_ctx_s**, double*);
+template SolveTask splr_task<float>(TaskIO*, const float*, const double*, const double*, double*,
+                                    int, int, SplrParams, const double*, double*, int*, int*,
+                                    cg_ctx_s**, double*);
 template int splr_solve<double>(const double*, const double*, const double*, double*, int, int,
                                 const SplrParams&, const double*, double*, int*, int*,
                                 cg_ctx_s**, double*, cudaStream_t);

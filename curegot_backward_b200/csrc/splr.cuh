@@ -41,7 +41,17 @@ struct SplrParams {
   const std::atomic<bool>* cancel = nullptr;
 };
 
-// The SPLR solve (splr.cu).  M is float (mixed) or double; everything else FP64.
+struct TaskIO;
+struct SolveTask;
+
+// The SPLR solve as a resumable task on io->st (task.cuh; splr.cu).
+template <typename TM>
+SolveTask splr_task(TaskIO* io, const TM* M, const double* a, const double* b, double* Pout,
+                    int n, int m, SplrParams prm, const double* x0, double* dual,
+                    int* niter_out, int* converged_out, cg_ctx_s** ctx_out, double* trace);
+
+// The SPLR solve (splr.cu), driven to completion on the calling thread.  M is
+// float (mixed) or double; everything else FP64.
 template <typename TM>
 int splr_solve(const TM* M, const double* a, const double* b, double* Pout, int n, int m,
                const SplrParams& prm, const double* x0, double* dual, int* niter_out,

@@ -116,7 +116,7 @@ int cg_bcd_set_cluster_path(int enable);
 
 /*
  * Memory pipeline of the multi-CTA Sinkhorn passes (process-wide; default
- * on).  When enabled, rows and column strips long enough to stream are
+ * off: on B200 the register path measured 10-18% faster).  When enabled, rows and column strips long enough to stream are
  * brought into per-warp shared-memory rings by bulk asynchronous copies
  * (three 2 KB stages per warp, completion on mbarriers with bounded waits)
  * and read from there; disabled, the passes load M straight into registers.

@@ -226,6 +226,6 @@ def test_staged_passes_are_bitwise_the_unstaged_ones(cuda_dev, precision, n, m):
             out[on] = _solvers._bcd_device(M, a, b, 0.02, 1e-8, 3000, None, precision,
                                            want_plan=False)
     finally:
-        cg.set_bcd_staging(True)
+        cg.set_bcd_staging(False)  # the library default
     assert out[True][0] == out[False][0]
     assert torch.equal(out[True][2], out[False][2])
