@@ -80,6 +80,22 @@ def set_bcd_staging(enabled: bool = True) -> None:
     _native.call("cg_bcd_set_staging", 1 if enabled else 0)
 
 
+def set_bcd_shifted_lse(enabled: bool = True) -> None:
+    """Shifted log-sum-exp sums in the Sinkhorn passes (default on): after
+    the first pass, each row / column sums relative to its previous LSE when
+    the other side's duals moved by less than 40 base-2 units, with no running
+    maximum.  Off, every pass keeps the running maximum.  Results agree to
+    rounding."""
+    _native.call("cg_bcd_set_shifted_lse", 1 if enabled else 0)
+
+
+def set_bcd_l2_prefetch(chunks: int) -> None:
+    """L2 prefetch distance of the Sinkhorn passes, in warp loop steps
+    (0 = off, at most 64).  A hint only: results are bitwise the same for
+    every setting."""
+    _native.call("cg_bcd_set_l2_prefetch", int(chunks))
+
+
 _DIRSOLVE = {"auto": 0, "dense": 1, "sparse": 2, "peel": 3}
 
 

@@ -110,6 +110,8 @@ SIGNATURES = {
                            c_int, c_int, c_int_p, c_void_p, c_void_p, c_void_p],
     "cg_bcd_set_cluster_path": [c_int],
     "cg_bcd_set_staging": [c_int],
+    "cg_bcd_set_l2_prefetch": [c_int],
+    "cg_bcd_set_shifted_lse": [c_int],
     "cg_points_cost_bf16": [c_void_p, c_void_p, c_int, c_int, c_int, c_double, c_void_p, c_void_p],
     "cg_bcd_points_bf16": [c_void_p, c_void_p, c_int, c_int, c_int, c_double, c_void_p, c_void_p,
                            c_double, c_int, c_double, c_int, c_int_p, c_void_p, c_int_p,

@@ -50,16 +50,23 @@ struct RowU {
   static constexpr int U = (Vec<TM>::N == 4) ? 2 : 4;
 };
 
+// L2 bulk prefetch of the chunk [pos, min(pos + span, c1)) of a row whose
+// 16-byte vectors are aligned (c1 is a multiple of the vector width).
+template <typename TM>
+__device__ __forceinline__ void prefetch_row_chunk(const TM* Mrow, int pos, int c1, int span) {
+  if (pos < c1) prefetch_l2_bulk(Mrow + pos, (uint32_t)(min(span, c1 - pos) * (int)sizeof(TM)));
+}
+
 // One warp's segment [c0, c1) of row `row`: LSE over j of (betas_j - s2*M_ij).
 // Full chunks run predicate-free with the next chunk's M vectors prefetched.
 // CHECK (first pass of a solve): a NaN exponent (NaN in M or the duals) makes
 // the row's sum NaN.  Without it a NaN entry would drop out of the sum like
 // an infinite cost: the exponent clamp of the exponential ignores NaN.
-template <typename TM, bool FAST, bool CHECK>
+template <typename TM, bool FAST, bool CHECK, bool SHIFT>
 __device__ __forceinline__ void row_segment(const TM* __restrict__ Mrow,
                                             const double* __restrict__ betas, double s2, int c0,
                                             int c1, int lane, bool vec_ok, const double* tab,
-                                            double& mx, double& s) {
+                                            int pf, double& mx, double& s) {
   bool bad = false;
   constexpr int VN = Vec<TM>::N;
   if (vec_ok) {
@@ -73,7 +80,12 @@ __device__ __forceinline__ void row_segment(const TM* __restrict__ Mrow,
 #pragma unroll
       for (int u = 0; u < U; ++u) nxt[u] = Raw<TM>::load(Mrow + cb + lane * VN + u * step);
     }
+    // L2 prefetch pf chunks ahead (lane 0, one bulk hint per chunk); chunks
+    // 0 and 1 are already on their way through the register prefetch.
+    if (pf > 0 && lane == 0)
+      for (int k = 2; k < pf; ++k) prefetch_row_chunk(Mrow, cb + k * span, c1, span);
     for (; cb + span <= c1; cb += span) {
+      if (pf > 0 && lane == 0) prefetch_row_chunk(Mrow, cb + pf * span, c1, span);
       RT cur[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) cur[u] = nxt[u];
@@ -92,7 +104,7 @@ __device__ __forceinline__ void row_segment(const TM* __restrict__ Mrow,
       if (CHECK)
 #pragma unroll
         for (int q = 0; q < U * VN; ++q) bad |= (d[q] != d[q]);
-      lse_chunk_full<FAST, U * VN>(d, mx, s, tab);
+      lse_chunk_full<FAST, U * VN, SHIFT>(d, mx, s, tab);
     }
     // tail (vectors that are in range, then nothing: c1 is a multiple of VN)
     for (int j = cb + lane * VN; j < c1; j += step) {
@@ -109,7 +121,7 @@ __device__ __forceinline__ void row_segment(const TM* __restrict__ Mrow,
       if (CHECK)
 #pragma unroll
         for (int q = 0; q < VN; ++q) bad |= (d[q] != d[q]);
-      lse_chunk<FAST, VN>(d, ok, mx, s, tab);
+      lse_chunk<FAST, VN, SHIFT>(d, ok, mx, s, tab);
     }
   } else {
     for (int j0 = c0 + lane; j0 < c1; j0 += 32 * kUnroll) {
@@ -124,7 +136,7 @@ __device__ __forceinline__ void row_segment(const TM* __restrict__ Mrow,
       if (CHECK)
 #pragma unroll
         for (int q = 0; q < kUnroll; ++q) bad |= (ok[q] && d[q] != d[q]);
-      lse_chunk<FAST, kUnroll>(d, ok, mx, s, tab);
+      lse_chunk<FAST, kUnroll, SHIFT>(d, ok, mx, s, tab);
     }
   }
   if (CHECK && bad) s = __longlong_as_double(0x7ff8000000000000LL);
@@ -137,7 +149,7 @@ __device__ __forceinline__ void row_segment(const TM* __restrict__ Mrow,
 // span is processed exactly like row_segment's loop body -- same grouping,
 // same order, bitwise the same (mx, s).  The tail (< one span) is read as in
 // row_segment.  A ring wait that gives up leaves ring.failed set.
-template <typename TM, bool FAST, bool CHECK>
+template <typename TM, bool FAST, bool CHECK, bool SHIFT>
 __device__ __forceinline__ void row_segment_staged(const TM* __restrict__ Mrow,
                                                    const double* __restrict__ betas, double s2,
                                                    int c0, int c1, int lane, const double* tab,
@@ -186,7 +198,7 @@ __device__ __forceinline__ void row_segment_staged(const TM* __restrict__ Mrow,
       if (CHECK)
 #pragma unroll
         for (int q = 0; q < U * VN; ++q) bad |= (d[q] != d[q]);
-      lse_chunk_full<FAST, U * VN>(d, mx, s, tab);
+      lse_chunk_full<FAST, U * VN, SHIFT>(d, mx, s, tab);
     }
     ring.consumed++;
     __syncwarp();
@@ -212,7 +224,7 @@ __device__ __forceinline__ void row_segment_staged(const TM* __restrict__ Mrow,
     if (CHECK)
 #pragma unroll
       for (int q = 0; q < VN; ++q) bad |= (d[q] != d[q]);
-    lse_chunk<FAST, VN>(d, ok, mx, s, tab);
+    lse_chunk<FAST, VN, SHIFT>(d, ok, mx, s, tab);
   }
   if (CHECK && bad) s = __longlong_as_double(0x7ff8000000000000LL);
 }
@@ -257,6 +269,17 @@ __device__ __forceinline__ void cta_stats(double v, bool valid, double* red, dou
 }
 }  // namespace
 
+template <typename TM, bool FAST, bool CHECK, bool SHIFT>
+__device__ __forceinline__ void row_any(bool use_ring, const TM* __restrict__ Mrow,
+                                        const double* __restrict__ betas, double s2, int c0,
+                                        int c1, int lane, bool vec_ok, const double* tab, int pf,
+                                        WarpRing& ring, double& mx, double& s) {
+  if (use_ring)
+    row_segment_staged<TM, FAST, CHECK, SHIFT>(Mrow, betas, s2, c0, c1, lane, tab, ring, mx, s);
+  else
+    row_segment<TM, FAST, CHECK, SHIFT>(Mrow, betas, s2, c0, c1, lane, vec_ok, tab, pf, mx, s);
+}
+
 // ---------------------------------------------------------------------------
 // Row pass: alpha^{t+1}_i = eta * (log a_i - LSE_j((beta^t_j - M_ij) / eta))
 // ---------------------------------------------------------------------------
@@ -265,7 +288,10 @@ template <typename TM>
 __device__ __forceinline__ void row_block(const BcdProb* __restrict__ probs,
                                           const int* __restrict__ cta_prob,
                                           const int* __restrict__ cta_start, int vb,
-                                          bool staged, WarpRing& ring) {
+                                          int flags, WarpRing& ring) {
+  const bool staged = (flags & kPassStaged) != 0;
+  const bool online = (flags & kPassOnline) != 0;
+  const int pf = flags >> kPassPrefetchShift;
   __shared__ double tab[kExp2TableSize];
   __shared__ double sm_mx[kWarps], sm_s[kWarps];
   __shared__ double sm_v[kWarps][2];
@@ -282,6 +308,7 @@ __device__ __forceinline__ void row_block(const BcdProb* __restrict__ probs,
   const bool check = ldcg(&st->check_pending) != 0;
   const bool fast = ldcg(&st->fast) != 0;
   const int phase = ldcg(&st->phase);
+  const double drift_b = ldcg(&st->drift_b);
   __syncthreads();
 
   const int n = P.n, m = P.m;
@@ -310,23 +337,27 @@ __device__ __forceinline__ void row_block(const BcdProb* __restrict__ probs,
     const TM* __restrict__ Mrow = M + (size_t)row * m;
     // stream through the ring when the segment holds at least two chunks
     const bool use_ring = staged && vec_ok && (c1 - c0) * (int)sizeof(TM) >= 2 * kRingBytes;
-    const bool first = (t == 0);  // the first pass also flags NaN exponents
-    if (use_ring) {
-      if (first && fast)
-        row_segment_staged<TM, true, true>(Mrow, betas, s2, c0, c1, lane, tab, ring, mx, s);
-      else if (first)
-        row_segment_staged<TM, false, true>(Mrow, betas, s2, c0, c1, lane, tab, ring, mx, s);
-      else if (fast)
-        row_segment_staged<TM, true, false>(Mrow, betas, s2, c0, c1, lane, tab, ring, mx, s);
-      else
-        row_segment_staged<TM, false, false>(Mrow, betas, s2, c0, c1, lane, tab, ring, mx, s);
-    } else if (first) {
-      if (fast) row_segment<TM, true, true>(Mrow, betas, s2, c0, c1, lane, vec_ok, tab, mx, s);
-      else row_segment<TM, false, true>(Mrow, betas, s2, c0, c1, lane, vec_ok, tab, mx, s);
-    } else if (fast) {
-      row_segment<TM, true, false>(Mrow, betas, s2, c0, c1, lane, vec_ok, tab, mx, s);
+    // Mode: the first pass also flags NaN exponents (online maximum); later
+    // passes sum relative to the row's previous LSE, log2 a_i - alphas^t_i,
+    // when the column duals moved by less than kShiftDrift since it was taken.
+    int mode = 1;
+    if (t == 0) {
+      mode = 0;
+    } else if (!online && drift_b < kShiftDrift) {
+      const double sh = rint(P.loga[row] * kLog2e - alphas_cur[row]);
+      if (fabs(sh) < 1.0e6) {
+        mx = sh;
+        mode = 2;
+      }
+    }
+    if (fast) {
+      if (mode == 0) row_any<TM, true, true, false>(use_ring, Mrow, betas, s2, c0, c1, lane, vec_ok, tab, pf, ring, mx, s);
+      else if (mode == 1) row_any<TM, true, false, false>(use_ring, Mrow, betas, s2, c0, c1, lane, vec_ok, tab, pf, ring, mx, s);
+      else row_any<TM, true, false, true>(use_ring, Mrow, betas, s2, c0, c1, lane, vec_ok, tab, pf, ring, mx, s);
     } else {
-      row_segment<TM, false, false>(Mrow, betas, s2, c0, c1, lane, vec_ok, tab, mx, s);
+      if (mode == 0) row_any<TM, false, true, false>(use_ring, Mrow, betas, s2, c0, c1, lane, vec_ok, tab, pf, ring, mx, s);
+      else if (mode == 1) row_any<TM, false, false, false>(use_ring, Mrow, betas, s2, c0, c1, lane, vec_ok, tab, pf, ring, mx, s);
+      else row_any<TM, false, false, true>(use_ring, Mrow, betas, s2, c0, c1, lane, vec_ok, tab, pf, ring, mx, s);
     }
   }
   if (ring.failed && lane == 0) {
@@ -386,8 +417,17 @@ __device__ __forceinline__ void row_block(const BcdProb* __restrict__ probs,
     out[1] = mean;
     out[2] = m2;
     out[3] = acc;
+    // largest |alphas change| of the CTA's rows (NaN orders above +inf)
+    unsigned long long dbits = 0ull;
+    for (int q = 0; q < R; ++q)
+      if (cta * R + q < n) {
+        const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(sm_v[q][1] * s2));
+        dbits = b > dbits ? b : dbits;
+      }
+    atomicMax(&st->acc_a, dbits);
   }
   if (!elect_last(&P.counters[0], (unsigned)P.row_ctas)) return;
+  if (threadIdx.x == 0) st->drift_a = __longlong_as_double((long long)atomicExch(&st->acc_a, 0ull));
 
   // Last CTA of the row pass.
   if (phase == 1) {
@@ -450,13 +490,17 @@ __device__ __forceinline__ void row_block(const BcdProb* __restrict__ probs,
 // ---------------------------------------------------------------------------
 // Column pass: beta^{t+1}_j = eta * (log b_j - LSE_i((alpha^{t+1}_i - M_ij)/eta))
 // ---------------------------------------------------------------------------
-template <typename TM, bool FAST>
+// pf > 0: lanes 0..U-1 also send the strip segments of the rows pf steps
+// ahead to L2 (one bulk hint of strip_bytes per row, from column strip_c0).
+template <typename TM, bool FAST, bool SHIFT>
 __device__ __forceinline__ void col_rows(const TM* __restrict__ M, const double* __restrict__ alphas,
                                          double s2, int m, int jb, int r0, int r1, int warp,
-                                         bool vec_ok, const double* tab, double* mx, double* s) {
+                                         bool vec_ok, const double* tab, int pf, int strip_c0,
+                                         int strip_bytes, double* mx, double* s) {
   constexpr int VN = Vec<TM>::N;
   constexpr int U = (VN == 4) ? 2 : 4;  // 8 elements per lane per step
   constexpr int rstep = kWarps * U;
+  const int lane = threadIdx.x & 31;
   if (vec_ok) {
     using RT = typename Raw<TM>::T;
     int i0 = r0 + warp;
@@ -465,7 +509,16 @@ __device__ __forceinline__ void col_rows(const TM* __restrict__ M, const double*
 #pragma unroll
       for (int u = 0; u < U; ++u) nxt[u] = Raw<TM>::load(M + (size_t)(i0 + u * kWarps) * m + jb);
     }
+    if (pf > 0 && lane < U)
+      for (int k = 2; k < pf; ++k) {
+        const int i = i0 + k * rstep + lane * kWarps;
+        if (i < r1) prefetch_l2_bulk(M + (size_t)i * m + strip_c0, (uint32_t)strip_bytes);
+      }
     for (; i0 + (U - 1) * kWarps < r1; i0 += rstep) {
+      if (pf > 0 && lane < U) {
+        const int i = i0 + pf * rstep + lane * kWarps;
+        if (i < r1) prefetch_l2_bulk(M + (size_t)i * m + strip_c0, (uint32_t)strip_bytes);
+      }
       RT cur[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) cur[u] = nxt[u];
@@ -482,7 +535,7 @@ __device__ __forceinline__ void col_rows(const TM* __restrict__ M, const double*
         double d[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) d[u] = fma(-Raw<TM>::get(cur[u], k), s2, ai[u]);
-        lse_chunk_full<FAST, U>(d, mx[k], s[k], tab);
+        lse_chunk_full<FAST, U, SHIFT>(d, mx[k], s[k], tab);
       }
     }
     // remaining rows of this warp (fewer than U)
@@ -494,7 +547,7 @@ __device__ __forceinline__ void col_rows(const TM* __restrict__ M, const double*
       for (int k = 0; k < VN; ++k) {
         double d[1] = {fma(-mv[k], s2, ai)};
         bool ok[1] = {true};
-        lse_chunk<FAST, 1>(d, ok, mx[k], s[k], tab);
+        lse_chunk<FAST, 1, SHIFT>(d, ok, mx[k], s[k], tab);
       }
     }
   } else {
@@ -506,7 +559,7 @@ __device__ __forceinline__ void col_rows(const TM* __restrict__ M, const double*
         double d[1];
         bool ok[1] = {jb + k < m};
         d[0] = ok[0] ? fma(-ld1(p + k), s2, ai) : kNegInf;
-        lse_chunk<FAST, 1>(d, ok, mx[k], s[k], tab);
+        lse_chunk<FAST, 1, SHIFT>(d, ok, mx[k], s[k], tab);
       }
     }
   }
@@ -519,7 +572,7 @@ __device__ __forceinline__ void col_rows(const TM* __restrict__ M, const double*
 // same (mx, s).  The remaining rows (fewer than U) are read as in col_rows.
 // lane_in: this lane's columns exist (the last strip may be partial);
 // strip_bytes: bytes of the strip in one row.
-template <typename TM, bool FAST>
+template <typename TM, bool FAST, bool SHIFT>
 __device__ __forceinline__ void col_rows_staged(const TM* __restrict__ M,
                                                 const double* __restrict__ alphas, double s2,
                                                 int m, int strip_c0, int strip_bytes, int jb,
@@ -570,7 +623,7 @@ __device__ __forceinline__ void col_rows_staged(const TM* __restrict__ M,
           double d[U];
 #pragma unroll
           for (int u = 0; u < U; ++u) d[u] = fma(-Raw<TM>::get(cur[u], kk), s2, ai[u]);
-          lse_chunk_full<FAST, U>(d, mx[kk], s[kk], tab);
+          lse_chunk_full<FAST, U, SHIFT>(d, mx[kk], s[kk], tab);
         }
       }
     }
@@ -593,7 +646,7 @@ __device__ __forceinline__ void col_rows_staged(const TM* __restrict__ M,
     for (int kk = 0; kk < VN; ++kk) {
       double d[1] = {fma(-mv[kk], s2, ai)};
       bool ok[1] = {true};
-      lse_chunk<FAST, 1>(d, ok, mx[kk], s[kk], tab);
+      lse_chunk<FAST, 1, SHIFT>(d, ok, mx[kk], s[kk], tab);
     }
   }
 }
@@ -603,7 +656,10 @@ template <typename TM>
 __device__ __forceinline__ void col_block(const BcdProb* __restrict__ probs,
                                           const int* __restrict__ cta_prob,
                                           const int* __restrict__ cta_start, int vb,
-                                          bool staged, WarpRing& ring) {
+                                          int flags, WarpRing& ring) {
+  const bool staged = (flags & kPassStaged) != 0;
+  const bool online = (flags & kPassOnline) != 0;
+  const int pf = flags >> kPassPrefetchShift;
   constexpr int VN = Vec<TM>::N;
   constexpr int W = 32 * VN;
   constexpr int G = kThreads / W;  // merge groups per column
@@ -622,6 +678,7 @@ __device__ __forceinline__ void col_block(const BcdProb* __restrict__ probs,
   const int t = ldcg(&st->iter);
   const bool fast = ldcg(&st->fast) != 0;
   const int phase = ldcg(&st->phase);
+  const double drift_a = ldcg(&st->drift_a);
   __syncthreads();
 
   const int n = P.n, m = P.m;
@@ -637,33 +694,64 @@ __device__ __forceinline__ void col_block(const BcdProb* __restrict__ probs,
   const int jb = strip * W + lane * VN;
   const bool vec_ok = (m % VN) == 0 && (reinterpret_cast<uintptr_t>(M) % 16) == 0;
 
+  // Mode: from the second pass on, each column sums relative to its previous
+  // LSE, log2 b_j - betas^t_j, when the row duals of this iteration moved by
+  // less than kShiftDrift; the CTA takes the online maximum if any of its
+  // columns has no usable shift.
+  const double* __restrict__ betas_cur = P.betas[t & 1];
   double mx[VN], s[VN];
+  bool no_shift = online || !(t >= 1 && drift_a < kShiftDrift);
 #pragma unroll
   for (int k = 0; k < VN; ++k) {
     mx[k] = kNegInf;
     s[k] = 0.0;
+    if (!no_shift && jb + k < m) {
+      const double sh = rint(P.logb[jb + k] * kLog2e - betas_cur[jb + k]);
+      if (fabs(sh) < 1.0e6) mx[k] = sh;
+      else no_shift = true;
+    }
   }
+  const bool shift = !__syncthreads_or(no_shift ? 1 : 0);
+  if (!shift)
+#pragma unroll
+    for (int k = 0; k < VN; ++k) mx[k] = kNegInf;
   // stream through the ring when every warp has at least two chunks of rows
   const bool use_ring = staged && vec_ok && (r1 - r0) >= 2 * kWarps * (kRingBytes / 512);
   if (use_ring) {
     const int strip_c0 = strip * W;
     const int strip_bytes = min(W, m - strip_c0) * (int)sizeof(TM);
-    if (fast)
-      col_rows_staged<TM, true>(M, alphas, s2, m, strip_c0, strip_bytes, jb, jb < m, r0, r1,
-                                warp, lane, tab, ring, mx, s);
+    if (fast && shift)
+      col_rows_staged<TM, true, true>(M, alphas, s2, m, strip_c0, strip_bytes, jb, jb < m, r0,
+                                      r1, warp, lane, tab, ring, mx, s);
+    else if (fast)
+      col_rows_staged<TM, true, false>(M, alphas, s2, m, strip_c0, strip_bytes, jb, jb < m, r0,
+                                       r1, warp, lane, tab, ring, mx, s);
+    else if (shift)
+      col_rows_staged<TM, false, true>(M, alphas, s2, m, strip_c0, strip_bytes, jb, jb < m, r0,
+                                       r1, warp, lane, tab, ring, mx, s);
     else
-      col_rows_staged<TM, false>(M, alphas, s2, m, strip_c0, strip_bytes, jb, jb < m, r0, r1,
-                                 warp, lane, tab, ring, mx, s);
+      col_rows_staged<TM, false, false>(M, alphas, s2, m, strip_c0, strip_bytes, jb, jb < m, r0,
+                                        r1, warp, lane, tab, ring, mx, s);
     if (ring.failed && lane == 0) {
       // a staging wait gave up: the problem ends with an error status
       atomicExch(&st->error, 1);
       atomicExch(&st->done, 1);
     }
   } else if (jb < m) {
-    if (fast)
-      col_rows<TM, true>(M, alphas, s2, m, jb, r0, r1, warp, vec_ok, tab, mx, s);
+    const int strip_c0 = strip * W;
+    const int strip_bytes = min(W, m - strip_c0) * (int)sizeof(TM);
+    if (fast && shift)
+      col_rows<TM, true, true>(M, alphas, s2, m, jb, r0, r1, warp, vec_ok, tab, pf, strip_c0,
+                               strip_bytes, mx, s);
+    else if (fast)
+      col_rows<TM, true, false>(M, alphas, s2, m, jb, r0, r1, warp, vec_ok, tab, pf, strip_c0,
+                                strip_bytes, mx, s);
+    else if (shift)
+      col_rows<TM, false, true>(M, alphas, s2, m, jb, r0, r1, warp, vec_ok, tab, pf, strip_c0,
+                                strip_bytes, mx, s);
     else
-      col_rows<TM, false>(M, alphas, s2, m, jb, r0, r1, warp, vec_ok, tab, mx, s);
+      col_rows<TM, false, false>(M, alphas, s2, m, jb, r0, r1, warp, vec_ok, tab, pf, strip_c0,
+                                 strip_bytes, mx, s);
   }
 #pragma unroll
   for (int k = 0; k < VN; ++k) {
@@ -720,6 +808,16 @@ __device__ __forceinline__ void col_block(const BcdProb* __restrict__ probs,
     P.betas[(t + 1) & 1][j] = b_new * s2;
     db = b_new - P.beta[t & 1][j];
   }
+  {
+    // largest |betas change| of the strip (NaN orders above +inf)
+    unsigned long long b = valid ? (unsigned long long)__double_as_longlong(fabs(db * s2)) : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long x = __shfl_xor_sync(0xffffffffu, b, o);
+      b = x > b ? x : b;
+    }
+    if (lane == 0 && b != 0ull) atomicMax(&st->acc_b, b);
+  }
   if (phase == 1) {
     double sn, smu, sm2;
     cta_stats(db, valid, red, sn, smu, sm2);
@@ -734,6 +832,7 @@ __device__ __forceinline__ void col_block(const BcdProb* __restrict__ probs,
 
   // Last strip finisher: iteration bookkeeping (reference :551-591).
   const int tn = t + 1;
+  if (threadIdx.x == 0) st->drift_b = __longlong_as_double((long long)atomicExch(&st->acc_b, 0ull));
   if (phase == 1) {
     double bn = 0, bmu = 0, bm2 = 0;
     for (int q = threadIdx.x; q < P.col_strips; q += blockDim.x)
@@ -770,23 +869,27 @@ __device__ __forceinline__ void col_block(const BcdProb* __restrict__ probs,
 // the same work, in the same per-block order, leaving SM slots free for
 // latency-bound kernels on other streams.
 // LOOP = false: one virtual CTA per CTA (uncapped launches).
-// staged != 0: long rows / column strips stream through per-warp shared-memory
-// rings filled by bulk copies (dynamic shared memory: kRingDynBytes).
+// flags & kPassStaged: long rows / column strips stream through per-warp
+// shared-memory rings filled by bulk copies (dynamic shared memory:
+// kRingDynBytes; launched with none otherwise, which leaves the SM's L1 to the
+// cached dual vectors).  flags & kPassOnline: every pass takes the running
+// maximum (no shifted sums).  flags >> kPassPrefetchShift: L2 bulk-prefetch
+// distance of the register path, in chunks (0: none).
 template <typename TM, bool LOOP>
 __global__ void __launch_bounds__(kThreads, kBcdMinBlocks) bcd_row_kernel(const BcdProb* __restrict__ probs,
                                                             const int* __restrict__ cta_prob,
                                                             const int* __restrict__ cta_start,
-                                                            int total, int staged) {
+                                                            int total, int flags) {
   extern __shared__ __align__(128) unsigned char ring_smem[];
   __shared__ uint64_t ring_bars[kWarps * kRingStages];
   WarpRing ring;
   rings_init(ring_smem, ring_bars, kWarps, ring);
   if (!LOOP) {
-    row_block<TM>(probs, cta_prob, cta_start, (int)blockIdx.x, staged != 0, ring);
+    row_block<TM>(probs, cta_prob, cta_start, (int)blockIdx.x, flags, ring);
     return;
   }
   for (int vb = blockIdx.x; vb < total; vb += gridDim.x) {
-    row_block<TM>(probs, cta_prob, cta_start, vb, staged != 0, ring);
+    row_block<TM>(probs, cta_prob, cta_start, vb, flags, ring);
     __syncthreads();
   }
 }
@@ -795,17 +898,17 @@ template <typename TM, bool LOOP>
 __global__ void __launch_bounds__(kThreads, kBcdMinBlocks) bcd_col_kernel(const BcdProb* __restrict__ probs,
                                                             const int* __restrict__ cta_prob,
                                                             const int* __restrict__ cta_start,
-                                                            int total, int staged) {
+                                                            int total, int flags) {
   extern __shared__ __align__(128) unsigned char ring_smem[];
   __shared__ uint64_t ring_bars[kWarps * kRingStages];
   WarpRing ring;
   rings_init(ring_smem, ring_bars, kWarps, ring);
   if (!LOOP) {
-    col_block<TM>(probs, cta_prob, cta_start, (int)blockIdx.x, staged != 0, ring);
+    col_block<TM>(probs, cta_prob, cta_start, (int)blockIdx.x, flags, ring);
     return;
   }
   for (int vb = blockIdx.x; vb < total; vb += gridDim.x) {
-    col_block<TM>(probs, cta_prob, cta_start, vb, staged != 0, ring);
+    col_block<TM>(probs, cta_prob, cta_start, vb, flags, ring);
     __syncthreads();
   }
 }
@@ -827,6 +930,8 @@ __global__ void plan_kernel(const TM* __restrict__ M, const double* __restrict__
 namespace {
 constexpr int kRingDynBytes = kWarps * kRingStages * kRingBytes;
 std::atomic<int> g_staged{0};
+std::atomic<int> g_l2pf{0};
+std::atomic<int> g_online{0};
 std::once_flag g_ring_attr_once;
 
 // Opt the pass kernels into kRingDynBytes of dynamic shared memory (once per
@@ -846,14 +951,26 @@ void set_ring_attributes() {
 }  // namespace
 
 void bcd_set_staging(bool on) { g_staged.store(on ? 1 : 0); }
+void bcd_set_l2_prefetch(int chunks) { g_l2pf.store(std::clamp(chunks, 0, 64)); }
+int bcd_l2_prefetch() { return g_l2pf.load(); }
+void bcd_set_shifted_lse(bool on) { g_online.store(on ? 0 : 1); }
+
+namespace {
+int pass_flags(size_t& dyn_smem) {
+  const int sg = g_staged.load();
+  dyn_smem = sg ? (size_t)kRingDynBytes : 0;
+  return (sg ? kPassStaged : 0) | (g_online.load() ? kPassOnline : 0) |
+         (g_l2pf.load() << kPassPrefetchShift);
+}
+}  // namespace
 
 void launch_bcd_row(bool f32, const BcdProb* d_probs, const int* d_cta_prob,
                     const int* d_cta_start, int total_ctas, cudaStream_t stream, int grid_cap) {
   set_ring_attributes();
   const bool loop = grid_cap > 0 && grid_cap < total_ctas;
   const int grid = loop ? grid_cap : total_ctas;
-  const int sg = g_staged.load();
-  const size_t sm = kRingDynBytes;
+  size_t sm = 0;
+  const int sg = pass_flags(sm);
   if (f32 && loop)
     { bcd_row_kernel<float, true><<<grid, kThreads, sm, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas, sg); cg::count_launch(); }
   else if (f32)
@@ -868,8 +985,8 @@ void launch_bcd_col(bool f32, const BcdProb* d_probs, const int* d_cta_prob,
   set_ring_attributes();
   const bool loop = grid_cap > 0 && grid_cap < total_ctas;
   const int grid = loop ? grid_cap : total_ctas;
-  const int sg = g_staged.load();
-  const size_t sm = kRingDynBytes;
+  size_t sm = 0;
+  const int sg = pass_flags(sm);
   if (f32 && loop)
     { bcd_col_kernel<float, true><<<grid, kThreads, sm, stream>>>(d_probs, d_cta_prob, d_cta_start, total_ctas, sg); cg::count_launch(); }
   else if (f32)

@@ -29,6 +29,14 @@ struct BcdState {
   int nonfinite;      // a stop-test value was NaN / Inf (non-finite M, a, b or x0): done
   int error;          // a bounded device wait gave up (staging ring): done
   int pad_;
+  // Largest dual change, in base-2 exponent units, of the latest row pass
+  // (max_i |alphas^{t+1}_i - alphas^t_i|) and column pass; +inf until known.
+  // The next pass of the other side sums relative to the previous LSE of its
+  // row / column when this bound is below kShiftDrift.
+  double drift_a;
+  double drift_b;
+  unsigned long long acc_a;  // running maxima (bit patterns of non-negative doubles)
+  unsigned long long acc_b;
 };
 
 struct BcdProb {
@@ -71,6 +79,20 @@ void launch_plan(const TM* M, const double* alpha, const double* beta, double* P
 // filled by bulk copies (process-wide; default off, measured slower on B200).  Off: every pass reads M
 // with vector loads straight into registers.  Same results either way.
 void bcd_set_staging(bool on);
+// L2 bulk-prefetch distance (chunks ahead) of the register-path passes; 0 off.
+void bcd_set_l2_prefetch(int chunks);
+int bcd_l2_prefetch();  // the current distance (also used by the plan pass)
+
+// Shifted LSE sums (default on): passes after the first sum relative to the
+// previous LSE of their row / column when the drift bound allows; off, every
+// pass keeps a running maximum.
+void bcd_set_shifted_lse(bool on);
+
+// Pass kernel flag word: bit 0 staging, bit 1 online maximum only, bits 8..
+// the prefetch distance.
+constexpr int kPassStaged = 1;
+constexpr int kPassOnline = 2;
+constexpr int kPassPrefetchShift = 8;
 
 // Launch geometry for one problem.
 void bcd_geometry(int n, int m, int elem_bytes, int sm_count, BcdProb& p);

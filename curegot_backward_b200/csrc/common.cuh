@@ -286,6 +286,24 @@ __device__ __forceinline__ double exp2_neg_f64(double x, const double* __restric
   return __hiloint2double(__double2hiint(y) + ((N >> kExp2Bits) << 20), __double2loint(y));
 }
 
+// 2^(x - k) for an integer k, inside the LSE passes that sum relative to a
+// fixed shift k instead of a running maximum: the same table method applied
+// to x itself, with k taken off the result's binary exponent (an integer add
+// in place of an FP64 subtraction).  x is first raised to lo = k - 1000, so
+// terms far below the shift come out near 2^-1000 instead of underflowing
+// through the exponent field; the caller guarantees x - k <= 1000.
+__device__ __forceinline__ double exp2_shift_f64(double x, double lo, int k,
+                                                 const double* __restrict__ tab) {
+  x = fmax(x, lo);
+  const double t = fma(x, kExp2Scale, kExpMagic);
+  const int N = __double2loint(t);
+  const double kf = t - kExpMagic;
+  const double f = fma(kf, -kExp2InvScale, x);
+  const double y = exp2_poly(f) * tab[N & (kExp2TableSize - 1)];
+  return __hiloint2double(__double2hiint(y) + (((N >> kExp2Bits) - k) << 20),
+                          __double2loint(y));
+}
+
 // Hardware 2^x on the SFU (ex2.approx.ftz.f32).
 __device__ __forceinline__ float ex2_approx(float x) {
   float y;

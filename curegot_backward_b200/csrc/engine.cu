@@ -144,6 +144,8 @@ __global__ void engine_init_kernel(const double* a, const double* b, int n, int 
     st->fast_iters = 0;
     st->nonfinite = 0;
     st->error = 0;
+    st->drift_a = st->drift_b = INFINITY;
+    st->acc_a = st->acc_b = 0ull;
   }
 }
 
@@ -630,7 +632,7 @@ void splr_loop(cg_engine_s* E, int slots) {
     // meets tol on rows and on all m columns (the reference's test leaves
     // the gauge column out)
     SplrParams prm{r.eta, r.tol, r.max_iter, std::min(10.0 / std::min(n, m), 1.0), 1e-3, 30, 3,
-                   0, 1, &j->q->cancel};
+                   0, 1, 1, &j->q->cancel};
     if (r.m_f32)
       j->task = splr_task<float>(&j->io, static_cast<const float*>(dM), da, db, nullptr, n, m,
                                  prm, nullptr, j->ddual, &j->niter, &j->conv, nullptr, nullptr);

@@ -26,10 +26,42 @@ __device__ __forceinline__ void lse2_merge(double& mx, double& s, double mx2, do
   }
 }
 
-// Accumulate K exponents (valid ones only) into the running (mx, s).
+// Shifted accumulation: with SHIFT the pair (mx, s) holds a fixed integer
+// shift mx chosen before the pass (the previous iteration's LSE of the same
+// row or column) and s += sum_q 2^(d_q - mx), with no running maximum.  The
+// caller guarantees every exponent d_q - mx <= kShiftDrift (the LSE moved by
+// at most the largest dual change of the other side since that LSE was
+// taken), so no term overflows in FP32 or FP64.
+constexpr double kShiftDrift = 40.0;
+
 template <bool FAST, int K>
+__device__ __forceinline__ void lse_shift_terms(const double (&d)[K], const bool* ok, double mx,
+                                                double& s, const double* tab) {
+  if (FAST) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int q = 0; q < K; ++q)
+      if (ok == nullptr || ok[q]) acc += exp2_neg_mixed(d[q] - mx);
+    s += static_cast<double>(acc);
+  } else {
+    const int k = static_cast<int>(mx);
+    const double lo = mx - 1000.0;
+    double acc = 0.0;
+#pragma unroll
+    for (int q = 0; q < K; ++q)
+      if (ok == nullptr || ok[q]) acc += exp2_shift_f64(d[q], lo, k, tab);
+    s += acc;
+  }
+}
+
+// Accumulate K exponents (valid ones only) into the running (mx, s).
+template <bool FAST, int K, bool SHIFT = false>
 __device__ __forceinline__ void lse_chunk(const double (&d)[K], const bool (&ok)[K], double& mx,
                                           double& s, const double* tab) {
+  if (SHIFT) {
+    lse_shift_terms<FAST, K>(d, ok, mx, s, tab);
+    return;
+  }
   double cmax = kNegInf;
 #pragma unroll
   for (int q = 0; q < K; ++q)
@@ -52,9 +84,13 @@ __device__ __forceinline__ void lse_chunk(const double (&d)[K], const bool (&ok)
 }
 
 // Same, for a chunk known to be fully in range (no predicates).
-template <bool FAST, int K>
+template <bool FAST, int K, bool SHIFT = false>
 __device__ __forceinline__ void lse_chunk_full(const double (&d)[K], double& mx, double& s,
                                                const double* tab) {
+  if (SHIFT) {
+    lse_shift_terms<FAST, K>(d, nullptr, mx, s, tab);
+    return;
+  }
   double cmax = d[0];
 #pragma unroll
   for (int q = 1; q < K; ++q) cmax = fmax(cmax, d[q]);

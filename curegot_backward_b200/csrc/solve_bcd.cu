@@ -310,6 +310,8 @@ __global__ void bcd_init_kernel(const double* __restrict__ a, const double* __re
     st->fast_iters = 0;
     st->nonfinite = 0;
     st->error = 0;
+    st->drift_a = st->drift_b = INFINITY;
+    st->acc_a = st->acc_b = 0ull;
   }
 }
 
@@ -692,6 +694,17 @@ int cg_bcd_f64_noalloc(const double* M, const double* a, const double* b, double
 
 int cg_bcd_set_staging(int enable) {
   cg::bcd_set_staging(enable != 0);
+  return CG_OK;
+}
+
+int cg_bcd_set_shifted_lse(int enable) {
+  cg::bcd_set_shifted_lse(enable != 0);
+  return CG_OK;
+}
+
+int cg_bcd_set_l2_prefetch(int chunks) {
+  if (chunks < 0 || chunks > 64) return CG_ERR_INVALID_ARG;
+  cg::bcd_set_l2_prefetch(chunks);
   return CG_OK;
 }
 

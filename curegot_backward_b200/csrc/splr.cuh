@@ -36,6 +36,11 @@ struct SplrParams {
   // marginal error ||(T1 - a, T^T 1 - b)||_2 < tol, which adds the gauge
   // column's error (the serving engine's per-result accuracy guarantee).
   int full_stop = 0;
+  // with full_stop: once the reference's test passes, also accept the point
+  // whose gauge column m - 1 is made exact (beta_{m-1} moved, then the gauge
+  // shifted back) when that gives a full marginal error below tol; the
+  // returned duals then carry the correction.  Without a context only.
+  int gauge_fix = 0;
   // set by another thread to stop the solve at the next iteration with
   // CG_ERR_CANCELLED (the serving engine's request cancellation); may be null
   const std::atomic<bool>* cancel = nullptr;

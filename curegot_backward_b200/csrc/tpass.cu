@@ -18,6 +18,8 @@
 // overflow gives +inf and NaN propagates, as the reference's exp() does.
 #include <algorithm>
 
+#include "bcd.cuh"
+#include "bulk.cuh"
 #include "tpass.cuh"
 
 namespace cg {
@@ -114,7 +116,20 @@ __global__ void __launch_bounds__(kThreads, (K == 1) ? 3 : 2) tpass_kernel(const
 #pragma unroll
     for (int q = 0; q < NV * VN; ++q) cacc[p][q] = 0.0;
 
+  // L2 prefetch (lane 0, one bulk hint per row segment) of the warp's rows
+  // pf steps ahead, when the segments are 16-byte aligned
+  const int pf = vec_ok ? A.l2pf : 0;
+  const uint32_t seg_bytes = (uint32_t)(min(kTStrip, m - c0) * (int)sizeof(TM));
+  if (pf > 0 && lane == 0)
+    for (int k = 1; k < pf; ++k) {
+      const int ip = r0 + warp + k * kWarps;
+      if (ip < r1) prefetch_l2_bulk(M + (size_t)ip * m + c0, seg_bytes);
+    }
   for (int i = r0 + warp; i < r1; i += kWarps) {
+    if (pf > 0 && lane == 0) {
+      const int ip = i + pf * kWarps;
+      if (ip < r1) prefetch_l2_bulk(M + (size_t)ip * m + c0, seg_bytes);
+    }
     double as[K], rsum[K];
 #pragma unroll
     for (int p = 0; p < K; ++p) {
@@ -273,7 +288,9 @@ size_t tpass_workspace_doubles(int n, int m, int strips, int splits) {
   return (size_t)strips * n + (size_t)splits * m + (size_t)(splits + strips) * kTScal;
 }
 
-int launch_tpass(bool f32, const TPassArgs& a, cudaStream_t stream) {
+int launch_tpass(bool f32, const TPassArgs& a_in, cudaStream_t stream) {
+  TPassArgs a = a_in;
+  a.l2pf = bcd_l2_prefetch();
   const int grid = a.strips * a.splits;
   const bool multi = a.trial && a.nsteps > 1;
   if (f32 && multi)

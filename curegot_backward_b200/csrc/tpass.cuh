@@ -47,6 +47,7 @@ struct TPassArgs {
   double* colpart;         // [splits * m]
   double* scal;            // [(splits + strips) * kTScal]
   unsigned int* counters;  // [splits + strips + 1], zero-initialised
+  int l2pf;                // L2 prefetch distance in row steps (set by launch_tpass)
 };
 
 constexpr int kTStrip = 256;  // columns per strip

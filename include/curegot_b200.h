@@ -127,6 +127,31 @@ int cg_bcd_set_cluster_path(int enable);
 int cg_bcd_set_staging(int enable);
 
 /*
+ * Shifted log-sum-exp in the Sinkhorn row / column passes (default on).  The
+ * first pass of a solve keeps a running maximum per row / column.  Later
+ * passes sum 2^(x - k) with k the previous LSE of the same row (column),
+ * recovered from the current dual, whenever the other side's duals moved by
+ * less than 40 (base-2 exponent units) since: every term is then at most
+ * 2^41 and the sum at least 2^-41, so no maximum is needed.  This removes
+ * the per-element maximum and shift from the passes.  Results agree with the
+ * running-maximum passes to rounding (a few ulp per LSE).  enable = 0 keeps
+ * the running maximum in every pass.  Process-wide; captured engine graphs
+ * keep the setting they were captured with.  No reference counterpart.
+ */
+int cg_bcd_set_shifted_lse(int enable);
+
+/*
+ * L2 prefetch distance of the Sinkhorn row / column passes (register path),
+ * in chunks of one warp's loop step (0 = off, at most 64; default below in
+ * the implementation).  Each warp sends a bulk L2 prefetch hint for the chunk
+ * `chunks` steps ahead of the one it reads, so more of M is in flight than
+ * the registers hold.  A hint only: results are bitwise identical for every
+ * setting.  Process-wide; the serving engine's captured batch graphs keep the
+ * setting they were captured with.  No reference counterpart.
+ */
+int cg_bcd_set_l2_prefetch(int chunks);
+
+/*
  * Mixed-precision BCD: M stored in FP32, duals and all reductions in FP64.
  * Same contract as cg_bcd_f64; P (nullable) is written in FP64.  The
  * FP32-M form of cuda_sinkhorn_bcd; the stopping rule is evaluated with the

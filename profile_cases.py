@@ -86,7 +86,7 @@ def case_bcd(a):
     bytes_ = 2.0 * a.n * a.m * M.element_size() * niter
     gbs = bytes_ / (ms / 1e3) / 1e9
     peak, kind = _peak()
-    return {"case": "bcd", "path": a.path, "staging": a.staging, "n": a.n, "m": a.m,
+    return {"case": "bcd", "path": a.path, "staging": a.staging, "l2pf": a.l2pf, "lse": a.lse, "n": a.n, "m": a.m,
             "precision": a.precision, "eta": a.eta,
             "iterations": niter, "ms_per_solve": ms, "us_per_iteration": 1e3 * ms / niter,
             "algorithmic_GBps": gbs, "peak_GBps": peak, "peak_kind": kind, "frac": gbs / peak}
@@ -152,7 +152,7 @@ def case_splr(a):
     run = lambda: cg.torch.sinkhorn_splr(M, am, bm, a.eta, tol=a.tol, max_iter=1000,
                                          precision=a.precision, **kw)
     ms, out = _time(run, a.reps)
-    return {"case": "splr", "n": a.n, "m": a.m, "precision": a.precision, "eta": a.eta,
+    return {"case": "splr", "l2pf": a.l2pf, "n": a.n, "m": a.m, "precision": a.precision, "eta": a.eta,
             "density": a.density, "iterations": out["niter"], "ms_per_solve": ms,
             "direction_solver": cg.last_direction_solver()}
 
@@ -317,7 +317,10 @@ def main(argv=None):
     p.add_argument("--path", default="auto", choices=["auto", "multi"],
                    help="bcd: auto = cluster-resident solver when the problem fits")
     p.add_argument("--density", type=float, default=None, help="splr: density_max kwarg")
-    p.add_argument("--staging", default="on", choices=["on", "off"],
+    p.add_argument("--l2pf", type=int, default=None, help="L2 prefetch distance of the Sinkhorn and plan passes")
+    p.add_argument("--lse", default="shifted", choices=["shifted", "online"],
+                   help="Sinkhorn passes: shifted sums or running maximum in every pass")
+    p.add_argument("--staging", default="off", choices=["on", "off"],
                    help="bcd: shared-memory staging of the passes")
     p.add_argument("--solver", default=None, choices=[None, "auto", "dense", "peel", "sparse"])
     p.add_argument("--tol", type=float, default=1e-8)
@@ -332,6 +335,10 @@ def main(argv=None):
     p.add_argument("--compare", action="store_true", help="points: also time the stored cost")
     p.add_argument("--batch", type=int, default=16, help="batch case: problems per batch")
     a = p.parse_args(argv)
+    import curegot_backward_b200 as cg
+    if a.l2pf is not None:
+        cg.set_bcd_l2_prefetch(a.l2pf)
+    cg.set_bcd_shifted_lse(a.lse == "shifted")
     res = {"bcd": case_bcd, "splr": case_splr, "backward": case_backward,
            "precision": case_precision, "points": case_points, "batch": case_batch,
            "c0": case_c0}[a.case](a)

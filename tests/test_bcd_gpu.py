@@ -229,3 +229,46 @@ def test_staged_passes_are_bitwise_the_unstaged_ones(cuda_dev, precision, n, m):
         cg.set_bcd_staging(False)  # the library default
     assert out[True][0] == out[False][0]
     assert torch.equal(out[True][2], out[False][2])
+
+
+@pytest.mark.parametrize("precision,n,m,eta", [("fp64", 1500, 4096, 0.02), ("fp64", 700, 5003, 0.01),
+                                               ("mixed", 2300, 8192, 0.02), ("fp64", 4000, 300, 0.01)])
+def test_shifted_lse_agrees_with_running_maximum(cuda_dev, precision, n, m, eta):
+    """Passes that sum relative to the previous LSE (no running maximum)
+    against passes that keep the running maximum in every pass: same
+    iteration count, duals within rounding, and both against the oracle's
+    marginal bar.  At these eta the first iterations move the duals by more
+    than the drift bound (|d beta| log2(e) / eta > 40), so both modes occur
+    within one solve."""
+    import torch
+    from curegot_backward_b200 import _solvers
+    g = torch.Generator(device=cuda_dev).manual_seed(3 * n + m)
+    X = torch.randn(n, 8, generator=g, device=cuda_dev, dtype=torch.float64)
+    Y = torch.randn(m, 8, generator=g, device=cuda_dev, dtype=torch.float64)
+    M = torch.cdist(X, Y) ** 2
+    M = M / M.max()
+    if precision == "mixed":
+        M = M.float()
+    a = torch.rand(n, generator=g, device=cuda_dev, dtype=torch.float64) + 0.5
+    b = torch.rand(m, generator=g, device=cuda_dev, dtype=torch.float64) + 0.5
+    a, b = a / a.sum(), b / b.sum()
+    out = {}
+    try:
+        for on in (True, False):
+            cg.set_bcd_shifted_lse(on)
+            out[on] = _solvers._bcd_device(M, a, b, eta, 1e-8, 5000, None, precision,
+                                           want_plan=False)
+    finally:
+        cg.set_bcd_shifted_lse(True)  # the library default
+    assert out[True][0] < 5000
+    if precision == "fp64":
+        assert out[True][0] == out[False][0]
+    else:  # the SFU passes decide only when FP64 passes take over
+        assert abs(out[True][0] - out[False][0]) <= 2
+    d1, d0 = out[True][2], out[False][2]
+    assert (d1 - d0).abs().max().item() <= 1e-9 * d0.abs().max().item()
+    # the marginal error of the shifted result, in FP64
+    Md = M.double()
+    P = torch.exp((d1[:n, None] + d1[None, n:] - Md) / eta)
+    err = torch.sqrt(((P.sum(1) - a) ** 2).sum()).item()
+    assert err < 1e-8
