@@ -48,7 +48,7 @@ METRIC = "solves/s + p99 latency, mixed-size OT stream @1e-8 marginal err, vs pl
 TOL = 1e-8
 WORKLOAD = ("serving stream: n,m log-uniform [64,8192], d in {8,32}, Gaussian clouds/max, "
             "eta in {0.1,0.05,0.01}, 70% BCD / 30% SPLR, tol 1e-8, uniform marginals")
-SPLR_WORKERS = 16
+SPLR_WORKERS = 32
 IN_FLIGHT = 24
 
 
@@ -585,7 +585,8 @@ def main():
                                     f"saturation: closed loop over the timed steps' {n_req} requests, "
                                     f"{args.in_flight} in flight"),
                        "l2": "inputs larger than L2 (each step streams > 126 MB of M)",
-                       "engine": f"max_batch 64, {args.splr_workers} SPLR workers, 8 ticks per graph launch",
+                       "engine": f"max_batch 64, up to {args.splr_workers} SPLR solves in flight on "
+                                 f"{(args.splr_workers + 7) // 8} scheduler threads, 8 ticks per graph launch",
                        "parallelism": f"replicas x{world}"},
             "latency_ms": {"p50": float(np.percentile(lat, 50)),
                            "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},

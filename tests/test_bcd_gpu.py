@@ -261,12 +261,15 @@ def test_shifted_lse_agrees_with_running_maximum(cuda_dev, precision, n, m, eta)
     finally:
         cg.set_bcd_shifted_lse(True)  # the library default
     assert out[True][0] < 5000
+    d1, d0 = out[True][2], out[False][2]
     if precision == "fp64":
         assert out[True][0] == out[False][0]
-    else:  # the SFU passes decide only when FP64 passes take over
+        assert (d1 - d0).abs().max().item() <= 1e-9 * d0.abs().max().item()
+    else:
+        # the SFU passes only decide when FP64 passes take over, so the two
+        # solves may stop at neighbouring iterates, both within tol
         assert abs(out[True][0] - out[False][0]) <= 2
-    d1, d0 = out[True][2], out[False][2]
-    assert (d1 - d0).abs().max().item() <= 1e-9 * d0.abs().max().item()
+        assert (d1 - d0).abs().max().item() <= 1e-6 * d0.abs().max().item()
     # the marginal error of the shifted result, in FP64
     Md = M.double()
     P = torch.exp((d1[:n, None] + d1[None, n:] - Md) / eta)
