@@ -62,11 +62,49 @@ __device__ __forceinline__ void prefetch_row_chunk(const TM* Mrow, int pos, int 
 // CHECK (first pass of a solve): a NaN exponent (NaN in M or the duals) makes
 // the row's sum NaN.  Without it a NaN entry would drop out of the sum like
 // an infinite cost: the exponent clamp of the exponential ignores NaN.
-template <typename TM, bool FAST, bool CHECK, bool SHIFT>
+// Float-pair form of a row chunk (FP32 M, SFU, shifted): U float4 vectors of
+// M and their columns' (hi, lo) beta pairs at bp + u * step; k = the row's
+// shift, s2 = s2h + s2l.  Same grouping as the FP64-argument chunk: one FP32
+// partial per chunk, added to s.
+template <int U>
+__device__ __forceinline__ void split_chunk_row(const float4 (&mv)[U], const float2* __restrict__ bp,
+                                                int step, float k, float s2h, float s2l,
+                                                double& s) {
+  float acc = 0.0f;
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    const float4 b01 = *reinterpret_cast<const float4*>(bp + u * step);
+    const float4 b23 = *reinterpret_cast<const float4*>(bp + u * step + 2);
+    acc += split_term(mv[u].x, b01.x, b01.y, k, s2h, s2l);
+    acc += split_term(mv[u].y, b01.z, b01.w, k, s2h, s2l);
+    acc += split_term(mv[u].z, b23.x, b23.y, k, s2h, s2l);
+    acc += split_term(mv[u].w, b23.z, b23.w, k, s2h, s2l);
+  }
+  s += static_cast<double>(acc);
+}
+
+// Float pair (hi, lo) of a scaled dual; false when |v| >= kSplitMax or v is
+// not finite (the pair is then unusable).
+__device__ __forceinline__ bool split_of(double v, float2& out) {
+  if (!(fabs(v) < kSplitMax)) {
+    out = make_float2(0.0f, 0.0f);
+    return false;
+  }
+  const double hi = rint(v * 512.0) * (1.0 / 512.0);
+  out = make_float2(static_cast<float>(hi), static_cast<float>(v - hi));
+  return true;
+}
+
+// SPLIT (FP32 M, FAST and SHIFT only): the full vector chunks take their
+// exponents from the float-pair betas bsplit (split_chunk_row); the tail
+// keeps the FP64-argument form.
+template <typename TM, bool FAST, bool CHECK, bool SHIFT, bool SPLIT = false>
 __device__ __forceinline__ void row_segment(const TM* __restrict__ Mrow,
                                             const double* __restrict__ betas, double s2, int c0,
                                             int c1, int lane, bool vec_ok, const double* tab,
-                                            int pf, double& mx, double& s) {
+                                            int pf, double& mx, double& s,
+                                            const float2* __restrict__ bsplit = nullptr,
+                                            float s2h = 0.0f, float s2l = 0.0f) {
   bool bad = false;
   constexpr int VN = Vec<TM>::N;
   if (vec_ok) {
@@ -93,18 +131,23 @@ __device__ __forceinline__ void row_segment(const TM* __restrict__ Mrow,
 #pragma unroll
         for (int u = 0; u < U; ++u) nxt[u] = Raw<TM>::load(Mrow + cb + span + lane * VN + u * step);
       }
-      double d[U * VN];
+      if constexpr (SPLIT) {
+        split_chunk_row<U>(cur, bsplit + cb + lane * VN, step, static_cast<float>(mx), s2h, s2l,
+                           s);
+      } else {
+        double d[U * VN];
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        double bv[VN];
-        ld_duals<VN>(betas + cb + lane * VN + u * step, bv);
+        for (int u = 0; u < U; ++u) {
+          double bv[VN];
+          ld_duals<VN>(betas + cb + lane * VN + u * step, bv);
 #pragma unroll
-        for (int k = 0; k < VN; ++k) d[u * VN + k] = fma(-Raw<TM>::get(cur[u], k), s2, bv[k]);
+          for (int k = 0; k < VN; ++k) d[u * VN + k] = fma(-Raw<TM>::get(cur[u], k), s2, bv[k]);
+        }
+        if (CHECK)
+#pragma unroll
+          for (int q = 0; q < U * VN; ++q) bad |= (d[q] != d[q]);
+        lse_chunk_full<FAST, U * VN, SHIFT>(d, mx, s, tab);
       }
-      if (CHECK)
-#pragma unroll
-        for (int q = 0; q < U * VN; ++q) bad |= (d[q] != d[q]);
-      lse_chunk_full<FAST, U * VN, SHIFT>(d, mx, s, tab);
     }
     // tail (vectors that are in range, then nothing: c1 is a multiple of VN)
     for (int j = cb + lane * VN; j < c1; j += step) {
@@ -149,11 +192,13 @@ __device__ __forceinline__ void row_segment(const TM* __restrict__ Mrow,
 // span is processed exactly like row_segment's loop body -- same grouping,
 // same order, bitwise the same (mx, s).  The tail (< one span) is read as in
 // row_segment.  A ring wait that gives up leaves ring.failed set.
-template <typename TM, bool FAST, bool CHECK, bool SHIFT>
+template <typename TM, bool FAST, bool CHECK, bool SHIFT, bool SPLIT = false>
 __device__ __forceinline__ void row_segment_staged(const TM* __restrict__ Mrow,
                                                    const double* __restrict__ betas, double s2,
                                                    int c0, int c1, int lane, const double* tab,
-                                                   WarpRing& ring, double& mx, double& s) {
+                                                   WarpRing& ring, double& mx, double& s,
+                                                   const float2* __restrict__ bsplit = nullptr,
+                                                   float s2h = 0.0f, float s2l = 0.0f) {
   bool bad = false;
   constexpr int VN = Vec<TM>::N;
   constexpr int U = RowU<TM>::U;
@@ -186,19 +231,26 @@ __device__ __forceinline__ void row_segment_staged(const TM* __restrict__ Mrow,
     const int sp0 = k * SPC, nsp = min(SPC, nspans - sp0);
     for (int q = 0; q < nsp; ++q) {
       const int cb = c0 + (sp0 + q) * span;
-      double d[U * VN];
+      if constexpr (SPLIT) {
+        RT v[U];
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const RT v = chunk[q * (span / VN) + u * 32 + lane];
-        double bv[VN];
-        ld_duals<VN>(betas + cb + lane * VN + u * step, bv);
+        for (int u = 0; u < U; ++u) v[u] = chunk[q * (span / VN) + u * 32 + lane];
+        split_chunk_row<U>(v, bsplit + cb + lane * VN, step, static_cast<float>(mx), s2h, s2l, s);
+      } else {
+        double d[U * VN];
 #pragma unroll
-        for (int kk = 0; kk < VN; ++kk) d[u * VN + kk] = fma(-Raw<TM>::get(v, kk), s2, bv[kk]);
+        for (int u = 0; u < U; ++u) {
+          const RT v = chunk[q * (span / VN) + u * 32 + lane];
+          double bv[VN];
+          ld_duals<VN>(betas + cb + lane * VN + u * step, bv);
+#pragma unroll
+          for (int kk = 0; kk < VN; ++kk) d[u * VN + kk] = fma(-Raw<TM>::get(v, kk), s2, bv[kk]);
+        }
+        if (CHECK)
+#pragma unroll
+          for (int q = 0; q < U * VN; ++q) bad |= (d[q] != d[q]);
+        lse_chunk_full<FAST, U * VN, SHIFT>(d, mx, s, tab);
       }
-      if (CHECK)
-#pragma unroll
-        for (int q = 0; q < U * VN; ++q) bad |= (d[q] != d[q]);
-      lse_chunk_full<FAST, U * VN, SHIFT>(d, mx, s, tab);
     }
     ring.consumed++;
     __syncwarp();
@@ -269,15 +321,19 @@ __device__ __forceinline__ void cta_stats(double v, bool valid, double* red, dou
 }
 }  // namespace
 
-template <typename TM, bool FAST, bool CHECK, bool SHIFT>
+template <typename TM, bool FAST, bool CHECK, bool SHIFT, bool SPLIT = false>
 __device__ __forceinline__ void row_any(bool use_ring, const TM* __restrict__ Mrow,
                                         const double* __restrict__ betas, double s2, int c0,
                                         int c1, int lane, bool vec_ok, const double* tab, int pf,
-                                        WarpRing& ring, double& mx, double& s) {
+                                        WarpRing& ring, double& mx, double& s,
+                                        const float2* __restrict__ bsplit = nullptr,
+                                        float s2h = 0.0f, float s2l = 0.0f) {
   if (use_ring)
-    row_segment_staged<TM, FAST, CHECK, SHIFT>(Mrow, betas, s2, c0, c1, lane, tab, ring, mx, s);
+    row_segment_staged<TM, FAST, CHECK, SHIFT, SPLIT>(Mrow, betas, s2, c0, c1, lane, tab, ring,
+                                                      mx, s, bsplit, s2h, s2l);
   else
-    row_segment<TM, FAST, CHECK, SHIFT>(Mrow, betas, s2, c0, c1, lane, vec_ok, tab, pf, mx, s);
+    row_segment<TM, FAST, CHECK, SHIFT, SPLIT>(Mrow, betas, s2, c0, c1, lane, vec_ok, tab, pf,
+                                               mx, s, bsplit, s2h, s2l);
 }
 
 // ---------------------------------------------------------------------------
@@ -309,6 +365,7 @@ __device__ __forceinline__ void row_block(const BcdProb* __restrict__ probs,
   const bool fast = ldcg(&st->fast) != 0;
   const int phase = ldcg(&st->phase);
   const double drift_b = ldcg(&st->drift_b);
+  const bool split_ok = P.bsplit != nullptr && ldcg(&st->split_bad_b) == 0;
   __syncthreads();
 
   const int n = P.n, m = P.m;
@@ -317,6 +374,8 @@ __device__ __forceinline__ void row_block(const BcdProb* __restrict__ probs,
   const double* __restrict__ alphas_cur = P.alphas[t & 1];
   const double* __restrict__ alpha_cur = P.alpha[t & 1];
   const double s2 = P.s2;
+  const float s2h = static_cast<float>(s2);
+  const float s2l = static_cast<float>(s2 - static_cast<double>(s2h));
 
   const int R = P.rows_per_cta;
   const int wpr = kWarps / R;
@@ -340,6 +399,8 @@ __device__ __forceinline__ void row_block(const BcdProb* __restrict__ probs,
     // Mode: the first pass also flags NaN exponents (online maximum); later
     // passes sum relative to the row's previous LSE, log2 a_i - alphas^t_i,
     // when the column duals moved by less than kShiftDrift since it was taken.
+    // With FP32 M, SFU passes and float-pair betas in range, the shifted
+    // exponents are formed in FP32 from the pairs (mode 3).
     int mode = 1;
     if (t == 0) {
       mode = 0;
@@ -348,12 +409,14 @@ __device__ __forceinline__ void row_block(const BcdProb* __restrict__ probs,
       if (fabs(sh) < 1.0e6) {
         mx = sh;
         mode = 2;
+        if (sizeof(TM) == 4 && fast && split_ok && fabs(sh) < kSplitMax) mode = 3;
       }
     }
     if (fast) {
       if (mode == 0) row_any<TM, true, true, false>(use_ring, Mrow, betas, s2, c0, c1, lane, vec_ok, tab, pf, ring, mx, s);
       else if (mode == 1) row_any<TM, true, false, false>(use_ring, Mrow, betas, s2, c0, c1, lane, vec_ok, tab, pf, ring, mx, s);
-      else row_any<TM, true, false, true>(use_ring, Mrow, betas, s2, c0, c1, lane, vec_ok, tab, pf, ring, mx, s);
+      else if (mode == 2) row_any<TM, true, false, true>(use_ring, Mrow, betas, s2, c0, c1, lane, vec_ok, tab, pf, ring, mx, s);
+      else row_any<TM, true, false, true, sizeof(TM) == 4>(use_ring, Mrow, betas, s2, c0, c1, lane, vec_ok, tab, pf, ring, mx, s, P.bsplit, s2h, s2l);
     } else {
       if (mode == 0) row_any<TM, false, true, false>(use_ring, Mrow, betas, s2, c0, c1, lane, vec_ok, tab, pf, ring, mx, s);
       else if (mode == 1) row_any<TM, false, false, false>(use_ring, Mrow, betas, s2, c0, c1, lane, vec_ok, tab, pf, ring, mx, s);
@@ -385,6 +448,7 @@ __device__ __forceinline__ void row_block(const BcdProb* __restrict__ probs,
       const double as_new = a_new * s2;
       P.alpha[(t + 1) & 1][row] = a_new;
       P.alphas[(t + 1) & 1][row] = as_new;
+      if (P.asplit != nullptr && !split_of(as_new, P.asplit[row])) atomicOr(&st->split_bad_a, 1);
       if (check) {
         const double ai = P.a[row];
         const double e = ai * exp2_f64(alphas_cur[row] - as_new, tab) - ai;
@@ -427,7 +491,10 @@ __device__ __forceinline__ void row_block(const BcdProb* __restrict__ probs,
     atomicMax(&st->acc_a, dbits);
   }
   if (!elect_last(&P.counters[0], (unsigned)P.row_ctas)) return;
-  if (threadIdx.x == 0) st->drift_a = __longlong_as_double((long long)atomicExch(&st->acc_a, 0ull));
+  if (threadIdx.x == 0) {
+    st->drift_a = __longlong_as_double((long long)atomicExch(&st->acc_a, 0ull));
+    st->split_bad_b = 0;  // every CTA of this pass has read it
+  }
 
   // Last CTA of the row pass.
   if (phase == 1) {
@@ -492,11 +559,36 @@ __device__ __forceinline__ void row_block(const BcdProb* __restrict__ probs,
 // ---------------------------------------------------------------------------
 // pf > 0: lanes 0..U-1 also send the strip segments of the rows pf steps
 // ahead to L2 (one bulk hint of strip_bytes per row, from column strip_c0).
-template <typename TM, bool FAST, bool SHIFT>
+// Float-pair form of a column group (FP32 M, SFU, shifted): U rows' float4
+// vectors, the rows' (hi, lo) alpha pairs, this lane's column shifts k[].
+// Same grouping as the FP64-argument group: per column one FP32 partial over
+// the U rows, added to s[column].
+template <int U>
+__device__ __forceinline__ void split_group_col(const float4 (&mv)[U], const float2 (&ap)[U],
+                                                const float (&k)[4], float s2h, float s2l,
+                                                double* s) {
+  float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    acc[0] += split_term(mv[u].x, ap[u].x, ap[u].y, k[0], s2h, s2l);
+    acc[1] += split_term(mv[u].y, ap[u].x, ap[u].y, k[1], s2h, s2l);
+    acc[2] += split_term(mv[u].z, ap[u].x, ap[u].y, k[2], s2h, s2l);
+    acc[3] += split_term(mv[u].w, ap[u].x, ap[u].y, k[3], s2h, s2l);
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) s[q] += static_cast<double>(acc[q]);
+}
+
+// SPLIT (FP32 M, FAST and SHIFT only): the full row groups take their
+// exponents from the float-pair alphas asplit (split_group_col); the
+// remaining rows keep the FP64-argument form.
+template <typename TM, bool FAST, bool SHIFT, bool SPLIT = false>
 __device__ __forceinline__ void col_rows(const TM* __restrict__ M, const double* __restrict__ alphas,
                                          double s2, int m, int jb, int r0, int r1, int warp,
                                          bool vec_ok, const double* tab, int pf, int strip_c0,
-                                         int strip_bytes, double* mx, double* s) {
+                                         int strip_bytes, double* mx, double* s,
+                                         const float2* __restrict__ asplit = nullptr,
+                                         float s2h = 0.0f, float s2l = 0.0f) {
   constexpr int VN = Vec<TM>::N;
   constexpr int U = (VN == 4) ? 2 : 4;  // 8 elements per lane per step
   constexpr int rstep = kWarps * U;
@@ -527,15 +619,24 @@ __device__ __forceinline__ void col_rows(const TM* __restrict__ M, const double*
         for (int u = 0; u < U; ++u)
           nxt[u] = Raw<TM>::load(M + (size_t)(i0 + rstep + u * kWarps) * m + jb);
       }
-      double ai[U];
+      if constexpr (SPLIT) {
+        float2 ap[U];
 #pragma unroll
-      for (int u = 0; u < U; ++u) ai[u] = alphas[i0 + u * kWarps];
+        for (int u = 0; u < U; ++u) ap[u] = asplit[i0 + u * kWarps];
+        const float kf[4] = {static_cast<float>(mx[0]), static_cast<float>(mx[1]),
+                             static_cast<float>(mx[2]), static_cast<float>(mx[3])};
+        split_group_col<U>(cur, ap, kf, s2h, s2l, s);
+      } else {
+        double ai[U];
 #pragma unroll
-      for (int k = 0; k < VN; ++k) {
-        double d[U];
+        for (int u = 0; u < U; ++u) ai[u] = alphas[i0 + u * kWarps];
 #pragma unroll
-        for (int u = 0; u < U; ++u) d[u] = fma(-Raw<TM>::get(cur[u], k), s2, ai[u]);
-        lse_chunk_full<FAST, U, SHIFT>(d, mx[k], s[k], tab);
+        for (int k = 0; k < VN; ++k) {
+          double d[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) d[u] = fma(-Raw<TM>::get(cur[u], k), s2, ai[u]);
+          lse_chunk_full<FAST, U, SHIFT>(d, mx[k], s[k], tab);
+        }
       }
     }
     // remaining rows of this warp (fewer than U)
@@ -572,13 +673,14 @@ __device__ __forceinline__ void col_rows(const TM* __restrict__ M, const double*
 // same (mx, s).  The remaining rows (fewer than U) are read as in col_rows.
 // lane_in: this lane's columns exist (the last strip may be partial);
 // strip_bytes: bytes of the strip in one row.
-template <typename TM, bool FAST, bool SHIFT>
+template <typename TM, bool FAST, bool SHIFT, bool SPLIT = false>
 __device__ __forceinline__ void col_rows_staged(const TM* __restrict__ M,
                                                 const double* __restrict__ alphas, double s2,
                                                 int m, int strip_c0, int strip_bytes, int jb,
                                                 bool lane_in, int r0, int r1, int warp, int lane,
                                                 const double* tab, WarpRing& ring, double* mx,
-                                                double* s) {
+                                                double* s, const float2* __restrict__ asplit = nullptr,
+                                                float s2h = 0.0f, float s2l = 0.0f) {
   constexpr int VN = Vec<TM>::N;
   constexpr int U = (VN == 4) ? 2 : 4;
   constexpr int RPC = kRingBytes / 512;  // warp rows per ring chunk
@@ -612,18 +714,26 @@ __device__ __forceinline__ void col_rows_staged(const TM* __restrict__ M,
     if (lane_in) {
       for (int qg = 0; qg < nq; qg += U) {
         RT cur[U];
-        double ai[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-          cur[u] = reinterpret_cast<const RT*>(chunk + (qg + u) * 512)[lane];
-          ai[u] = alphas[i_first + (q0 + qg + u) * kWarps];
-        }
+        for (int u = 0; u < U; ++u) cur[u] = reinterpret_cast<const RT*>(chunk + (qg + u) * 512)[lane];
+        if constexpr (SPLIT) {
+          float2 ap[U];
 #pragma unroll
-        for (int kk = 0; kk < VN; ++kk) {
-          double d[U];
+          for (int u = 0; u < U; ++u) ap[u] = asplit[i_first + (q0 + qg + u) * kWarps];
+          const float kf[4] = {static_cast<float>(mx[0]), static_cast<float>(mx[1]),
+                               static_cast<float>(mx[2]), static_cast<float>(mx[3])};
+          split_group_col<U>(cur, ap, kf, s2h, s2l, s);
+        } else {
+          double ai[U];
 #pragma unroll
-          for (int u = 0; u < U; ++u) d[u] = fma(-Raw<TM>::get(cur[u], kk), s2, ai[u]);
-          lse_chunk_full<FAST, U, SHIFT>(d, mx[kk], s[kk], tab);
+          for (int u = 0; u < U; ++u) ai[u] = alphas[i_first + (q0 + qg + u) * kWarps];
+#pragma unroll
+          for (int kk = 0; kk < VN; ++kk) {
+            double d[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) d[u] = fma(-Raw<TM>::get(cur[u], kk), s2, ai[u]);
+            lse_chunk_full<FAST, U, SHIFT>(d, mx[kk], s[kk], tab);
+          }
         }
       }
     }
@@ -679,6 +789,7 @@ __device__ __forceinline__ void col_block(const BcdProb* __restrict__ probs,
   const bool fast = ldcg(&st->fast) != 0;
   const int phase = ldcg(&st->phase);
   const double drift_a = ldcg(&st->drift_a);
+  const bool split_a_ok = P.asplit != nullptr && ldcg(&st->split_bad_a) == 0;
   __syncthreads();
 
   const int n = P.n, m = P.m;
@@ -715,12 +826,27 @@ __device__ __forceinline__ void col_block(const BcdProb* __restrict__ probs,
   if (!shift)
 #pragma unroll
     for (int k = 0; k < VN; ++k) mx[k] = kNegInf;
+  // FP32 M with SFU passes: exponents from the float-pair alphas when they
+  // and every column shift of the CTA are in range
+  bool fsplit = false;
+  if (sizeof(TM) == 4 && fast && shift && split_a_ok) {
+    bool bad = false;
+#pragma unroll
+    for (int k = 0; k < VN; ++k) bad |= (jb + k < m) && !(fabs(mx[k]) < kSplitMax);
+    fsplit = !__syncthreads_or(bad ? 1 : 0);
+  }
+  const float s2h = static_cast<float>(s2);
+  const float s2l = static_cast<float>(s2 - static_cast<double>(s2h));
   // stream through the ring when every warp has at least two chunks of rows
   const bool use_ring = staged && vec_ok && (r1 - r0) >= 2 * kWarps * (kRingBytes / 512);
   if (use_ring) {
     const int strip_c0 = strip * W;
     const int strip_bytes = min(W, m - strip_c0) * (int)sizeof(TM);
-    if (fast && shift)
+    if (fast && fsplit)
+      col_rows_staged<TM, true, true, sizeof(TM) == 4>(M, alphas, s2, m, strip_c0, strip_bytes,
+                                                       jb, jb < m, r0, r1, warp, lane, tab, ring,
+                                                       mx, s, P.asplit, s2h, s2l);
+    else if (fast && shift)
       col_rows_staged<TM, true, true>(M, alphas, s2, m, strip_c0, strip_bytes, jb, jb < m, r0,
                                       r1, warp, lane, tab, ring, mx, s);
     else if (fast)
@@ -740,7 +866,11 @@ __device__ __forceinline__ void col_block(const BcdProb* __restrict__ probs,
   } else if (jb < m) {
     const int strip_c0 = strip * W;
     const int strip_bytes = min(W, m - strip_c0) * (int)sizeof(TM);
-    if (fast && shift)
+    if (fast && fsplit)
+      col_rows<TM, true, true, sizeof(TM) == 4>(M, alphas, s2, m, jb, r0, r1, warp, vec_ok, tab,
+                                                pf, strip_c0, strip_bytes, mx, s, P.asplit, s2h,
+                                                s2l);
+    else if (fast && shift)
       col_rows<TM, true, true>(M, alphas, s2, m, jb, r0, r1, warp, vec_ok, tab, pf, strip_c0,
                                strip_bytes, mx, s);
     else if (fast)
@@ -806,6 +936,7 @@ __device__ __forceinline__ void col_block(const BcdProb* __restrict__ probs,
     const double b_new = P.eta * P.logb[j] - (P.eta * kLn2) * (Mc + log2(Sc));
     P.beta[(t + 1) & 1][j] = b_new;
     P.betas[(t + 1) & 1][j] = b_new * s2;
+    if (P.bsplit != nullptr && !split_of(b_new * s2, P.bsplit[j])) atomicOr(&st->split_bad_b, 1);
     db = b_new - P.beta[t & 1][j];
   }
   {
@@ -832,7 +963,10 @@ __device__ __forceinline__ void col_block(const BcdProb* __restrict__ probs,
 
   // Last strip finisher: iteration bookkeeping (reference :551-591).
   const int tn = t + 1;
-  if (threadIdx.x == 0) st->drift_b = __longlong_as_double((long long)atomicExch(&st->acc_b, 0ull));
+  if (threadIdx.x == 0) {
+    st->drift_b = __longlong_as_double((long long)atomicExch(&st->acc_b, 0ull));
+    st->split_bad_a = 0;  // every CTA of this pass has read it
+  }
   if (phase == 1) {
     double bn = 0, bmu = 0, bm2 = 0;
     for (int q = threadIdx.x; q < P.col_strips; q += blockDim.x)

@@ -37,7 +37,17 @@ struct BcdState {
   double drift_b;
   unsigned long long acc_a;  // running maxima (bit patterns of non-negative doubles)
   unsigned long long acc_b;
+  // The float-pair copies of the latest scaled duals (BcdProb asplit /
+  // bsplit) are out of range (|value| >= kSplitMax) or absent: set by the
+  // pass that writes them, cleared by the last CTA of the pass that reads them.
+  int split_bad_a;
+  int split_bad_b;
 };
+
+// Float-pair duals for the mixed-precision shifted passes: v = hi + lo with hi
+// a multiple of 2^-9 (exact in FP32 for |v| < kSplitMax) and lo the FP32
+// rounding of the remainder.
+constexpr double kSplitMax = 16384.0;
 
 struct BcdProb {
   const void* M;        // row-major n x m (float or double, fixed per launch)
@@ -61,6 +71,10 @@ struct BcdProb {
   double* col_part;     // [col_strips * 3] stats partials
   unsigned int* counters;  // [2 + col_strips], zero-initialised
   BcdState* st;
+  // float-pair copies of the latest alphas / betas (FP32-M problems; null
+  // otherwise): the SFU passes form exponents from them in FP32
+  float2* asplit;       // [n]
+  float2* bsplit;       // [m]
 };
 
 // total_ctas virtual CTAs; grid_cap > 0 limits the launched grid (the

@@ -93,7 +93,7 @@ size_t bcd_footprint(const cg_request_t& r, BcdProb& geo, int sms) {
   size_t b = 0;
   if (r.host_inputs) b += align256((size_t)n * m * es) + align256(8 * (size_t)(n + m));
   b += align256(8 * (size_t)(n + m));          // dual out (device)
-  b += 2 * align256(8 * (size_t)n) + 2 * align256(8 * (size_t)m);  // loga logb (+ spare)
+  b += 2 * align256(8 * (size_t)n) + 2 * align256(8 * (size_t)m);  // loga logb, float-pair duals
   b += 4 * align256(8 * (size_t)n) + 4 * align256(8 * (size_t)m);  // alpha/beta (scaled) x2
   const size_t parts = geo.col_splits > 1 ? (size_t)geo.col_splits * m : 1;
   b += 2 * align256(8 * parts);
@@ -146,6 +146,7 @@ __global__ void engine_init_kernel(const double* a, const double* b, int n, int 
     st->error = 0;
     st->drift_a = st->drift_b = INFINITY;
     st->acc_a = st->acc_b = 0ull;
+    st->split_bad_a = st->split_bad_b = 0;
   }
 }
 
@@ -241,9 +242,9 @@ int bcd_admit(cg_engine_s* E, Req* q, cudaStream_t st) {
   }
   q->ddual = reinterpret_cast<double*>(take(8 * (size_t)(n + m)));
   double* loga = reinterpret_cast<double*>(take(8 * (size_t)n));
-  take(8 * (size_t)n);
+  float2* asplit = reinterpret_cast<float2*>(take(8 * (size_t)n));
   double* logb = reinterpret_cast<double*>(take(8 * (size_t)m));
-  take(8 * (size_t)m);
+  float2* bsplit = reinterpret_cast<float2*>(take(8 * (size_t)m));
   for (int k = 0; k < 2; ++k) {
     P.alpha[k] = reinterpret_cast<double*>(take(8 * (size_t)n));
     P.alphas[k] = reinterpret_cast<double*>(take(8 * (size_t)n));
@@ -257,6 +258,8 @@ int bcd_admit(cg_engine_s* E, Req* q, cudaStream_t st) {
   P.col_part = reinterpret_cast<double*>(take(8 * (size_t)P.col_strips * 3));
   P.counters = reinterpret_cast<unsigned int*>(take(4 * (size_t)(2 + P.col_strips)));
   P.st = reinterpret_cast<BcdState*>(take(sizeof(BcdState)));
+  P.asplit = r.m_f32 ? asplit : nullptr;
+  P.bsplit = r.m_f32 ? bsplit : nullptr;
   P.M = q->dM;
   P.n = n;
   P.m = m;

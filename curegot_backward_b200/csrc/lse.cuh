@@ -54,6 +54,22 @@ __device__ __forceinline__ void lse_shift_terms(const double (&d)[K], const bool
   }
 }
 
+// One term of the mixed-precision shifted sum from float-pair duals:
+// 2^(v - k - s2 M) with v = hi + lo, s2 = s2h + s2l (FP32 pairs) and the
+// integer shift k.  t = hi - k is exact (hi a multiple of 2^-9, |hi|, |k| <
+// 2^14); fmaf(-s2h, M, t) is t - s2h M rounded once; the low parts add
+// lo - s2l M.  The exponent is within 2^-18 of the FP64 value when it is
+// at most 64 in magnitude (the terms that matter), the same order as the
+// FP32 rounding the FP64-argument form applies.  No FP64 work and no
+// conversions: one SFU operation per element.
+__device__ __forceinline__ float split_term(float m, float hi, float lo, float k, float s2h,
+                                            float s2l) {
+  const float t = __fsub_rn(hi, k);
+  const float u = fmaf(-s2h, m, t);
+  const float c = fmaf(-s2l, m, lo);
+  return ex2_approx(__fadd_rn(u, c));
+}
+
 // Accumulate K exponents (valid ones only) into the running (mx, s).
 template <bool FAST, int K, bool SHIFT = false>
 __device__ __forceinline__ void lse_chunk(const double (&d)[K], const bool (&ok)[K], double& mx,

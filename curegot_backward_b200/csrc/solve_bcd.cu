@@ -312,6 +312,7 @@ __global__ void bcd_init_kernel(const double* __restrict__ a, const double* __re
     st->error = 0;
     st->drift_a = st->drift_b = INFINITY;
     st->acc_a = st->acc_b = 0ull;
+    st->split_bad_a = st->split_bad_b = 0;
   }
 }
 
@@ -427,6 +428,8 @@ int bcd_solve(const TM* M, const double* a, const double* b, double* Pout, doubl
   const size_t o_cnt = ws.reserve<unsigned int>(ncount);
   const size_t o_st = ws.reserve<BcdState>(1);
   const size_t o_prob = ws.reserve<BcdProb>(1);
+  const bool split = sizeof(TM) == 4;  // float-pair duals for the SFU passes
+  const size_t o_asp = ws.reserve<float2>(split ? n : 1), o_bsp = ws.reserve<float2>(split ? m : 1);
   CG_TRY(ws.allocate());
 
   hp.M = M;
@@ -449,6 +452,8 @@ int bcd_solve(const TM* M, const double* a, const double* b, double* Pout, doubl
   hp.col_part = ws.at<double>(o_cp);
   hp.counters = ws.at<unsigned int>(o_cnt);
   hp.st = ws.at<BcdState>(o_st);
+  hp.asplit = split ? ws.at<float2>(o_asp) : nullptr;
+  hp.bsplit = split ? ws.at<float2>(o_bsp) : nullptr;
   BcdProb* dprob = ws.at<BcdProb>(o_prob);
 
   const bool f32 = sizeof(TM) == 4;

@@ -206,6 +206,7 @@ __global__ void bcd_seed_kernel(const double* beta_src, int zero, double* beta0,
     st->error = 0;
     st->drift_a = st->drift_b = INFINITY;
     st->acc_a = st->acc_b = 0ull;
+    st->split_bad_a = st->split_bad_b = 0;
   }
 }
 
