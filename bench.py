@@ -396,6 +396,7 @@ def cpu_sample(specs, get_problem, budget_s, seed=0):
         return time.perf_counter() - t
 
     first = int(np.argmin(cost))
+    solve(first)  # untimed: thread-pool start-up and first touches stay out of the calibration
     t_first = solve(first)
     sec_per_cost = t_first / max(cost[first], 1.0)
     # water-filling: sum_i min(c_i, lam) * sec_per_cost = remaining budget

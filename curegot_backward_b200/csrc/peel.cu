@@ -15,7 +15,7 @@
 //   the result is deterministic), one CTA per Schur row assembles the core
 //   Schur complement, cuSOLVER potrf factors it.  The solve is a forward
 //   sweep over the rounds, potrs on the core, and a backward sweep.
-// Small cores (kc <= kPeelSmallCore = 160, 200 KB of shared memory for the
+// Small cores (kc <= kPeelSmallCore = 160, 204 KB of shared memory for the
 //   dense core factor): the whole factorization and solve run in
 //   ONE single-CTA kernel -- pivots and forward values in the same rounds,
 //   the core Schur complement assembled and Cholesky-factored in shared
@@ -260,26 +260,30 @@ __device__ void dev_core_rhs(const double* __restrict__ val, const PeelPtrs& p,
   __syncthreads();
 }
 
-// z <- (L L^T)^{-1} z for nrhs columns; L lower, row-major kc x kc (shared).
-// One warp per right-hand side: the column sweeps synchronise with
-// __syncwarp only (the block-wide version paid two __syncthreads per column).
-// Every z entry receives its updates in the same order as a column sweep.
-__device__ void dev_trisolve(const double* __restrict__ L, int kc, double* __restrict__ z,
+// Row stride of the in-shared-memory core matrix: odd, so that a warp reading
+// one column (consecutive rows) touches distinct bank pairs.
+__host__ __device__ __forceinline__ int core_ld(int kc) { return kc | 1; }
+
+// z <- (L L^T)^{-1} z for nrhs columns; L lower, row-major kc x kc with row
+// stride ld (shared).  One warp per right-hand side: the column sweeps
+// synchronise with __syncwarp only.  Every z entry receives its updates in
+// the same order as a column sweep.
+__device__ void dev_trisolve(const double* __restrict__ L, int kc, int ld, double* __restrict__ z,
                              int nrhs) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp < nrhs) {
     double* zc = z + (size_t)warp * kc;
     for (int j = 0; j < kc; ++j) {
-      const double zj = zc[j] / L[j * kc + j];
+      const double zj = zc[j] / L[j * ld + j];
       __syncwarp();
-      for (int i = j + 1 + lane; i < kc; i += 32) zc[i] = fma(-L[i * kc + j], zj, zc[i]);
+      for (int i = j + 1 + lane; i < kc; i += 32) zc[i] = fma(-L[i * ld + j], zj, zc[i]);
       if (lane == 0) zc[j] = zj;
       __syncwarp();
     }
     for (int j = kc - 1; j >= 0; --j) {
-      const double zj = zc[j] / L[j * kc + j];
+      const double zj = zc[j] / L[j * ld + j];
       __syncwarp();
-      for (int i = lane; i < j; i += 32) zc[i] = fma(-L[j * kc + i], zj, zc[i]);
+      for (int i = lane; i < j; i += 32) zc[i] = fma(-L[j * ld + i], zj, zc[i]);
       if (lane == 0) zc[j] = zj;
       __syncwarp();
     }
@@ -287,60 +291,84 @@ __device__ void dev_trisolve(const double* __restrict__ L, int kc, double* __res
   __syncthreads();
 }
 
-// In-place Cholesky S = L L^T of the lower triangle (row-major kc x kc,
-// shared), one __syncthreads per column.  Step j applies column j's rank-1
-// update to the trailing lower triangle and, in the same sweep, finishes
-// column c = j+1: every thread recomputes that column's pivot
-// d = S[c][c] - L[c][j]^2 itself (the same fma as a plain right-looking
-// sweep), so the column can be scaled by 1/sqrt(d) without a second barrier.
-// The diagonal entry is read by every thread during the sweep, so it is
-// stored (as sqrt(d)) at the start of the next sweep.  A pivot that is not
-// positive and finite sets info = column + 1 and continues with d = 1.
-__device__ void dev_cholesky(double* __restrict__ S, int kc, int* __restrict__ info) {
-  double d0 = S[0];
-  if (!(d0 > 0.0) || !isfinite(d0)) {
-    if (threadIdx.x == 0) info[0] = 1;
-    d0 = 1.0;
-  }
-  double lj = sqrt(d0);  // L[j][j] of the column finished last
-  for (int i = 1 + threadIdx.x; i < kc; i += blockDim.x) S[i * kc] = S[i * kc] / lj;
-  __syncthreads();
-  for (int j = 0; j + 1 < kc; ++j) {
-    if (threadIdx.x == 0) S[j * kc + j] = lj;  // nobody reads it in this sweep
-    const int c = j + 1;
-    const double lcj = S[c * kc + j];
-    double dc = fma(-lcj, lcj, S[c * kc + c]);
-    if (!(dc > 0.0) || !isfinite(dc)) {
-      if (threadIdx.x == 0) info[0] = c + 1;
-      dc = 1.0;
-    }
-    const double lc = sqrt(dc);
-    // lower triangle of the trailing block without its first diagonal entry:
-    // rows i = c..kc-1, columns k = c..i; rows ii and w-1-ii share one index
-    // range of length w+1
-    const int w = kc - c;
-    const int total = ((w + 1) >> 1) * (w + 1);
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-      const int pr = e / (w + 1), q = e - pr * (w + 1);
-      int ii, kk;
-      if (q <= pr) {
-        ii = pr;
-        kk = q;
-      } else {
-        ii = w - 1 - pr;
-        kk = q - pr - 1;
-        if (ii == pr) continue;  // odd w: the middle row is covered by q <= pr
+// In-place Cholesky S = L L^T of the lower triangle (row-major kc x kc, row
+// stride ld, shared), blocked by panels of 32 columns, three block barriers
+// per panel:
+//   1. the 32 x 32 diagonal block, by warp 0 alone (lane r owns row r of the
+//      block; a right-looking sweep with __syncwarp between columns);
+//   2. the panel below it, L21 = S21 L11^{-T}: each thread solves whole rows
+//      by forward substitution along the panel's columns;
+//   3. the trailing update S22 -= L21 L21^T on the lower triangle: a work
+//      item is one column c of a 4-row tile (rows i0..i0+3, c <= i), its
+//      four dot products over the panel accumulated in registers.
+// A pivot that is not positive and finite sets info = column + 1 and
+// continues with d = 1 (the last such column is reported).
+__device__ void dev_cholesky(double* __restrict__ S, int kc, int ld, int* __restrict__ info) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int j0 = 0; j0 < kc; j0 += 32) {
+    const int bw = min(32, kc - j0);
+    if (warp == 0) {
+      double* Sr = S + (size_t)(j0 + lane) * ld + j0;  // this lane's block row
+      for (int k = 0; k < bw; ++k) {
+        double d = S[(size_t)(j0 + k) * ld + j0 + k];
+        if (!(d > 0.0) || !isfinite(d)) {
+          if (lane == 0) info[0] = j0 + k + 1;
+          d = 1.0;
+        }
+        const double lkk = sqrt(d);
+        double lrk = 0.0;
+        if (lane > k && lane < bw) {
+          lrk = Sr[k] / lkk;
+          Sr[k] = lrk;
+        }
+        __syncwarp();
+        if (lane == k) Sr[k] = lkk;
+        if (lane > k && lane < bw)
+          for (int c = k + 1; c <= lane; ++c)
+            Sr[c] = fma(-lrk, S[(size_t)(j0 + c) * ld + j0 + k], Sr[c]);
+        __syncwarp();
       }
-      if (ii == 0) continue;  // S[c][c]: stored next sweep
-      const int i = c + ii, k = c + kk;
-      const double v = fma(-S[i * kc + j], S[k * kc + j], S[i * kc + k]);
-      S[i * kc + k] = (kk == 0) ? v / lc : v;
     }
-    lj = lc;
+    __syncthreads();
+    const int r0 = j0 + bw;  // first row below the block
+    for (int i = r0 + threadIdx.x; i < kc; i += blockDim.x) {
+      double* Si = S + (size_t)i * ld + j0;
+      for (int k = 0; k < bw; ++k) {
+        const double v = Si[k] / S[(size_t)(j0 + k) * ld + j0 + k];
+        Si[k] = v;
+        for (int c = k + 1; c < bw; ++c) Si[c] = fma(-v, S[(size_t)(j0 + c) * ld + j0 + k], Si[c]);
+      }
+    }
+    __syncthreads();
+    const int w = kc - r0;
+    if (w > 0) {
+      // items: row tile ti (rows r0 + 4 ti .. + 3) has 4 (ti + 1) columns
+      // c = r0 .. r0 + 4 ti + 3; items before tile ti: 2 ti (ti + 1)
+      const int nt = (w + 3) >> 2;
+      const int items = 2 * nt * (nt + 1);
+      for (int e = threadIdx.x; e < items; e += blockDim.x) {
+        int ti = (int)((sqrt(2.0 * e + 1.0) - 1.0) * 0.5);
+        while (2 * (ti + 1) * (ti + 2) <= e) ++ti;
+        while (2 * ti * (ti + 1) > e) --ti;
+        const int c = r0 + (e - 2 * ti * (ti + 1));
+        const int i0 = r0 + 4 * ti;
+        if (c >= kc) continue;
+        const double* Sc = S + (size_t)c * ld + j0;
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        const int nr = min(4, kc - i0);
+        for (int k = 0; k < bw; ++k) {
+          const double b = Sc[k];
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+            if (r < nr) acc[r] = fma(S[(size_t)(i0 + r) * ld + j0 + k], b, acc[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+          if (r < nr && c <= i0 + r) S[(size_t)(i0 + r) * ld + c] -= acc[r];
+      }
+    }
     __syncthreads();
   }
-  if (threadIdx.x == 0) S[(kc - 1) * kc + (kc - 1)] = lj;
-  __syncthreads();
 }
 
 // Core back-substitution from the Schur-side solution zc, then the backward
@@ -376,15 +404,17 @@ __device__ void dev_backward(const double* __restrict__ val, const PeelPtrs& p, 
 }
 
 // Factorization (pivots d, core factor L -> Lout) and, for nrhs > 0, the
-// solve x = A^{-1} rhs.  Dynamic shared memory: kc*kc + 2*kc doubles.
+// solve x = A^{-1} rhs.  Dynamic shared memory: kc*ld + 2*kc doubles (ld =
+// core_ld(kc), the shared row stride of the core matrix).
 __global__ void __launch_bounds__(kPeelThreads) peel_fused_kernel(
     const double* __restrict__ val, PeelPtrs p, int rounds, int kc, int ke, int H,
     const double* __restrict__ rhs, int nrhs, double* __restrict__ x, double* __restrict__ d,
     double* __restrict__ y, double* __restrict__ Lout, int* __restrict__ info,
     double* __restrict__ W) {
   extern __shared__ double sm[];
+  const int ld = core_ld(kc);
   double* S = sm;
-  double* z = sm + (size_t)kc * kc;
+  double* z = sm + (size_t)kc * ld;
   // pivots and forward values, round by round (core last)
   for (int r = 0; r <= rounds; ++r) {
     for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
@@ -418,14 +448,14 @@ __global__ void __launch_bounds__(kPeelThreads) peel_fused_kernel(
       const int t = idx / kc, t2 = idx - t * kc;
       double acc = (t == t2) ? d[p.snodes[t]] : 0.0;
       for (int q = p.ccp[idx]; q < p.ccp[idx + 1]; ++q) acc -= W[p.cw[q]] * val[p.cq2[q]];
-      S[idx] = acc;
+      S[(size_t)t * ld + t2] = acc;
     }
     __syncthreads();
   } else if (kc > 0) {
     // core Schur complement, one warp per row (same order as the multi-CTA path)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     for (int t = warp; t < kc; t += nw) {
-      double* Sr = S + (size_t)t * kc;
+      double* Sr = S + (size_t)t * ld;
       for (int c = lane; c < kc; c += 32) Sr[c] = 0.0;
       __syncwarp();
       if (lane == 0) Sr[t] = d[p.snodes[t]];
@@ -441,13 +471,16 @@ __global__ void __launch_bounds__(kPeelThreads) peel_fused_kernel(
     __syncthreads();
   }
   if (kc > 0) {
-    dev_cholesky(S, kc, info);
-    for (int e = threadIdx.x; e < kc * kc; e += blockDim.x) Lout[e] = S[e];
+    dev_cholesky(S, kc, ld, info);
+    for (int e = threadIdx.x; e < kc * kc; e += blockDim.x) {
+      const int t = e / kc;
+      Lout[e] = S[(size_t)t * ld + (e - t * kc)];
+    }
   }
   if (nrhs == 0) return;
   if (kc > 0) {
     dev_core_rhs(val, p, d, y, nrhs, H, kc, z);
-    dev_trisolve(S, kc, z, nrhs);
+    dev_trisolve(S, kc, ld, z, nrhs);
   }
   dev_backward(val, p, rounds, d, y, z, nrhs, H, kc, ke, x);
 }
@@ -458,18 +491,24 @@ __global__ void __launch_bounds__(kPeelThreads) peel_small_solve_kernel(
     const double* __restrict__ rhs, int nrhs, double* __restrict__ x,
     const double* __restrict__ d, double* __restrict__ y, const double* __restrict__ Lin) {
   extern __shared__ double sm[];
+  const int ld = core_ld(kc);
   double* S = sm;
-  double* z = sm + (size_t)kc * kc;
-  for (int e = threadIdx.x; e < kc * kc; e += blockDim.x) S[e] = Lin[e];
+  double* z = sm + (size_t)kc * ld;
+  for (int e = threadIdx.x; e < kc * kc; e += blockDim.x) {
+    const int t = e / kc;
+    S[(size_t)t * ld + (e - t * kc)] = Lin[e];
+  }
   dev_forward(val, p, rounds, d, rhs, nrhs, H, y);  // its round barriers also publish S
   if (kc > 0) {
     dev_core_rhs(val, p, d, y, nrhs, H, kc, z);
-    dev_trisolve(S, kc, z, nrhs);
+    dev_trisolve(S, kc, ld, z, nrhs);
   }
   dev_backward(val, p, rounds, d, y, z, nrhs, H, kc, ke, x);
 }
 
-size_t small_smem(int kc) { return ((size_t)kc * kc + 2 * (size_t)std::max(kc, 1)) * sizeof(double); }
+size_t small_smem(int kc) {
+  return ((size_t)kc * core_ld(kc) + 2 * (size_t)std::max(kc, 1)) * sizeof(double);
+}
 
 int ensure_small_smem() {
   static thread_local int done_dev = -1;
