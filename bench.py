@@ -536,10 +536,15 @@ def main():
         hsteps = [to_host_pinned(p) for p in steps]
         h2d = sum(p[1].numel() * 4 + (p[0].n + p[0].m) * 8 for st in hsteps for p in st)
         d2h = sum((p[0].n + p[0].m) * 8 for st in hsteps for p in st)
-        e_ms, _ = timed_engine_pass(eng, hsteps, True, args.rate, world, args.in_flight)
+        e_ms, e_res = timed_engine_pass(eng, hsteps, True, args.rate, world, args.in_flight)
+        e_lat = np.array([r["latency"] for r in e_res]) * 1000.0
         e2e = {"value": total_req / (e_ms / 1000.0), "unit": "solves/s",
                "h2d_bytes_per_step": int(h2d / max(args.steps, 1)),
-               "d2h_bytes_per_step": int(d2h / max(args.steps, 1))}
+               "d2h_bytes_per_step": int(d2h / max(args.steps, 1)),
+               "latency_ms": {"p50": float(np.percentile(e_lat, 50)),
+                              "p99": float(np.percentile(e_lat, 99))},
+               "all_status_ok": all(r["status"] == 0 for r in e_res),
+               "solves_per_s_by_step": per_step_rates(e_res, args.requests)}
         del hsteps
 
     # plain FP64 path on the same requests (also the FP64 reference solutions)

@@ -213,13 +213,36 @@ void finish(cg_engine_s* E, Req* q) {
   E->cv.notify_all();
 }
 
-// Allocate and initialise a Sinkhorn problem (engine stream).
-int bcd_admit(cg_engine_s* E, Req* q, cudaStream_t st) {
+// Stage a Sinkhorn problem: its device block (stream-ordered on the copy
+// stream cst) and, for host inputs, the copies of M, a and b on cst, with
+// *ev recorded after them (null for device inputs: nothing to wait for).
+// The copies overlap the batch chunks already running on the batch stream.
+int bcd_stage(Req* q, cudaStream_t cst, cudaEvent_t ev_free, cudaEvent_t* ev) {
+  const cg_request_t& r = q->r;
+  *ev = nullptr;
+  CG_TRY(pool_alloc_async(&q->block, q->footprint, cst));
+  if (r.host_inputs) {
+    const int n = r.n, m = r.m;
+    const size_t es = r.m_f32 ? 4 : 8;
+    char* p = static_cast<char*>(q->block);
+    double* dab = reinterpret_cast<double*>(p + align256((size_t)n * m * es));
+    CG_TRY_CUDA(cudaMemcpyAsync(p, r.M, (size_t)n * m * es, cudaMemcpyHostToDevice, cst));
+    CG_TRY_CUDA(cudaMemcpyAsync(dab, r.a, 8 * (size_t)n, cudaMemcpyHostToDevice, cst));
+    CG_TRY_CUDA(cudaMemcpyAsync(dab + n, r.b, 8 * (size_t)m, cudaMemcpyHostToDevice, cst));
+    CG_TRY_CUDA(cudaEventRecord(ev_free, cst));
+    *ev = ev_free;
+  }
+  return CG_OK;
+}
+
+// Initialise a staged Sinkhorn problem on the batch stream st (its copies,
+// if any, have completed or are waited for here).
+int bcd_admit(cg_engine_s* E, Req* q, cudaStream_t st, cudaEvent_t ev) {
   const cg_request_t& r = q->r;
   const int n = r.n, m = r.m;
   const size_t es = r.m_f32 ? 4 : 8;
   BcdProb& P = q->prob;
-  CG_TRY(pool_alloc_async(&q->block, q->footprint, st));
+  if (ev) CG_TRY_CUDA(cudaStreamWaitEvent(st, ev, 0));
   char* p = static_cast<char*>(q->block);
   auto take = [&](size_t bytes) {
     char* x = p;
@@ -229,9 +252,6 @@ int bcd_admit(cg_engine_s* E, Req* q, cudaStream_t st) {
   if (r.host_inputs) {
     void* dM = take((size_t)n * m * es);
     double* dab = reinterpret_cast<double*>(take(8 * (size_t)(n + m)));
-    CG_TRY_CUDA(cudaMemcpyAsync(dM, r.M, (size_t)n * m * es, cudaMemcpyHostToDevice, st));
-    CG_TRY_CUDA(cudaMemcpyAsync(dab, r.a, 8 * (size_t)n, cudaMemcpyHostToDevice, st));
-    CG_TRY_CUDA(cudaMemcpyAsync(dab + n, r.b, 8 * (size_t)m, cudaMemcpyHostToDevice, st));
     q->dM = dM;
     q->da = dab;
     q->db = dab + n;
@@ -290,6 +310,26 @@ void bcd_loop(cg_engine_s* E, int cls) {
   cudaEvent_t ev0, ev1;
   cudaEventCreate(&ev0);
   cudaEventCreate(&ev1);
+  // host-input copies run on their own stream, overlapping the chunks
+  cudaStream_t cst;
+  cudaStreamCreateWithFlags(&cst, cudaStreamNonBlocking);
+  std::vector<cudaEvent_t> ev_pool;
+  auto take_event = [&]() -> cudaEvent_t {
+    if (!ev_pool.empty()) {
+      cudaEvent_t e = ev_pool.back();
+      ev_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+    return e;
+  };
+  // problems whose block is allocated and whose copies are in flight
+  struct Staged {
+    Req* q;
+    cudaEvent_t ev;
+  };
+  std::vector<Staged> staging;
   std::vector<Req*> active;  // one precision class per batch (f32 or f64 kernels)
   bool batch_f32 = true;
   // device-side batch description
@@ -324,17 +364,18 @@ void bcd_loop(cg_engine_s* E, int cls) {
   };
 
   while (true) {
-    // ---- admission --------------------------------------------------------
+    // ---- admission: reserve, allocate and start the copies (staging) -------
     {
       std::unique_lock<std::mutex> lk(E->mu);
-      if (active.empty())
+      if (active.empty() && staging.empty())
         E->cv.wait(lk, [&] { return E->stop || !bq.empty(); });
-      if (E->stop && active.empty()) break;
-      while (!E->stop && !bq.empty() && (int)active.size() < E->max_batch) {
+      if (E->stop && active.empty() && staging.empty()) break;
+      while (!E->stop && !bq.empty() && (int)(active.size() + staging.size()) < E->max_batch) {
         Req* q = bq.front();
-        if (!active.empty() && (q->r.m_f32 != 0) != batch_f32) break;
+        const bool none = active.empty() && staging.empty();
+        if (!none && (q->r.m_f32 != 0) != batch_f32) break;
         if (!try_reserve(E, q->footprint)) {
-          if (!active.empty() || E->in_use > 0) break;
+          if (!none || E->in_use > 0) break;
           // larger than the whole budget: reject
           bq.pop_front();
           q->status = CG_ERR_ADMISSION;
@@ -346,10 +387,14 @@ void bcd_loop(cg_engine_s* E, int cls) {
         bq.pop_front();
         lk.unlock();
         q->t_admit = now_s();
-        if (active.empty()) batch_f32 = q->r.m_f32 != 0;
-        int rc = bcd_admit(E, q, st);
+        if (none) batch_f32 = q->r.m_f32 != 0;
+        cudaEvent_t evq = take_event(), used = nullptr;
+        int rc = evq ? bcd_stage(q, cst, evq, &used) : CG_ERR_CUDA;
+        if (evq && !used) ev_pool.push_back(evq);
         lk.lock();
         if (rc != CG_OK) {
+          if (q->block) cudaFreeAsync(q->block, cst);
+          q->block = nullptr;
           q->status = rc;
           E->in_use -= q->footprint;
           lk.unlock();
@@ -357,14 +402,40 @@ void bcd_loop(cg_engine_s* E, int cls) {
           lk.lock();
           continue;
         }
-        active.push_back(q);
-        E->active_bcd += (long long)active.size() - my_active;
-        my_active = (long long)active.size();
-        dirty = true;
+        staging.push_back({q, used});
       }
     }
+    // ---- staged problems whose copies have landed join the batch ------------
+    for (size_t k = 0; k < staging.size();) {
+      const Staged sg = staging[k];
+      if (sg.ev && cudaEventQuery(sg.ev) == cudaErrorNotReady) {
+        ++k;
+        continue;
+      }
+      staging.erase(staging.begin() + (long)k);
+      const int rc = bcd_admit(E, sg.q, st, sg.ev);
+      if (sg.ev) ev_pool.push_back(sg.ev);
+      if (rc != CG_OK) {
+        cudaFreeAsync(sg.q->block, st);
+        sg.q->block = nullptr;
+        sg.q->status = rc;
+        release(E, sg.q->footprint);
+        finish(E, sg.q);
+        continue;
+      }
+      active.push_back(sg.q);
+      {
+        std::lock_guard<std::mutex> lk(E->mu);
+        E->active_bcd += (long long)active.size() - my_active;
+      }
+      my_active = (long long)active.size();
+      dirty = true;
+    }
     if (active.empty()) {
-      if (E->stop) break;
+      if (!staging.empty() && staging.front().ev) {
+        // nothing to run until the oldest copy lands
+        while (cudaEventQuery(staging.front().ev) == cudaErrorNotReady) std::this_thread::yield();
+      }
       continue;
     }
     // ---- (re)build the batch description and its chunk graph ---------------
@@ -572,6 +643,9 @@ void bcd_loop(cg_engine_s* E, int cls) {
     }
   }
   if (gexec) cudaGraphExecDestroy(gexec);
+  for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+  cudaStreamSynchronize(cst);
+  cudaStreamDestroy(cst);
   if (d_states) cudaFreeAsync(d_states, st);
   if (h_states) cudaFreeHost(h_states);
   if (d_probs) cudaFreeAsync(d_probs, st);

@@ -73,24 +73,184 @@ PeelPtrs ptrs_of(const PeelFactor& P) {
   return p;
 }
 
+
+// ---- pipelined rounds ------------------------------------------------------
+// Rounds r0, r0 + dir, ..., r1 (inclusive), one __syncthreads after each.
+// Node work is split into pre(idx, st): the loads that do not depend on
+// values computed in earlier rounds (indices, matrix values, right-hand
+// sides), and fin(st): the rest.  Each thread issues pre() for its first node
+// of the next round before the barrier that ends the current one, so a
+// round's critical path is the barrier plus the loads of the children's (or
+// parent's) fresh values.  Nodes past a thread's first in a round (rounds
+// wider than the block) run pre() and fin() back to back.
+template <typename St, typename Pre, typename Fin>
+__device__ __forceinline__ void run_rounds(const int* __restrict__ rptr, int r0, int r1, int dir,
+                                           Pre pre, Fin fin) {
+  if (dir > 0 ? r0 > r1 : r0 < r1) return;
+  St s;
+  int idx = rptr[r0] + threadIdx.x;
+  bool has = idx < rptr[r0 + 1];
+  if (has) pre(idx, s);
+  for (int r = r0;; r += dir) {
+    const int end = rptr[r + 1];
+    if (has) fin(s);
+    for (int k = rptr[r] + threadIdx.x + blockDim.x; k < end; k += blockDim.x) {
+      St o;
+      pre(k, o);
+      fin(o);
+    }
+    const bool last = (r == r1);
+    has = false;
+    if (!last) {
+      const int rn = r + dir;
+      const int in = rptr[rn] + threadIdx.x;
+      if (in < rptr[rn + 1]) {
+        pre(in, s);
+        has = true;
+      }
+    }
+    __syncthreads();
+    if (last) break;
+  }
+}
+
+constexpr int kPreChildren = 4;  // children whose static data a pre() keeps in registers
+
+// Pivot (and up to two forward values) of one node: the static part.
+struct PivotPre {
+  int v, q0, q1;
+  double dv, y0, y1;
+  int ch[kPreChildren];
+  double a[kPreChildren];
+};
+__device__ __forceinline__ void pivot_pre(const double* __restrict__ val, const PeelPtrs& p,
+                                          const double* __restrict__ rhs, int nrhs, int H, int idx,
+                                          PivotPre& o) {
+  const int v = p.order[idx];
+  o.v = v;
+  o.q0 = p.cptr[v];
+  o.q1 = p.cptr[v + 1];
+  o.dv = val[p.diagq[v]];
+  o.y0 = nrhs > 0 ? rhs[v] : 0.0;
+  o.y1 = nrhs > 1 ? rhs[(size_t)H + v] : 0.0;
+#pragma unroll
+  for (int k = 0; k < kPreChildren; ++k) {
+    const int q = o.q0 + k;
+    o.ch[k] = (q < o.q1) ? p.child[q] : 0;
+    o.a[k] = (q < o.q1) ? val[p.childq[q]] : 0.0;
+  }
+}
+// The children's contributions in child order (the same expressions, in the
+// same order, as one loop over the child list).
+__device__ __forceinline__ void pivot_fin(const double* __restrict__ val, const PeelPtrs& p,
+                                          const PivotPre& o, int nrhs, int H,
+                                          double* __restrict__ d, double* __restrict__ y,
+                                          int* __restrict__ info) {
+  double dv = o.dv, y0 = o.y0, y1 = o.y1;
+#pragma unroll
+  for (int k = 0; k < kPreChildren; ++k) {
+    if (o.q0 + k < o.q1) {
+      const int ch = o.ch[k];
+      const double a = o.a[k];
+      const double w = a / d[ch];
+      dv -= w * a;
+      if (nrhs > 0) y0 -= w * y[ch];
+      if (nrhs > 1) y1 -= w * y[(size_t)H + ch];
+    }
+  }
+  for (int q = o.q0 + kPreChildren; q < o.q1; ++q) {
+    const int ch = p.child[q];
+    const double a = val[p.childq[q]];
+    const double w = a / d[ch];
+    dv -= w * a;
+    if (nrhs > 0) y0 -= w * y[ch];
+    if (nrhs > 1) y1 -= w * y[(size_t)H + ch];
+  }
+  d[o.v] = dv;
+  if (nrhs > 0) y[o.v] = y0;
+  if (nrhs > 1) y[(size_t)H + o.v] = y1;
+  if (!(dv > 0.0) || !isfinite(dv)) info[1] = 1;
+}
+
+// Forward values of one node with known pivots: the static part (the child
+// weights a / d_child are final before the solve starts).
+struct ForwardPre {
+  int v, q0, q1;
+  double r0, r1;
+  int ch[kPreChildren];
+  double w[kPreChildren];
+};
+__device__ __forceinline__ void forward_pre(const double* __restrict__ val, const PeelPtrs& p,
+                                            const double* __restrict__ d,
+                                            const double* __restrict__ rhs, int nrhs, int H,
+                                            int idx, ForwardPre& o) {
+  const int v = p.order[idx];
+  o.v = v;
+  o.q0 = p.cptr[v];
+  o.q1 = p.cptr[v + 1];
+  o.r0 = nrhs > 0 ? rhs[v] : 0.0;
+  o.r1 = nrhs > 1 ? rhs[(size_t)H + v] : 0.0;
+#pragma unroll
+  for (int k = 0; k < kPreChildren; ++k) {
+    const int q = o.q0 + k;
+    const int ch = (q < o.q1) ? p.child[q] : 0;
+    o.ch[k] = ch;
+    o.w[k] = (q < o.q1) ? val[p.childq[q]] / d[ch] : 0.0;
+  }
+}
+__device__ __forceinline__ void forward_fin(const double* __restrict__ val, const PeelPtrs& p,
+                                            const double* __restrict__ d, const ForwardPre& o,
+                                            int nrhs, int H, double* __restrict__ y) {
+  for (int c = 0; c < nrhs; ++c) {
+    const double* yc = y + (size_t)c * H;
+    double yv = (c == 0) ? o.r0 : o.r1;
+#pragma unroll
+    for (int k = 0; k < kPreChildren; ++k)
+      if (o.q0 + k < o.q1) yv -= o.w[k] * yc[o.ch[k]];
+    for (int q = o.q0 + kPreChildren; q < o.q1; ++q) {
+      const int ch = p.child[q];
+      yv -= (val[p.childq[q]] / d[ch]) * yc[ch];
+    }
+    y[(size_t)c * H + o.v] = yv;
+  }
+}
+
+// Backward value of one node: the static part (its parent, the edge value,
+// its forward values and pivot).
+struct BackwardPre {
+  int v, u;
+  double pv, dv, y0, y1;
+};
+__device__ __forceinline__ void backward_pre(const double* __restrict__ val, const PeelPtrs& p,
+                                             const double* __restrict__ d,
+                                             const double* __restrict__ y, int nrhs, int H,
+                                             int idx, BackwardPre& o) {
+  const int v = p.order[idx];
+  o.v = v;
+  o.u = p.par[v];
+  o.pv = (o.u >= 0) ? val[p.parq[v]] : 0.0;
+  o.dv = d[v];
+  o.y0 = nrhs > 0 ? y[v] : 0.0;
+  o.y1 = nrhs > 1 ? y[(size_t)H + v] : 0.0;
+}
+__device__ __forceinline__ void backward_fin(const BackwardPre& o, int nrhs, int H,
+                                             double* __restrict__ x) {
+  for (int c = 0; c < nrhs; ++c) {
+    double xv = (c == 0) ? o.y0 : o.y1;
+    if (o.u >= 0) xv -= o.pv * x[(size_t)c * H + o.u];
+    x[(size_t)c * H + o.v] = xv / o.dv;
+  }
+}
+
 // Pivots of every node, round by round; the core nodes come last (one round)
 // and receive their diagonal updated by their peeled children.
 __global__ void __launch_bounds__(kPeelThreads) peel_factor_kernel(
     const double* __restrict__ val, PeelPtrs p, int rounds, double* __restrict__ d,
     int* __restrict__ info) {
-  for (int r = 0; r <= rounds; ++r) {
-    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
-      const int v = p.order[idx];
-      double dv = val[p.diagq[v]];
-      for (int q = p.cptr[v]; q < p.cptr[v + 1]; ++q) {
-        const double a = val[p.childq[q]];
-        dv -= (a / d[p.child[q]]) * a;
-      }
-      d[v] = dv;
-      if (!(dv > 0.0) || !isfinite(dv)) info[1] = 1;
-    }
-    __syncthreads();
-  }
+  run_rounds<PivotPre>(
+      p.rptr, 0, rounds, 1,
+      [&](int idx, PivotPre& o) { pivot_pre(val, p, nullptr, 0, 0, idx, o); },
+      [&](const PivotPre& o) { pivot_fin(val, p, o, 0, 0, d, nullptr, info); });
 }
 
 // Row t of the core Schur complement:
@@ -159,21 +319,10 @@ __global__ void __launch_bounds__(kPeelThreads) peel_forward_kernel(
     const double* __restrict__ val, PeelPtrs p, int rounds, const double* __restrict__ d,
     const double* __restrict__ rhs, int nrhs, int H, int kc, double* __restrict__ y,
     double* __restrict__ rs) {
-  for (int r = 0; r <= rounds; ++r) {
-    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
-      const int v = p.order[idx];
-      for (int c = 0; c < nrhs; ++c) {
-        const double* yc = y + (size_t)c * H;
-        double yv = rhs[(size_t)c * H + v];
-        for (int q = p.cptr[v]; q < p.cptr[v + 1]; ++q) {
-          const int ch = p.child[q];
-          yv -= (val[p.childq[q]] / d[ch]) * yc[ch];
-        }
-        y[(size_t)c * H + v] = yv;
-      }
-    }
-    __syncthreads();
-  }
+  run_rounds<ForwardPre>(
+      p.rptr, 0, rounds, 1,
+      [&](int idx, ForwardPre& o) { forward_pre(val, p, d, rhs, nrhs, H, idx, o); },
+      [&](const ForwardPre& o) { forward_fin(val, p, d, o, nrhs, H, y); });
   for (int t = threadIdx.x; t < kc; t += blockDim.x) {
     const int s = p.snodes[t];
     for (int c = 0; c < nrhs; ++c) {
@@ -205,18 +354,10 @@ __global__ void __launch_bounds__(kPeelThreads) peel_backward_kernel(
     }
   }
   __syncthreads();
-  for (int r = rounds - 1; r >= 0; --r) {
-    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
-      const int v = p.order[idx];
-      const int u = p.par[v];
-      for (int c = 0; c < nrhs; ++c) {
-        double xv = y[(size_t)c * H + v];
-        if (u >= 0) xv -= val[p.parq[v]] * x[(size_t)c * H + u];
-        x[(size_t)c * H + v] = xv / d[v];
-      }
-    }
-    __syncthreads();
-  }
+  run_rounds<BackwardPre>(
+      p.rptr, rounds - 1, 0, -1,
+      [&](int idx, BackwardPre& o) { backward_pre(val, p, d, y, nrhs, H, idx, o); },
+      [&](const BackwardPre& o) { backward_fin(o, nrhs, H, x); });
 }
 
 // ---- small-core path: everything in one CTA --------------------------------
@@ -224,21 +365,10 @@ __global__ void __launch_bounds__(kPeelThreads) peel_backward_kernel(
 __device__ void dev_forward(const double* __restrict__ val, const PeelPtrs& p, int rounds,
                             const double* __restrict__ d, const double* __restrict__ rhs,
                             int nrhs, int H, double* __restrict__ y) {
-  for (int r = 0; r <= rounds; ++r) {
-    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
-      const int v = p.order[idx];
-      for (int c = 0; c < nrhs; ++c) {
-        const double* yc = y + (size_t)c * H;
-        double yv = rhs[(size_t)c * H + v];
-        for (int q = p.cptr[v]; q < p.cptr[v + 1]; ++q) {
-          const int ch = p.child[q];
-          yv -= (val[p.childq[q]] / d[ch]) * yc[ch];
-        }
-        y[(size_t)c * H + v] = yv;
-      }
-    }
-    __syncthreads();
-  }
+  run_rounds<ForwardPre>(
+      p.rptr, 0, rounds, 1,
+      [&](int idx, ForwardPre& o) { forward_pre(val, p, d, rhs, nrhs, H, idx, o); },
+      [&](const ForwardPre& o) { forward_fin(val, p, d, o, nrhs, H, y); });
 }
 
 // Core right-hand side reduced to the Schur side, into z[c * kc + t].
@@ -265,26 +395,58 @@ __device__ void dev_core_rhs(const double* __restrict__ val, const PeelPtrs& p,
 __host__ __device__ __forceinline__ int core_ld(int kc) { return kc | 1; }
 
 // z <- (L L^T)^{-1} z for nrhs columns; L lower, row-major kc x kc with row
-// stride ld (shared).  One warp per right-hand side: the column sweeps
-// synchronise with __syncwarp only.  Every z entry receives its updates in
-// the same order as a column sweep.
-__device__ void dev_trisolve(const double* __restrict__ L, int kc, int ld, double* __restrict__ z,
-                             int nrhs) {
+// stride ld (shared), idiag[j] = 1 / L_jj.  One warp per right-hand side,
+// blocks of 32 rows: the diagonal block is solved in registers (lane r holds
+// z_r; the solved value is broadcast by a shuffle), the rows below (forward)
+// or the block's own entries (backward) take the other blocks' contributions
+// as dot products.  __syncwarp only.
+__device__ void dev_trisolve(const double* __restrict__ L, const double* __restrict__ idiag,
+                             int kc, int ld, double* __restrict__ z, int nrhs) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp < nrhs) {
     double* zc = z + (size_t)warp * kc;
-    for (int j = 0; j < kc; ++j) {
-      const double zj = zc[j] / L[j * ld + j];
+    for (int j0 = 0; j0 < kc; j0 += 32) {  // L y = z
+      const int bw = min(32, kc - j0);
+      double zr = (lane < bw) ? zc[j0 + lane] : 0.0;
+      for (int jj = 0; jj < bw; ++jj) {
+        const double zj = __shfl_sync(0xffffffffu, zr, jj) * idiag[j0 + jj];
+        if (lane == jj) zr = zj;
+        if (lane > jj && lane < bw) zr = fma(-L[(size_t)(j0 + lane) * ld + j0 + jj], zj, zr);
+      }
+      if (lane < bw) zc[j0 + lane] = zr;
       __syncwarp();
-      for (int i = j + 1 + lane; i < kc; i += 32) zc[i] = fma(-L[i * ld + j], zj, zc[i]);
-      if (lane == 0) zc[j] = zj;
+      for (int i = j0 + bw + lane; i < kc; i += 32) {
+        const double* Li = L + (size_t)i * ld + j0;
+        double a0 = zc[i], a1 = 0.0;
+        int c = 0;
+        for (; c + 1 < bw; c += 2) {
+          a0 = fma(-Li[c], zc[j0 + c], a0);
+          a1 = fma(-Li[c + 1], zc[j0 + c + 1], a1);
+        }
+        if (c < bw) a0 = fma(-Li[c], zc[j0 + c], a0);
+        zc[i] = a0 + a1;
+      }
       __syncwarp();
     }
-    for (int j = kc - 1; j >= 0; --j) {
-      const double zj = zc[j] / L[j * ld + j];
-      __syncwarp();
-      for (int i = lane; i < j; i += 32) zc[i] = fma(-L[j * ld + i], zj, zc[i]);
-      if (lane == 0) zc[j] = zj;
+    for (int j1 = kc; j1 > 0; j1 -= 32) {  // L^T x = y
+      const int j0 = max(0, j1 - 32), bw = j1 - j0;
+      double zr = 0.0;
+      if (lane < bw) {
+        double a0 = zc[j0 + lane], a1 = 0.0;
+        int i = j1;
+        for (; i + 1 < kc; i += 2) {
+          a0 = fma(-L[(size_t)i * ld + j0 + lane], zc[i], a0);
+          a1 = fma(-L[(size_t)(i + 1) * ld + j0 + lane], zc[i + 1], a1);
+        }
+        if (i < kc) a0 = fma(-L[(size_t)i * ld + j0 + lane], zc[i], a0);
+        zr = a0 + a1;
+      }
+      for (int jj = bw - 1; jj >= 0; --jj) {
+        const double zj = __shfl_sync(0xffffffffu, zr, jj) * idiag[j0 + jj];
+        if (lane == jj) zr = zj;
+        if (lane < jj) zr = fma(-L[(size_t)(j0 + jj) * ld + j0 + lane], zj, zr);
+      }
+      if (lane < bw) zc[j0 + lane] = zr;
       __syncwarp();
     }
   }
@@ -293,22 +455,24 @@ __device__ void dev_trisolve(const double* __restrict__ L, int kc, int ld, doubl
 
 // In-place Cholesky S = L L^T of the lower triangle (row-major kc x kc, row
 // stride ld, shared), blocked by panels of 32 columns, three block barriers
-// per panel:
-//   1. the 32 x 32 diagonal block, by warp 0 alone (lane r owns row r of the
-//      block; a right-looking sweep with __syncwarp between columns);
-//   2. the panel below it, L21 = S21 L11^{-T}: each thread solves whole rows
-//      by forward substitution along the panel's columns;
+// per panel; idiag[j] <- 1 / L_jj.
+//   1. the 32 x 32 diagonal block, by warp 0 alone: lane r owns row r of the
+//      block; column k is scaled by its pivot, then each lane applies the
+//      rank-1 update to its own row, taking L_ck from lane c by a shuffle;
+//   2. the panel below it, L21 = S21 L11^{-T}: each thread solves whole rows,
+//      entry k as a dot product over the row's earlier entries;
 //   3. the trailing update S22 -= L21 L21^T on the lower triangle: a work
 //      item is one column c of a 4-row tile (rows i0..i0+3, c <= i), its
 //      four dot products over the panel accumulated in registers.
 // A pivot that is not positive and finite sets info = column + 1 and
 // continues with d = 1 (the last such column is reported).
-__device__ void dev_cholesky(double* __restrict__ S, int kc, int ld, int* __restrict__ info) {
+__device__ void dev_cholesky(double* __restrict__ S, double* __restrict__ idiag, int kc, int ld,
+                             int* __restrict__ info) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int j0 = 0; j0 < kc; j0 += 32) {
     const int bw = min(32, kc - j0);
     if (warp == 0) {
-      double* Sr = S + (size_t)(j0 + lane) * ld + j0;  // this lane's block row
+      double* Sr = S + (size_t)(j0 + min(lane, bw - 1)) * ld + j0;  // this lane's block row
       for (int k = 0; k < bw; ++k) {
         double d = S[(size_t)(j0 + k) * ld + j0 + k];
         if (!(d > 0.0) || !isfinite(d)) {
@@ -321,11 +485,15 @@ __device__ void dev_cholesky(double* __restrict__ S, int kc, int ld, int* __rest
           lrk = Sr[k] / lkk;
           Sr[k] = lrk;
         }
-        __syncwarp();
-        if (lane == k) Sr[k] = lkk;
-        if (lane > k && lane < bw)
-          for (int c = k + 1; c <= lane; ++c)
-            Sr[c] = fma(-lrk, S[(size_t)(j0 + c) * ld + j0 + k], Sr[c]);
+        __syncwarp();  // every lane has read the pivot
+        if (lane == k) {
+          Sr[k] = lkk;
+          idiag[j0 + k] = 1.0 / lkk;
+        }
+        for (int c = k + 1; c < bw; ++c) {
+          const double lck = __shfl_sync(0xffffffffu, lrk, c);
+          if (lane >= c && lane < bw) Sr[c] = fma(-lrk, lck, Sr[c]);
+        }
         __syncwarp();
       }
     }
@@ -334,9 +502,15 @@ __device__ void dev_cholesky(double* __restrict__ S, int kc, int ld, int* __rest
     for (int i = r0 + threadIdx.x; i < kc; i += blockDim.x) {
       double* Si = S + (size_t)i * ld + j0;
       for (int k = 0; k < bw; ++k) {
-        const double v = Si[k] / S[(size_t)(j0 + k) * ld + j0 + k];
-        Si[k] = v;
-        for (int c = k + 1; c < bw; ++c) Si[c] = fma(-v, S[(size_t)(j0 + c) * ld + j0 + k], Si[c]);
+        const double* Lk = S + (size_t)(j0 + k) * ld + j0;
+        double a0 = Si[k], a1 = 0.0;
+        int c = 0;
+        for (; c + 1 < k; c += 2) {
+          a0 = fma(-Si[c], Lk[c], a0);
+          a1 = fma(-Si[c + 1], Lk[c + 1], a1);
+        }
+        if (c < k) a0 = fma(-Si[c], Lk[c], a0);
+        Si[k] = (a0 + a1) * idiag[j0 + k];
       }
     }
     __syncthreads();
@@ -389,23 +563,16 @@ __device__ void dev_backward(const double* __restrict__ val, const PeelPtrs& p, 
     }
   }
   __syncthreads();
-  for (int r = rounds - 1; r >= 0; --r) {
-    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
-      const int v = p.order[idx];
-      const int u = p.par[v];
-      for (int c = 0; c < nrhs; ++c) {
-        double xv = y[(size_t)c * H + v];
-        if (u >= 0) xv -= val[p.parq[v]] * x[(size_t)c * H + u];
-        x[(size_t)c * H + v] = xv / d[v];
-      }
-    }
-    __syncthreads();
-  }
+  run_rounds<BackwardPre>(
+      p.rptr, rounds - 1, 0, -1,
+      [&](int idx, BackwardPre& o) { backward_pre(val, p, d, y, nrhs, H, idx, o); },
+      [&](const BackwardPre& o) { backward_fin(o, nrhs, H, x); });
 }
 
 // Factorization (pivots d, core factor L -> Lout) and, for nrhs > 0, the
-// solve x = A^{-1} rhs.  Dynamic shared memory: kc*ld + 2*kc doubles (ld =
-// core_ld(kc), the shared row stride of the core matrix).
+// solve x = A^{-1} rhs.  Dynamic shared memory: kc*ld + 3*kc doubles (ld =
+// core_ld(kc), the shared row stride of the core matrix; then 2 kc for the
+// reduced right-hand sides and kc for the inverse diagonal of the factor).
 __global__ void __launch_bounds__(kPeelThreads) peel_fused_kernel(
     const double* __restrict__ val, PeelPtrs p, int rounds, int kc, int ke, int H,
     const double* __restrict__ rhs, int nrhs, double* __restrict__ x, double* __restrict__ d,
@@ -415,27 +582,12 @@ __global__ void __launch_bounds__(kPeelThreads) peel_fused_kernel(
   const int ld = core_ld(kc);
   double* S = sm;
   double* z = sm + (size_t)kc * ld;
+  double* idiag = z + 2 * (size_t)kc;
   // pivots and forward values, round by round (core last)
-  for (int r = 0; r <= rounds; ++r) {
-    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
-      const int v = p.order[idx];
-      double dv = val[p.diagq[v]];
-      double y0 = nrhs > 0 ? rhs[v] : 0.0, y1 = nrhs > 1 ? rhs[(size_t)H + v] : 0.0;
-      for (int q = p.cptr[v]; q < p.cptr[v + 1]; ++q) {
-        const int ch = p.child[q];
-        const double a = val[p.childq[q]];
-        const double w = a / d[ch];
-        dv -= w * a;
-        if (nrhs > 0) y0 -= w * y[ch];
-        if (nrhs > 1) y1 -= w * y[(size_t)H + ch];
-      }
-      d[v] = dv;
-      if (nrhs > 0) y[v] = y0;
-      if (nrhs > 1) y[(size_t)H + v] = y1;
-      if (!(dv > 0.0) || !isfinite(dv)) info[1] = 1;
-    }
-    __syncthreads();
-  }
+  run_rounds<PivotPre>(
+      p.rptr, 0, rounds, 1,
+      [&](int idx, PivotPre& o) { pivot_pre(val, p, rhs, nrhs, H, idx, o); },
+      [&](const PivotPre& o) { pivot_fin(val, p, o, nrhs, H, d, y, info); });
   if (kc > 0 && p.ccp != nullptr) {
     // edge weights, then the core Schur complement from the contribution
     // lists, one thread per entry
@@ -471,7 +623,7 @@ __global__ void __launch_bounds__(kPeelThreads) peel_fused_kernel(
     __syncthreads();
   }
   if (kc > 0) {
-    dev_cholesky(S, kc, ld, info);
+    dev_cholesky(S, idiag, kc, ld, info);
     for (int e = threadIdx.x; e < kc * kc; e += blockDim.x) {
       const int t = e / kc;
       Lout[e] = S[(size_t)t * ld + (e - t * kc)];
@@ -480,7 +632,7 @@ __global__ void __launch_bounds__(kPeelThreads) peel_fused_kernel(
   if (nrhs == 0) return;
   if (kc > 0) {
     dev_core_rhs(val, p, d, y, nrhs, H, kc, z);
-    dev_trisolve(S, kc, ld, z, nrhs);
+    dev_trisolve(S, idiag, kc, ld, z, nrhs);
   }
   dev_backward(val, p, rounds, d, y, z, nrhs, H, kc, ke, x);
 }
@@ -494,20 +646,22 @@ __global__ void __launch_bounds__(kPeelThreads) peel_small_solve_kernel(
   const int ld = core_ld(kc);
   double* S = sm;
   double* z = sm + (size_t)kc * ld;
+  double* idiag = z + 2 * (size_t)kc;
   for (int e = threadIdx.x; e < kc * kc; e += blockDim.x) {
     const int t = e / kc;
     S[(size_t)t * ld + (e - t * kc)] = Lin[e];
   }
+  for (int t = threadIdx.x; t < kc; t += blockDim.x) idiag[t] = 1.0 / Lin[(size_t)t * kc + t];
   dev_forward(val, p, rounds, d, rhs, nrhs, H, y);  // its round barriers also publish S
   if (kc > 0) {
     dev_core_rhs(val, p, d, y, nrhs, H, kc, z);
-    dev_trisolve(S, kc, ld, z, nrhs);
+    dev_trisolve(S, idiag, kc, ld, z, nrhs);
   }
   dev_backward(val, p, rounds, d, y, z, nrhs, H, kc, ke, x);
 }
 
 size_t small_smem(int kc) {
-  return ((size_t)kc * core_ld(kc) + 2 * (size_t)std::max(kc, 1)) * sizeof(double);
+  return ((size_t)kc * core_ld(kc) + 3 * (size_t)std::max(kc, 1)) * sizeof(double);
 }
 
 int ensure_small_smem() {
