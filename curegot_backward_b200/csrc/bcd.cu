@@ -40,6 +40,14 @@
 #endif
 // Resident CTAs per SM the row/column passes are compiled for (register cap).
 constexpr int kBcdMinBlocks = CG_BCD_MINB;
+// FP32-M vectors per lane per loop step of the row pass and rows per step of
+// the column pass (4-float vectors; FP64 M takes 4 two-double vectors / rows).
+#ifndef CG_F32_ROW_U
+#define CG_F32_ROW_U 2
+#endif
+#ifndef CG_F32_COL_U
+#define CG_F32_COL_U 2
+#endif
 
 namespace cg {
 
@@ -47,7 +55,7 @@ namespace {
 // Elements per lane per step: 8 (two float4 or four double2 vectors).
 template <typename TM>
 struct RowU {
-  static constexpr int U = (Vec<TM>::N == 4) ? 2 : 4;
+  static constexpr int U = (Vec<TM>::N == 4) ? CG_F32_ROW_U : 4;
 };
 
 // L2 bulk prefetch of the chunk [pos, min(pos + span, c1)) of a row whose
@@ -590,7 +598,7 @@ __device__ __forceinline__ void col_rows(const TM* __restrict__ M, const double*
                                          const float2* __restrict__ asplit = nullptr,
                                          float s2h = 0.0f, float s2l = 0.0f) {
   constexpr int VN = Vec<TM>::N;
-  constexpr int U = (VN == 4) ? 2 : 4;  // 8 elements per lane per step
+  constexpr int U = (VN == 4) ? CG_F32_COL_U : 4;  // rows per lane per step
   constexpr int rstep = kWarps * U;
   const int lane = threadIdx.x & 31;
   if (vec_ok) {
@@ -682,7 +690,7 @@ __device__ __forceinline__ void col_rows_staged(const TM* __restrict__ M,
                                                 double* s, const float2* __restrict__ asplit = nullptr,
                                                 float s2h = 0.0f, float s2l = 0.0f) {
   constexpr int VN = Vec<TM>::N;
-  constexpr int U = (VN == 4) ? 2 : 4;
+  constexpr int U = (VN == 4) ? CG_F32_COL_U : 4;
   constexpr int RPC = kRingBytes / 512;  // warp rows per ring chunk
   static_assert(RPC % U == 0, "ring chunk must hold whole row groups");
   using RT = typename Raw<TM>::T;

@@ -74,183 +74,24 @@ PeelPtrs ptrs_of(const PeelFactor& P) {
 }
 
 
-// ---- pipelined rounds ------------------------------------------------------
-// Rounds r0, r0 + dir, ..., r1 (inclusive), one __syncthreads after each.
-// Node work is split into pre(idx, st): the loads that do not depend on
-// values computed in earlier rounds (indices, matrix values, right-hand
-// sides), and fin(st): the rest.  Each thread issues pre() for its first node
-// of the next round before the barrier that ends the current one, so a
-// round's critical path is the barrier plus the loads of the children's (or
-// parent's) fresh values.  Nodes past a thread's first in a round (rounds
-// wider than the block) run pre() and fin() back to back.
-template <typename St, typename Pre, typename Fin>
-__device__ __forceinline__ void run_rounds(const int* __restrict__ rptr, int r0, int r1, int dir,
-                                           Pre pre, Fin fin) {
-  if (dir > 0 ? r0 > r1 : r0 < r1) return;
-  St s;
-  int idx = rptr[r0] + threadIdx.x;
-  bool has = idx < rptr[r0 + 1];
-  if (has) pre(idx, s);
-  for (int r = r0;; r += dir) {
-    const int end = rptr[r + 1];
-    if (has) fin(s);
-    for (int k = rptr[r] + threadIdx.x + blockDim.x; k < end; k += blockDim.x) {
-      St o;
-      pre(k, o);
-      fin(o);
-    }
-    const bool last = (r == r1);
-    has = false;
-    if (!last) {
-      const int rn = r + dir;
-      const int in = rptr[rn] + threadIdx.x;
-      if (in < rptr[rn + 1]) {
-        pre(in, s);
-        has = true;
-      }
-    }
-    __syncthreads();
-    if (last) break;
-  }
-}
-
-constexpr int kPreChildren = 4;  // children whose static data a pre() keeps in registers
-
-// Pivot (and up to two forward values) of one node: the static part.
-struct PivotPre {
-  int v, q0, q1;
-  double dv, y0, y1;
-  int ch[kPreChildren];
-  double a[kPreChildren];
-};
-__device__ __forceinline__ void pivot_pre(const double* __restrict__ val, const PeelPtrs& p,
-                                          const double* __restrict__ rhs, int nrhs, int H, int idx,
-                                          PivotPre& o) {
-  const int v = p.order[idx];
-  o.v = v;
-  o.q0 = p.cptr[v];
-  o.q1 = p.cptr[v + 1];
-  o.dv = val[p.diagq[v]];
-  o.y0 = nrhs > 0 ? rhs[v] : 0.0;
-  o.y1 = nrhs > 1 ? rhs[(size_t)H + v] : 0.0;
-#pragma unroll
-  for (int k = 0; k < kPreChildren; ++k) {
-    const int q = o.q0 + k;
-    o.ch[k] = (q < o.q1) ? p.child[q] : 0;
-    o.a[k] = (q < o.q1) ? val[p.childq[q]] : 0.0;
-  }
-}
-// The children's contributions in child order (the same expressions, in the
-// same order, as one loop over the child list).
-__device__ __forceinline__ void pivot_fin(const double* __restrict__ val, const PeelPtrs& p,
-                                          const PivotPre& o, int nrhs, int H,
-                                          double* __restrict__ d, double* __restrict__ y,
-                                          int* __restrict__ info) {
-  double dv = o.dv, y0 = o.y0, y1 = o.y1;
-#pragma unroll
-  for (int k = 0; k < kPreChildren; ++k) {
-    if (o.q0 + k < o.q1) {
-      const int ch = o.ch[k];
-      const double a = o.a[k];
-      const double w = a / d[ch];
-      dv -= w * a;
-      if (nrhs > 0) y0 -= w * y[ch];
-      if (nrhs > 1) y1 -= w * y[(size_t)H + ch];
-    }
-  }
-  for (int q = o.q0 + kPreChildren; q < o.q1; ++q) {
-    const int ch = p.child[q];
-    const double a = val[p.childq[q]];
-    const double w = a / d[ch];
-    dv -= w * a;
-    if (nrhs > 0) y0 -= w * y[ch];
-    if (nrhs > 1) y1 -= w * y[(size_t)H + ch];
-  }
-  d[o.v] = dv;
-  if (nrhs > 0) y[o.v] = y0;
-  if (nrhs > 1) y[(size_t)H + o.v] = y1;
-  if (!(dv > 0.0) || !isfinite(dv)) info[1] = 1;
-}
-
-// Forward values of one node with known pivots: the static part (the child
-// weights a / d_child are final before the solve starts).
-struct ForwardPre {
-  int v, q0, q1;
-  double r0, r1;
-  int ch[kPreChildren];
-  double w[kPreChildren];
-};
-__device__ __forceinline__ void forward_pre(const double* __restrict__ val, const PeelPtrs& p,
-                                            const double* __restrict__ d,
-                                            const double* __restrict__ rhs, int nrhs, int H,
-                                            int idx, ForwardPre& o) {
-  const int v = p.order[idx];
-  o.v = v;
-  o.q0 = p.cptr[v];
-  o.q1 = p.cptr[v + 1];
-  o.r0 = nrhs > 0 ? rhs[v] : 0.0;
-  o.r1 = nrhs > 1 ? rhs[(size_t)H + v] : 0.0;
-#pragma unroll
-  for (int k = 0; k < kPreChildren; ++k) {
-    const int q = o.q0 + k;
-    const int ch = (q < o.q1) ? p.child[q] : 0;
-    o.ch[k] = ch;
-    o.w[k] = (q < o.q1) ? val[p.childq[q]] / d[ch] : 0.0;
-  }
-}
-__device__ __forceinline__ void forward_fin(const double* __restrict__ val, const PeelPtrs& p,
-                                            const double* __restrict__ d, const ForwardPre& o,
-                                            int nrhs, int H, double* __restrict__ y) {
-  for (int c = 0; c < nrhs; ++c) {
-    const double* yc = y + (size_t)c * H;
-    double yv = (c == 0) ? o.r0 : o.r1;
-#pragma unroll
-    for (int k = 0; k < kPreChildren; ++k)
-      if (o.q0 + k < o.q1) yv -= o.w[k] * yc[o.ch[k]];
-    for (int q = o.q0 + kPreChildren; q < o.q1; ++q) {
-      const int ch = p.child[q];
-      yv -= (val[p.childq[q]] / d[ch]) * yc[ch];
-    }
-    y[(size_t)c * H + o.v] = yv;
-  }
-}
-
-// Backward value of one node: the static part (its parent, the edge value,
-// its forward values and pivot).
-struct BackwardPre {
-  int v, u;
-  double pv, dv, y0, y1;
-};
-__device__ __forceinline__ void backward_pre(const double* __restrict__ val, const PeelPtrs& p,
-                                             const double* __restrict__ d,
-                                             const double* __restrict__ y, int nrhs, int H,
-                                             int idx, BackwardPre& o) {
-  const int v = p.order[idx];
-  o.v = v;
-  o.u = p.par[v];
-  o.pv = (o.u >= 0) ? val[p.parq[v]] : 0.0;
-  o.dv = d[v];
-  o.y0 = nrhs > 0 ? y[v] : 0.0;
-  o.y1 = nrhs > 1 ? y[(size_t)H + v] : 0.0;
-}
-__device__ __forceinline__ void backward_fin(const BackwardPre& o, int nrhs, int H,
-                                             double* __restrict__ x) {
-  for (int c = 0; c < nrhs; ++c) {
-    double xv = (c == 0) ? o.y0 : o.y1;
-    if (o.u >= 0) xv -= o.pv * x[(size_t)c * H + o.u];
-    x[(size_t)c * H + o.v] = xv / o.dv;
-  }
-}
-
 // Pivots of every node, round by round; the core nodes come last (one round)
 // and receive their diagonal updated by their peeled children.
 __global__ void __launch_bounds__(kPeelThreads) peel_factor_kernel(
     const double* __restrict__ val, PeelPtrs p, int rounds, double* __restrict__ d,
     int* __restrict__ info) {
-  run_rounds<PivotPre>(
-      p.rptr, 0, rounds, 1,
-      [&](int idx, PivotPre& o) { pivot_pre(val, p, nullptr, 0, 0, idx, o); },
-      [&](const PivotPre& o) { pivot_fin(val, p, o, 0, 0, d, nullptr, info); });
+  for (int r = 0; r <= rounds; ++r) {
+    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
+      const int v = p.order[idx];
+      double dv = val[p.diagq[v]];
+      for (int q = p.cptr[v]; q < p.cptr[v + 1]; ++q) {
+        const double a = val[p.childq[q]];
+        dv -= (a / d[p.child[q]]) * a;
+      }
+      d[v] = dv;
+      if (!(dv > 0.0) || !isfinite(dv)) info[1] = 1;
+    }
+    __syncthreads();
+  }
 }
 
 // Row t of the core Schur complement:
@@ -319,10 +160,21 @@ __global__ void __launch_bounds__(kPeelThreads) peel_forward_kernel(
     const double* __restrict__ val, PeelPtrs p, int rounds, const double* __restrict__ d,
     const double* __restrict__ rhs, int nrhs, int H, int kc, double* __restrict__ y,
     double* __restrict__ rs) {
-  run_rounds<ForwardPre>(
-      p.rptr, 0, rounds, 1,
-      [&](int idx, ForwardPre& o) { forward_pre(val, p, d, rhs, nrhs, H, idx, o); },
-      [&](const ForwardPre& o) { forward_fin(val, p, d, o, nrhs, H, y); });
+  for (int r = 0; r <= rounds; ++r) {
+    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
+      const int v = p.order[idx];
+      for (int c = 0; c < nrhs; ++c) {
+        const double* yc = y + (size_t)c * H;
+        double yv = rhs[(size_t)c * H + v];
+        for (int q = p.cptr[v]; q < p.cptr[v + 1]; ++q) {
+          const int ch = p.child[q];
+          yv -= (val[p.childq[q]] / d[ch]) * yc[ch];
+        }
+        y[(size_t)c * H + v] = yv;
+      }
+    }
+    __syncthreads();
+  }
   for (int t = threadIdx.x; t < kc; t += blockDim.x) {
     const int s = p.snodes[t];
     for (int c = 0; c < nrhs; ++c) {
@@ -354,10 +206,18 @@ __global__ void __launch_bounds__(kPeelThreads) peel_backward_kernel(
     }
   }
   __syncthreads();
-  run_rounds<BackwardPre>(
-      p.rptr, rounds - 1, 0, -1,
-      [&](int idx, BackwardPre& o) { backward_pre(val, p, d, y, nrhs, H, idx, o); },
-      [&](const BackwardPre& o) { backward_fin(o, nrhs, H, x); });
+  for (int r = rounds - 1; r >= 0; --r) {
+    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
+      const int v = p.order[idx];
+      const int u = p.par[v];
+      for (int c = 0; c < nrhs; ++c) {
+        double xv = y[(size_t)c * H + v];
+        if (u >= 0) xv -= val[p.parq[v]] * x[(size_t)c * H + u];
+        x[(size_t)c * H + v] = xv / d[v];
+      }
+    }
+    __syncthreads();
+  }
 }
 
 // ---- small-core path: everything in one CTA --------------------------------
@@ -365,10 +225,21 @@ __global__ void __launch_bounds__(kPeelThreads) peel_backward_kernel(
 __device__ void dev_forward(const double* __restrict__ val, const PeelPtrs& p, int rounds,
                             const double* __restrict__ d, const double* __restrict__ rhs,
                             int nrhs, int H, double* __restrict__ y) {
-  run_rounds<ForwardPre>(
-      p.rptr, 0, rounds, 1,
-      [&](int idx, ForwardPre& o) { forward_pre(val, p, d, rhs, nrhs, H, idx, o); },
-      [&](const ForwardPre& o) { forward_fin(val, p, d, o, nrhs, H, y); });
+  for (int r = 0; r <= rounds; ++r) {
+    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
+      const int v = p.order[idx];
+      for (int c = 0; c < nrhs; ++c) {
+        const double* yc = y + (size_t)c * H;
+        double yv = rhs[(size_t)c * H + v];
+        for (int q = p.cptr[v]; q < p.cptr[v + 1]; ++q) {
+          const int ch = p.child[q];
+          yv -= (val[p.childq[q]] / d[ch]) * yc[ch];
+        }
+        y[(size_t)c * H + v] = yv;
+      }
+    }
+    __syncthreads();
+  }
 }
 
 // Core right-hand side reduced to the Schur side, into z[c * kc + t].
@@ -563,10 +434,18 @@ __device__ void dev_backward(const double* __restrict__ val, const PeelPtrs& p, 
     }
   }
   __syncthreads();
-  run_rounds<BackwardPre>(
-      p.rptr, rounds - 1, 0, -1,
-      [&](int idx, BackwardPre& o) { backward_pre(val, p, d, y, nrhs, H, idx, o); },
-      [&](const BackwardPre& o) { backward_fin(o, nrhs, H, x); });
+  for (int r = rounds - 1; r >= 0; --r) {
+    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
+      const int v = p.order[idx];
+      const int u = p.par[v];
+      for (int c = 0; c < nrhs; ++c) {
+        double xv = y[(size_t)c * H + v];
+        if (u >= 0) xv -= val[p.parq[v]] * x[(size_t)c * H + u];
+        x[(size_t)c * H + v] = xv / d[v];
+      }
+    }
+    __syncthreads();
+  }
 }
 
 // Factorization (pivots d, core factor L -> Lout) and, for nrhs > 0, the
@@ -584,10 +463,26 @@ __global__ void __launch_bounds__(kPeelThreads) peel_fused_kernel(
   double* z = sm + (size_t)kc * ld;
   double* idiag = z + 2 * (size_t)kc;
   // pivots and forward values, round by round (core last)
-  run_rounds<PivotPre>(
-      p.rptr, 0, rounds, 1,
-      [&](int idx, PivotPre& o) { pivot_pre(val, p, rhs, nrhs, H, idx, o); },
-      [&](const PivotPre& o) { pivot_fin(val, p, o, nrhs, H, d, y, info); });
+  for (int r = 0; r <= rounds; ++r) {
+    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
+      const int v = p.order[idx];
+      double dv = val[p.diagq[v]];
+      double y0 = nrhs > 0 ? rhs[v] : 0.0, y1 = nrhs > 1 ? rhs[(size_t)H + v] : 0.0;
+      for (int q = p.cptr[v]; q < p.cptr[v + 1]; ++q) {
+        const int ch = p.child[q];
+        const double a = val[p.childq[q]];
+        const double w = a / d[ch];
+        dv -= w * a;
+        if (nrhs > 0) y0 -= w * y[ch];
+        if (nrhs > 1) y1 -= w * y[(size_t)H + ch];
+      }
+      d[v] = dv;
+      if (nrhs > 0) y[v] = y0;
+      if (nrhs > 1) y[(size_t)H + v] = y1;
+      if (!(dv > 0.0) || !isfinite(dv)) info[1] = 1;
+    }
+    __syncthreads();
+  }
   if (kc > 0 && p.ccp != nullptr) {
     // edge weights, then the core Schur complement from the contribution
     // lists, one thread per entry
