@@ -46,7 +46,7 @@ constexpr int kBcdMinBlocks = CG_BCD_MINB;
 #define CG_F32_ROW_U 2
 #endif
 #ifndef CG_F32_COL_U
-#define CG_F32_COL_U 2
+#define CG_F32_COL_U 4
 #endif
 
 namespace cg {

@@ -26,7 +26,10 @@
 #include <algorithm>
 #include <cmath>
 
+#include "chol.cuh"
+#include "dense.cuh"
 #include "peel.cuh"
+#include "schur.cuh"
 
 namespace cg {
 
@@ -327,9 +330,8 @@ __device__ void dev_trisolve(const double* __restrict__ L, const double* __restr
 // In-place Cholesky S = L L^T of the lower triangle (row-major kc x kc, row
 // stride ld, shared), blocked by panels of 32 columns, three block barriers
 // per panel; idiag[j] <- 1 / L_jj.
-//   1. the 32 x 32 diagonal block, by warp 0 alone: lane r owns row r of the
-//      block; column k is scaled by its pivot, then each lane applies the
-//      rank-1 update to its own row, taking L_ck from lane c by a shuffle;
+//   1. the 32 x 32 diagonal block, by warp 0 alone (warp_block_cholesky:
+//      left-looking, lane r computes row r of the block);
 //   2. the panel below it, L21 = S21 L11^{-T}: each thread solves whole rows,
 //      entry k as a dot product over the row's earlier entries;
 //   3. the trailing update S22 -= L21 L21^T on the lower triangle: a work
@@ -342,32 +344,7 @@ __device__ void dev_cholesky(double* __restrict__ S, double* __restrict__ idiag,
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int j0 = 0; j0 < kc; j0 += 32) {
     const int bw = min(32, kc - j0);
-    if (warp == 0) {
-      double* Sr = S + (size_t)(j0 + min(lane, bw - 1)) * ld + j0;  // this lane's block row
-      for (int k = 0; k < bw; ++k) {
-        double d = S[(size_t)(j0 + k) * ld + j0 + k];
-        if (!(d > 0.0) || !isfinite(d)) {
-          if (lane == 0) info[0] = j0 + k + 1;
-          d = 1.0;
-        }
-        const double lkk = sqrt(d);
-        double lrk = 0.0;
-        if (lane > k && lane < bw) {
-          lrk = Sr[k] / lkk;
-          Sr[k] = lrk;
-        }
-        __syncwarp();  // every lane has read the pivot
-        if (lane == k) {
-          Sr[k] = lkk;
-          idiag[j0 + k] = 1.0 / lkk;
-        }
-        for (int c = k + 1; c < bw; ++c) {
-          const double lck = __shfl_sync(0xffffffffu, lrk, c);
-          if (lane >= c && lane < bw) Sr[c] = fma(-lrk, lck, Sr[c]);
-        }
-        __syncwarp();
-      }
-    }
+    if (warp == 0) warp_block_cholesky(S + (size_t)j0 * ld + j0, ld, bw, idiag + j0, j0, info);
     __syncthreads();
     const int r0 = j0 + bw;  // first row below the block
     for (int i = r0 + threadIdx.x; i < kc; i += blockDim.x) {
@@ -814,6 +791,7 @@ int peel_upload(PeelFactor& P, cusolverDnHandle_t h, cudaStream_t st, bool plan_
     set_last_error("cusolverDnDpotrf_bufferSize failed", __FILE__, __LINE__);
     return CG_ERR_SOLVER;
   }
+  if (!plan_only && kc > kSmallCore) lwork = std::max(lwork, kc);  // dense.cu's inverse diagonal
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   const size_t ib = al(P.h_ints.size() * sizeof(int));
   const size_t wb = al((size_t)std::max<long long>(P.ne_adj, 1) * 8);
@@ -873,6 +851,7 @@ int peel_factor(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, cudaStream
       { peel_assemble_kernel<<<P.kc, 256, 0, st>>>(A.val, pp, P.d, P.kc, P.S); count_launch(); }
     }
     CG_TRY_CUDA(cudaGetLastError());
+    if (use_dense_custom(P.kc)) return dense_chol_factor(P.S, P.kc, P.work, P.info, st);
     if (cusolverDnSetStream(h, st) != CUSOLVER_STATUS_SUCCESS) return CG_ERR_SOLVER;
     if (cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, P.kc, P.S, P.kc, P.work, P.lwork, P.info) !=
         CUSOLVER_STATUS_SUCCESS) {
@@ -903,11 +882,15 @@ int peel_solve(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, const doubl
                                                     P.kc, P.y, P.rs); count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
   if (P.kc > 0) {
-    if (cusolverDnSetStream(h, st) != CUSOLVER_STATUS_SUCCESS) return CG_ERR_SOLVER;
-    if (cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, P.kc, nrhs, P.S, P.kc, P.rs, P.kc,
-                         P.info + 2) != CUSOLVER_STATUS_SUCCESS) {
-      set_last_error("cusolverDnDpotrs failed to launch", __FILE__, __LINE__);
-      return CG_ERR_SOLVER;
+    if (use_dense_custom(P.kc)) {
+      CG_TRY(dense_chol_solve(P.S, P.kc, P.work, P.rs, nrhs, st));
+    } else {
+      if (cusolverDnSetStream(h, st) != CUSOLVER_STATUS_SUCCESS) return CG_ERR_SOLVER;
+      if (cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, P.kc, nrhs, P.S, P.kc, P.rs, P.kc,
+                           P.info + 2) != CUSOLVER_STATUS_SUCCESS) {
+        set_last_error("cusolverDnDpotrs failed to launch", __FILE__, __LINE__);
+        return CG_ERR_SOLVER;
+      }
     }
   }
   { peel_backward_kernel<<<1, kPeelThreads, 0, st>>>(A.val, pp, P.rounds, P.d, P.y, P.rs, nrhs,
