@@ -111,14 +111,6 @@ def set_direction_solver(mode: str = "auto") -> None:
     _native.call("cg_splr_set_direction_solver", _DIRSOLVE[mode])
 
 
-def set_dense_factor(custom: bool = True) -> None:
-    """Dense FP64 Cholesky of the direction solve: this library's one-cluster
-    factorization and one-CTA triangular solves for orders up to 768 (default),
-    or cuSOLVER potrf / potrs everywhere (custom=False).  Results agree to
-    rounding."""
-    _native.call("cg_splr_set_dense_factor", 1 if custom else 0)
-
-
 def last_direction_solver() -> str | None:
     """Path of the last SPLR direction solve on this thread."""
     v = _native.lib().cg_splr_last_direction_solver()

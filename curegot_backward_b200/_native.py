@@ -129,7 +129,6 @@ SIGNATURES = {
     "cg_splr_f64": _SPLR_ARGS,
     "cg_splr_mixed": _SPLR_ARGS,
     "cg_splr_set_direction_solver": [c_int],
-    "cg_splr_set_dense_factor": [c_int],
     "cg_splr_last_direction_solver": [],
     "cg_ctx_info": [c_void_p, ctypes.POINTER(CtxInfo)],
     "cg_ctx_setup_diag": [c_void_p, c_void_p],

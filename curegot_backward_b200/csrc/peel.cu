@@ -27,9 +27,7 @@
 #include <cmath>
 
 #include "chol.cuh"
-#include "dense.cuh"
 #include "peel.cuh"
-#include "schur.cuh"
 
 namespace cg {
 
@@ -791,7 +789,6 @@ int peel_upload(PeelFactor& P, cusolverDnHandle_t h, cudaStream_t st, bool plan_
     set_last_error("cusolverDnDpotrf_bufferSize failed", __FILE__, __LINE__);
     return CG_ERR_SOLVER;
   }
-  if (!plan_only && kc > kSmallCore) lwork = std::max(lwork, kc);  // dense.cu's inverse diagonal
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   const size_t ib = al(P.h_ints.size() * sizeof(int));
   const size_t wb = al((size_t)std::max<long long>(P.ne_adj, 1) * 8);
@@ -851,7 +848,6 @@ int peel_factor(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, cudaStream
       { peel_assemble_kernel<<<P.kc, 256, 0, st>>>(A.val, pp, P.d, P.kc, P.S); count_launch(); }
     }
     CG_TRY_CUDA(cudaGetLastError());
-    if (use_dense_custom(P.kc)) return dense_chol_factor(P.S, P.kc, P.work, P.info, st);
     if (cusolverDnSetStream(h, st) != CUSOLVER_STATUS_SUCCESS) return CG_ERR_SOLVER;
     if (cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, P.kc, P.S, P.kc, P.work, P.lwork, P.info) !=
         CUSOLVER_STATUS_SUCCESS) {
@@ -882,15 +878,11 @@ int peel_solve(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, const doubl
                                                     P.kc, P.y, P.rs); count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
   if (P.kc > 0) {
-    if (use_dense_custom(P.kc)) {
-      CG_TRY(dense_chol_solve(P.S, P.kc, P.work, P.rs, nrhs, st));
-    } else {
-      if (cusolverDnSetStream(h, st) != CUSOLVER_STATUS_SUCCESS) return CG_ERR_SOLVER;
-      if (cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, P.kc, nrhs, P.S, P.kc, P.rs, P.kc,
-                           P.info + 2) != CUSOLVER_STATUS_SUCCESS) {
-        set_last_error("cusolverDnDpotrs failed to launch", __FILE__, __LINE__);
-        return CG_ERR_SOLVER;
-      }
+    if (cusolverDnSetStream(h, st) != CUSOLVER_STATUS_SUCCESS) return CG_ERR_SOLVER;
+    if (cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, P.kc, nrhs, P.S, P.kc, P.rs, P.kc,
+                         P.info + 2) != CUSOLVER_STATUS_SUCCESS) {
+      set_last_error("cusolverDnDpotrs failed to launch", __FILE__, __LINE__);
+      return CG_ERR_SOLVER;
     }
   }
   { peel_backward_kernel<<<1, kPeelThreads, 0, st>>>(A.val, pp, P.rounds, P.d, P.y, P.rs, nrhs,

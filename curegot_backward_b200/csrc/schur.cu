@@ -10,17 +10,12 @@
 // exactly and the Schur complement (size min(n, m-1)) is factored densely:
 //     S = D2 - B D1^{-1} B^T   (n >= m-1)   or   S = D1 - B^T D2^{-1} B.
 // S is assembled deterministically (one CTA per row of S, contributions in
-// CSR order, distinct targets per step) and factored in FP64 -- by the
-// one-cluster factorization of dense.cu for k <= kDenseMaxK, by cuSOLVER
-// potrf above; the solves are the matching triangular solves plus two sparse
-// sweeps.  The result is the same linear-algebra object the reference
-// computes (A^{-1} b), to rounding.
-#include <algorithm>
-#include <atomic>
+// CSR order, distinct targets per step) and factored with cuSOLVER potrf in
+// FP64; the solves are potrs plus two sparse sweeps.  The result is the same
+// linear-algebra object the reference computes (A^{-1} b), to rounding.
 #include <mutex>
 #include <unordered_map>
 
-#include "dense.cuh"
 #include "schur.cuh"
 
 namespace cg {
@@ -38,15 +33,8 @@ int schur_lwork(cusolverDnHandle_t h, int k, int& lwork) {
     set_last_error("cusolverDnDpotrf_bufferSize failed", __FILE__, __LINE__);
     return CG_ERR_SOLVER;
   }
-  lwork = std::max(lwork, k);  // also holds the inverse diagonal of dense_chol_factor
   return CG_OK;
 }
-
-namespace {
-std::atomic<int> g_dense_custom{1};
-}
-void set_dense_custom(bool on) { g_dense_custom.store(on ? 1 : 0); }
-bool use_dense_custom(int k) { return g_dense_custom.load() != 0 && dense_chol_fits(k); }
 
 int solver_handle(cusolverDnHandle_t* out) {
   thread_local std::unordered_map<int, cusolverDnHandle_t> handles;
@@ -193,7 +181,6 @@ int schur_factor(cusolverDnHandle_t h, const SpHess& A, SchurFactor& F, cudaStre
     { assemble_big_beta<<<F.k, 256, 0, st>>>(A.val, A.col, A.rowptr, A.ipt, A.ij, A.iv, A.n, F.k,
                                            F.S); cg::count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
-  if (use_dense_custom(F.k)) return dense_chol_factor(F.S, F.k, F.work, F.info, st);
   if (cusolverDnSetStream(h, st) != CUSOLVER_STATUS_SUCCESS) return CG_ERR_SOLVER;
   if (cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, F.k, F.S, F.k, F.work, F.lwork, F.info) !=
       CUSOLVER_STATUS_SUCCESS) {
@@ -211,15 +198,11 @@ int schur_solve(cusolverDnHandle_t h, const SpHess& A, const SchurFactor& F, con
     { reduce_rhs_kernel<<<std::max(1, std::min((k + 7) / 8, 148 * 8)), 256, 0, st>>>(
         mode, A.val, A.col, A.rowptr, A.ipt, A.ij, A.iv, A.n, A.H, k, rhs, nrhs, tmp); cg::count_launch(); }
     CG_TRY_CUDA(cudaGetLastError());
-    if (use_dense_custom(k)) {
-      CG_TRY(dense_chol_solve(F.S, k, F.work, tmp, nrhs, st));
-    } else {
-      if (cusolverDnSetStream(h, st) != CUSOLVER_STATUS_SUCCESS) return CG_ERR_SOLVER;
-      if (cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, k, nrhs, F.S, k, tmp, k, F.solve_info) !=
-          CUSOLVER_STATUS_SUCCESS) {
-        set_last_error("cusolverDnDpotrs failed to launch", __FILE__, __LINE__);
-        return CG_ERR_SOLVER;
-      }
+    if (cusolverDnSetStream(h, st) != CUSOLVER_STATUS_SUCCESS) return CG_ERR_SOLVER;
+    if (cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, k, nrhs, F.S, k, tmp, k, F.solve_info) !=
+        CUSOLVER_STATUS_SUCCESS) {
+      set_last_error("cusolverDnDpotrs failed to launch", __FILE__, __LINE__);
+      return CG_ERR_SOLVER;
     }
   }
   const int big = F.big_alpha ? A.n : (A.m - 1);

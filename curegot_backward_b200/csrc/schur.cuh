@@ -22,11 +22,6 @@ struct SchurFactor {
 // Schur dimension and potrf workspace size (doubles) for an (n, m) problem.
 void schur_dims(int n, int m, int& k, bool& big_alpha);
 int schur_lwork(cusolverDnHandle_t h, int k, int& lwork);
-// Dense factor / solve of Schur complements (and of large peel cores): the
-// cluster factorization of dense.cu when on (default) and k fits, else
-// cuSOLVER potrf / potrs.
-void set_dense_custom(bool on);
-bool use_dense_custom(int k);
 
 // cuSOLVER handle for the calling thread and current device (created once).
 int solver_handle(cusolverDnHandle_t* out);

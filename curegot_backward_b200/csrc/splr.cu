@@ -1252,11 +1252,6 @@ int cg_splr_set_direction_solver(int mode) {
 
 int cg_splr_last_direction_solver(void) { return cg::g_last_dir; }
 
-int cg_splr_set_dense_factor(int custom) {
-  cg::set_dense_custom(custom != 0);
-  return CG_OK;
-}
-
 int cg_test_inject_failure(int what, int count) {
   if (what != CG_INJECT_DIRECTION_SOLVE || count < 0) {
     cg::set_last_error("cg_test_inject_failure: unknown failure kind or negative count", __FILE__,

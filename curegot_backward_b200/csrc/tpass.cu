@@ -20,6 +20,7 @@
 
 #include "bcd.cuh"
 #include "bulk.cuh"
+#include "lse.cuh"
 #include "tpass.cuh"
 
 namespace cg {
@@ -74,7 +75,7 @@ __device__ __forceinline__ Slot slot_of(const TPassArgs& A, int k) {
 // finishers' reductions are exactly those of a one-point pass at step k, in
 // the same order, so slot k is bitwise what a one-point pass would give.
 template <typename TM, int K>
-__global__ void __launch_bounds__(kThreads, (K == 1) ? 3 : 2) tpass_kernel(const TPassArgs A) {
+__global__ void __launch_bounds__(kThreads, 2) tpass_kernel(const TPassArgs A) {
   constexpr int VN = TLayout<TM>::VN, NV = TLayout<TM>::NV;
   constexpr int VS = 32 * VN;  // column stride between a lane's vectors
   __shared__ double tab[kExp2TableSize];
@@ -125,43 +126,73 @@ __global__ void __launch_bounds__(kThreads, (K == 1) ? 3 : 2) tpass_kernel(const
       const int ip = r0 + warp + k * kWarps;
       if (ip < r1) prefetch_l2_bulk(M + (size_t)ip * m + c0, seg_bytes);
     }
-  for (int i = r0 + warp; i < r1; i += kWarps) {
-    if (pf > 0 && lane == 0) {
-      const int ip = i + pf * kWarps;
-      if (ip < r1) prefetch_l2_bulk(M + (size_t)ip * m + c0, seg_bytes);
-    }
+  // One row's contribution: T for this lane's columns and every point, the
+  // row sums reduced over the warp, the column sums kept in registers.
+  auto row_body = [&](int i, const double (&mv)[NV][VN]) {
     double as[K], rsum[K];
 #pragma unroll
     for (int p = 0; p < K; ++p) {
       as[p] = point_alpha(A, i, stp[p]) * s2;
       rsum[p] = 0.0;
     }
-    const TM* __restrict__ Mi = M + (size_t)i * m;
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      const int jb = c0 + v * VS + lane * VN;
-      double mv[VN];
-      if (vec_ok && jb + VN <= m) {
-        Vec<TM>::load(Mi + jb, mv);
-      } else {
-#pragma unroll
-        for (int k = 0; k < VN; ++k) mv[k] = (jb + k < m) ? ld1(Mi + jb + k) : 0.0;
-      }
+    for (int v = 0; v < NV; ++v)
 #pragma unroll
       for (int k = 0; k < VN; ++k) {
         const int q = v * VN + k;
 #pragma unroll
         for (int p = 0; p < K; ++p) {
-          const double T = cin[q] ? exp2_f64(fma(-mv[k], s2, as[p] + bs[p][q]), tab) : 0.0;
+          const double T = cin[q] ? exp2_f64(fma(-mv[v][k], s2, as[p] + bs[p][q]), tab) : 0.0;
           rsum[p] += T;
           cacc[p][q] += T;
         }
       }
-    }
 #pragma unroll
     for (int p = 0; p < K; ++p) {
       const double r = warp_sum_down(rsum[p]);
       if (lane == 0) slot_of(A, p).rowpart[(size_t)strip * n + i] = r;
+    }
+  };
+  if (vec_ok && c0 + kTStrip <= m) {
+    // full strip, aligned vectors: the next row's vectors are loaded before
+    // this row is processed (two rows of M in flight per warp)
+    using RT = typename Raw<TM>::T;
+    RT nxt[NV];
+    auto load_row = [&](int i) {
+      const TM* __restrict__ Mi = M + (size_t)i * m + c0 + lane * VN;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) nxt[v] = Raw<TM>::load(Mi + v * VS);
+    };
+    int i = r0 + warp;
+    if (i < r1) load_row(i);
+    for (; i < r1; i += kWarps) {
+      if (pf > 0 && lane == 0) {
+        const int ip = i + pf * kWarps;
+        if (ip < r1) prefetch_l2_bulk(M + (size_t)ip * m + c0, seg_bytes);
+      }
+      double mv[NV][VN];
+#pragma unroll
+      for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int k = 0; k < VN; ++k) mv[v][k] = Raw<TM>::get(nxt[v], k);
+      if (i + kWarps < r1) load_row(i + kWarps);
+      row_body(i, mv);
+    }
+  } else {
+    for (int i = r0 + warp; i < r1; i += kWarps) {
+      const TM* __restrict__ Mi = M + (size_t)i * m;
+      double mv[NV][VN];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        const int jb = c0 + v * VS + lane * VN;
+        if (vec_ok && jb + VN <= m) {
+          Vec<TM>::load(Mi + jb, mv[v]);
+        } else {
+#pragma unroll
+          for (int k = 0; k < VN; ++k) mv[v][k] = (jb + k < m) ? ld1(Mi + jb + k) : 0.0;
+        }
+      }
+      row_body(i, mv);
     }
   }
 #pragma unroll

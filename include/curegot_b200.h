@@ -244,15 +244,6 @@ enum { CG_DIRSOLVE_AUTO = 0, CG_DIRSOLVE_DENSE = 1, CG_DIRSOLVE_SPARSE = 2, CG_D
 int cg_splr_set_direction_solver(int mode);
 int cg_splr_last_direction_solver(void);
 
-/*
- * Dense FP64 Cholesky factor / solve used by the dense Schur path and by peel
- * cores above 160 nodes: custom != 0 (default) takes the one-cluster
- * factorization and one-CTA triangular solves of this library for orders up
- * to 768, custom = 0 takes cuSOLVER potrf / potrs everywhere.  Both are exact
- * Cholesky solves; results agree to rounding.  Process-wide.  No reference
- * counterpart (the reference factors the sparse Hessian with cuDSS).
- */
-int cg_splr_set_dense_factor(int custom);
 
 /* Context properties (reg, dim, low_rank_enabled, is_fallback, ...;
  * src/solvers_torch.cpp:691-696). */

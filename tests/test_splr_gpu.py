@@ -242,26 +242,3 @@ def test_peel_large_core_rowwise_assembly(cuda_dev, dirsolver):
     ref = oracle.splr(M, a, b, 0.02, tol=1e-8, max_iter=300, density=0.1)
     assert got["niter"] == ref["niter"]
     assert np.abs(got["dual"] - ref["dual"]).max() <= 1e-10 * np.abs(ref["dual"]).max()
-
-
-@pytest.mark.parametrize("n,m,reg", [(700, 421, 0.02), (130, 900, 0.05), (40, 34, 0.05),
-                                     (1000, 770, 0.05)])
-def test_dense_factor_custom_matches_cusolver(cuda_dev, dirsolver, n, m, reg):
-    """The dense Schur path with this library's cluster Cholesky (orders up to
-    768: k = 420, 130, 33 here) and with cuSOLVER potrf / potrs: the same
-    iterates and decisions, duals within 1e-10 relative.  (1000, 770): k = 769
-    is above the cluster limit, so both settings take cuSOLVER."""
-    dirsolver("dense")
-    M, a, b = problem(n, m, n + 7 * m, "gauss")
-    out = {}
-    try:
-        for custom in (True, False):
-            cg.set_dense_factor(custom)
-            out[custom] = cg.numpy.sinkhorn_splr(M, a, b, reg, tol=1e-8, max_iter=300,
-                                                 return_trace=True, density=0.1)
-    finally:
-        cg.set_dense_factor(True)
-    g, r = out[True], out[False]
-    assert g["niter"] == r["niter"]
-    np.testing.assert_array_equal(g["trace"][:, [3, 4, 5, 6, 7]], r["trace"][:, [3, 4, 5, 6, 7]])
-    assert np.abs(g["dual"] - r["dual"]).max() <= 1e-10 * np.abs(r["dual"]).max()
