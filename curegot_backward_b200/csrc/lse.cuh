@@ -127,13 +127,24 @@ __device__ __forceinline__ void lse_chunk_full(const double (&d)[K], double& mx,
   }
 }
 
+// Raw 16-byte vector of M.  M is streamed once per pass, so its loads do not
+// allocate in L1 (read-only path, L1::no_allocate): L1 stays with the dual
+// vectors the passes re-read for every row.
 template <typename TM>
-struct Raw;  // raw 16-byte vector of M
+struct Raw;
 template <>
 struct Raw<double> {
   using T = double2;
   __device__ __forceinline__ static T load(const double* p) {
+#ifdef CG_M_L1_ALLOCATE
     return __ldg(reinterpret_cast<const double2*>(p));
+#else
+    T v;
+    asm("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];"
+                 : "=d"(v.x), "=d"(v.y)
+                 : "l"(p));
+    return v;
+#endif
   }
   __device__ __forceinline__ static double get(const T& v, int k) { return k == 0 ? v.x : v.y; }
 };
@@ -141,7 +152,15 @@ template <>
 struct Raw<float> {
   using T = float4;
   __device__ __forceinline__ static T load(const float* p) {
+#ifdef CG_M_L1_ALLOCATE
     return __ldg(reinterpret_cast<const float4*>(p));
+#else
+    T v;
+    asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "l"(p));
+    return v;
+#endif
   }
   __device__ __forceinline__ static double get(const T& v, int k) {
     return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
