@@ -50,6 +50,7 @@ WORKLOAD = ("serving stream: n,m log-uniform [64,8192], d in {8,32}, Gaussian cl
             "eta in {0.1,0.05,0.01}, 70% BCD / 30% SPLR, tol 1e-8, uniform marginals")
 SPLR_WORKERS = 32
 IN_FLIGHT = 24
+CHUNK = 8
 
 
 def parse():
@@ -67,6 +68,7 @@ def parse():
     p.add_argument("--budget-gb", type=float, default=120.0)
     p.add_argument("--seed", type=int, default=4)
     p.add_argument("--splr-workers", type=int, default=SPLR_WORKERS)
+    p.add_argument("--chunk", type=int, default=CHUNK, help="Sinkhorn ticks per graph launch")
     p.add_argument("--in-flight", type=int, default=IN_FLIGHT,
                    help="saturation: requests kept in flight by the closed-loop client")
     return p.parse_args()
@@ -493,7 +495,7 @@ def main():
     dev = torch.device("cuda", local if world > 1 else 0)
     _native.lib().cg_launch_count_reset()
     eng = OTEngine(budget_bytes=args.budget_gb * 1e9, max_batch=64, splr_workers=args.splr_workers,
-                   chunk=8)
+                   chunk=args.chunk)
 
     # warm-up steps (untimed): device inputs, and host inputs for the e2e pass
     for st in range(args.warmup):
@@ -527,7 +529,7 @@ def main():
     gms = s1["bcd_gpu_ms"] - s0["bcd_gpu_ms"]
     peak, peak_kind = measured_hbm_peak()
     achieved = bytes_ / (gms / 1000.0) / 1e9 if gms > 0 else 0.0
-    launches_per_chunk = 2 * 8
+    launches_per_chunk = 2 * args.chunk
     n_chunks = s1["chunks"] - s0["chunks"]
 
     # e2e: host inputs, copies inside the timed region
@@ -592,7 +594,7 @@ def main():
                                     f"{args.in_flight} in flight"),
                        "l2": "inputs larger than L2 (each step streams > 126 MB of M)",
                        "engine": f"max_batch 64, up to {args.splr_workers} SPLR solves in flight on "
-                                 f"{(args.splr_workers + 7) // 8} scheduler threads, 8 ticks per graph launch",
+                                 f"{(args.splr_workers + 7) // 8} scheduler threads, {args.chunk} ticks per graph launch",
                        "parallelism": f"replicas x{world}"},
             "latency_ms": {"p50": float(np.percentile(lat, 50)),
                            "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},

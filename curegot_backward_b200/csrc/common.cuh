@@ -144,30 +144,40 @@ __device__ __forceinline__ double cta_sum(double v, double* red /* >= kWarps */)
 // Vector loads of row-major cost matrices.
 template <typename TM>
 struct Vec;
+// Vector and scalar loads of streamed matrices (M, T, G): read-only path,
+// no L1 allocation (each element is read once per pass; L1 is left to the
+// dual and index vectors that are re-read).
 template <>
 struct Vec<double> {
   static constexpr int N = 2;
   __device__ __forceinline__ static void load(const double* p, double* out) {
-    const double2 v = __ldg(reinterpret_cast<const double2*>(p));
-    out[0] = v.x;
-    out[1] = v.y;
+    asm("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(out[0]), "=d"(out[1]) : "l"(p));
   }
 };
 template <>
 struct Vec<float> {
   static constexpr int N = 4;
   __device__ __forceinline__ static void load(const float* p, double* out) {
-    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
-    out[0] = v.x;
-    out[1] = v.y;
-    out[2] = v.z;
-    out[3] = v.w;
+    float x, y, z, w;
+    asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+        : "=f"(x), "=f"(y), "=f"(z), "=f"(w)
+        : "l"(p));
+    out[0] = x;
+    out[1] = y;
+    out[2] = z;
+    out[3] = w;
   }
 };
 
-template <typename TM>
-__device__ __forceinline__ double ld1(const TM* p) {
-  return static_cast<double>(__ldg(p));
+__device__ __forceinline__ double ld1(const double* p) {
+  double v;
+  asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double ld1(const float* p) {
+  float v;
+  asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return static_cast<double>(v);
 }
 
 // Load VN consecutive FP64 duals (16-byte aligned when VN >= 2).
