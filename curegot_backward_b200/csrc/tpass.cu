@@ -308,9 +308,13 @@ __global__ void __launch_bounds__(kThreads, 2) tpass_kernel(const TPassArgs A) {
   }
 }
 
+// strips x splits CTAs, at most 2 per SM (the two-point trial kernel's
+// occupancy): one full wave.  Rounding the split count up instead left a few
+// CTAs for a second wave, which doubled the pass time (e.g. 16 strips x 19
+// splits = 304 CTAs on 296 slots).
 void tpass_geometry(int n, int m, int sm_count, int& strips, int& splits) {
   strips = (m + kTStrip - 1) / kTStrip;
-  int s = (2 * sm_count + strips - 1) / strips;
+  int s = (2 * sm_count) / strips;
   s = std::max(1, std::min(s, std::max(1, n / 64)));
   splits = s;
 }
