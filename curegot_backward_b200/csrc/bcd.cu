@@ -1169,28 +1169,6 @@ void bcd_geometry(int n, int m, int elem_bytes, int sm_count, BcdProb& p) {
     if (m < wpr * 32 * vn * kUnroll) break;
     R /= 2;
   }
-  // Wave quantization: with ctas CTAs on slots = kBcdMinBlocks per SM the
-  // pass takes ceil(ctas / slots) CTA durations.  Split rows over more warps
-  // (halving R) while that raises the filled fraction of the last wave by
-  // more than 5 % and each warp keeps a segment of at least 4096 elements
-  // (e.g. 4096 x 16384: 512 CTAs on 444 slots fill 58 %; R = 2 fills 92 %).
-  {
-    const int slots = kBcdMinBlocks * sm_count;
-    auto fill = [&](int r) {
-      const long long c = (n + r - 1) / r;
-      const long long waves = (c + slots - 1) / slots;
-      return (double)c / (double)(waves * slots);
-    };
-    double best = fill(R);
-    for (int r = R / 2; r >= 1; r /= 2) {
-      if (m / (kWarps / r) < 4096) break;
-      const double f = fill(r);
-      if (f > best + 0.05) {
-        best = f;
-        R = r;
-      }
-    }
-  }
   p.rows_per_cta = R;
   p.row_ctas = (n + R - 1) / R;
   // Column pass: 512-byte strips.

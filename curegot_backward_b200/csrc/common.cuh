@@ -284,6 +284,22 @@ __device__ __forceinline__ double exp2_f64(double x, const double* __restrict__ 
   return __hiloint2double(__double2hiint(y) + ((N >> kExp2Bits) << 20), __double2loint(y));
 }
 
+// exp2_f64 without branches: the same value for every x (bitwise), from the
+// table method on x clamped to [-1020, 1024] and selects for the arguments
+// outside [-1020, 1024) (0, +inf, NaN).  For loops over many elements, where
+// the two early returns of exp2_f64 cost branch and reconvergence code.
+__device__ __forceinline__ double exp2_f64_sel(double x, const double* __restrict__ tab) {
+  const double xc = fmin(fmax(x, -1020.0), 1024.0);
+  const double t = fma(xc, kExp2Scale, kExpMagic);
+  const int N = __double2loint(t);
+  const double kf = t - kExpMagic;
+  const double f = fma(kf, -kExp2InvScale, xc);
+  const double y = exp2_poly(f) * tab[N & (kExp2TableSize - 1)];
+  double r = __hiloint2double(__double2hiint(y) + ((N >> kExp2Bits) << 20), __double2loint(y));
+  r = (x >= 1024.0) ? INFINITY : r;
+  return (x >= -1020.0) ? r : ((x != x) ? x : 0.0);
+}
+
 // Non-positive-argument variant used inside the LSE passes (x <= 0 by
 // construction after the running-max shift): same method, no overflow branch.
 __device__ __forceinline__ double exp2_neg_f64(double x, const double* __restrict__ tab) {

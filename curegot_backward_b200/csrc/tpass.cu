@@ -128,7 +128,8 @@ __global__ void __launch_bounds__(kThreads, 2) tpass_kernel(const TPassArgs A) {
     }
   // One row's contribution: T for this lane's columns and every point, the
   // row sums reduced over the warp, the column sums kept in registers.
-  auto row_body = [&](int i, const double (&mv)[NV][VN]) {
+  // full: every column of the strip exists (no per-column predicate).
+  auto row_body = [&](int i, const double (&mv)[NV][VN], bool full) {
     double as[K], rsum[K];
 #pragma unroll
     for (int p = 0; p < K; ++p) {
@@ -142,7 +143,8 @@ __global__ void __launch_bounds__(kThreads, 2) tpass_kernel(const TPassArgs A) {
         const int q = v * VN + k;
 #pragma unroll
         for (int p = 0; p < K; ++p) {
-          const double T = cin[q] ? exp2_f64(fma(-mv[v][k], s2, as[p] + bs[p][q]), tab) : 0.0;
+          const double e = exp2_f64_sel(fma(-mv[v][k], s2, as[p] + bs[p][q]), tab);
+          const double T = (full || cin[q]) ? e : 0.0;
           rsum[p] += T;
           cacc[p][q] += T;
         }
@@ -176,7 +178,7 @@ __global__ void __launch_bounds__(kThreads, 2) tpass_kernel(const TPassArgs A) {
 #pragma unroll
         for (int k = 0; k < VN; ++k) mv[v][k] = Raw<TM>::get(nxt[v], k);
       if (i + kWarps < r1) load_row(i + kWarps);
-      row_body(i, mv);
+      row_body(i, mv, true);
     }
   } else {
     for (int i = r0 + warp; i < r1; i += kWarps) {
@@ -192,7 +194,7 @@ __global__ void __launch_bounds__(kThreads, 2) tpass_kernel(const TPassArgs A) {
           for (int k = 0; k < VN; ++k) mv[v][k] = (jb + k < m) ? ld1(Mi + jb + k) : 0.0;
         }
       }
-      row_body(i, mv);
+      row_body(i, mv, false);
     }
   }
 #pragma unroll
