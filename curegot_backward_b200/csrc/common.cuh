@@ -300,6 +300,23 @@ __device__ __forceinline__ double exp2_f64_sel(double x, const double* __restric
   return (x >= -1020.0) ? r : ((x != x) ? x : 0.0);
 }
 
+// exp2 for the plan pass, whose values only enter sums: the table method on x
+// clamped to [-1020, 1024] and one select for NaN.  Equal to exp2_f64 for x in
+// [-1020, 1024); +inf at or above 1024 (the clamped point 1024 assembles +inf
+// exactly); below -1020 it gives 2^-1020 instead of 0, which no FP64 sum of
+// the plan's magnitudes can see.
+__device__ __forceinline__ double exp2_f64_clamped(double x, const double* __restrict__ tab) {
+  const double xc = fmin(fmax(x, -1020.0), 1024.0);
+  const double t = fma(xc, kExp2Scale, kExpMagic);
+  const int N = __double2loint(t);
+  const double kf = t - kExpMagic;
+  const double f = fma(kf, -kExp2InvScale, xc);
+  const double y = exp2_poly(f) * tab[N & (kExp2TableSize - 1)];
+  const double r =
+      __hiloint2double(__double2hiint(y) + ((N >> kExp2Bits) << 20), __double2loint(y));
+  return (x != x) ? x : r;
+}
+
 // Non-positive-argument variant used inside the LSE passes (x <= 0 by
 // construction after the running-max shift): same method, no overflow branch.
 __device__ __forceinline__ double exp2_neg_f64(double x, const double* __restrict__ tab) {

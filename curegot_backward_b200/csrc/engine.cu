@@ -49,8 +49,14 @@ double now_s() {
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
-// SPLR solves multiplexed by one scheduler thread.
-constexpr int kSplrSlotsPerThread = 8;
+// SPLR solves multiplexed by one scheduler thread.  A solve's host-side
+// work (launches, and the sparsity-pattern planning of the direction solve
+// every 30 iterations, which runs inline) holds its thread, so fewer solves
+// per thread keep that from delaying the others.
+#ifndef CG_SPLR_SLOTS
+#define CG_SPLR_SLOTS 4
+#endif
+constexpr int kSplrSlotsPerThread = CG_SPLR_SLOTS;
 
 // Sinkhorn requests with at most this many bytes of M share the small batch.
 constexpr size_t kSmallBatchBytes = size_t(8) << 20;

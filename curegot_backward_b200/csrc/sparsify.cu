@@ -57,7 +57,7 @@ __device__ __forceinline__ Digit digit_of(int level) {
 template <typename TM>
 __device__ __forceinline__ double t_at(const TM* __restrict__ M, int i, int j, int m, double as,
                                        double bs, double s2, const double* tab) {
-  return fabs(exp2_f64(fma(-ld1(M + (size_t)i * m + j), s2, as + bs), tab));
+  return fabs(exp2_f64_sel(fma(-ld1(M + (size_t)i * m + j), s2, as + bs), tab));
 }
 
 __device__ __forceinline__ unsigned int flat_prime(int n, int H, int i, int j) {

@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(kThreads, 2) tpass_kernel(const TPassArgs A) {
         const int q = v * VN + k;
 #pragma unroll
         for (int p = 0; p < K; ++p) {
-          const double e = exp2_f64_sel(fma(-mv[v][k], s2, as[p] + bs[p][q]), tab);
+          const double e = exp2_f64_clamped(fma(-mv[v][k], s2, as[p] + bs[p][q]), tab);
           const double T = (full || cin[q]) ? e : 0.0;
           rsum[p] += T;
           cacc[p][q] += T;
