@@ -594,7 +594,7 @@ def main():
                                     f"{args.in_flight} in flight"),
                        "l2": "inputs larger than L2 (each step streams > 126 MB of M)",
                        "engine": f"max_batch 64, up to {args.splr_workers} SPLR solves in flight on "
-                                 f"{(args.splr_workers + 3) // 4} scheduler threads, {args.chunk} ticks per graph launch",
+                                 f"{(args.splr_workers + 7) // 8} scheduler threads, {args.chunk} ticks per graph launch",
                        "parallelism": f"replicas x{world}"},
             "latency_ms": {"p50": float(np.percentile(lat, 50)),
                            "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},

@@ -49,12 +49,10 @@ double now_s() {
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
-// SPLR solves multiplexed by one scheduler thread.  A solve's host-side
-// work (launches, and the sparsity-pattern planning of the direction solve
-// every 30 iterations, which runs inline) holds its thread, so fewer solves
-// per thread keep that from delaying the others.
+// SPLR solves multiplexed by one scheduler thread (2 and 4 per thread were
+// measured no better on the serving stream).
 #ifndef CG_SPLR_SLOTS
-#define CG_SPLR_SLOTS 4
+#define CG_SPLR_SLOTS 8
 #endif
 constexpr int kSplrSlotsPerThread = CG_SPLR_SLOTS;
 
