@@ -569,11 +569,7 @@ void peel_release(PeelFactor& P) {
 }
 
 int peel_plan(PeelFactor& P, const SpHess& A, cudaStream_t st, bool no_peel) {
-  const int n = A.n, m = A.m, H = A.H;
-  P.ready = false;
-  P.n = n;
-  P.m = m;
-  P.H = H;
+  const int H = A.H;
   // pattern to the host through pinned memory (pageable copies serialise
   // with the other streams' work)
   std::vector<int> rp(H + 1);
@@ -581,6 +577,16 @@ int peel_plan(PeelFactor& P, const SpHess& A, cudaStream_t st, bool no_peel) {
   const int nl = rp[H];
   std::vector<int> cl(std::max(nl, 1));
   CG_TRY(read_device_bulk(cl.data(), A.col, (size_t)nl * sizeof(int), st));
+  return peel_plan_host(P, A.n, A.m, rp, cl, no_peel);
+}
+
+int peel_plan_host(PeelFactor& P, int n, int m, const std::vector<int>& rp,
+                   const std::vector<int>& cl, bool no_peel) {
+  const int H = n + m - 1;
+  P.ready = false;
+  P.n = n;
+  P.m = m;
+  P.H = H;
 
   // diagonal positions and the bipartite adjacency (neighbour, value index)
   std::vector<int> diagq(H);

@@ -63,6 +63,11 @@ struct PeelFactor {
 // no_peel = true: no elimination rounds, the core is the whole graph -- the
 // contribution lists of the dense Schur complement (see peel_assemble_dense).
 int peel_plan(PeelFactor& P, const SpHess& A, cudaStream_t st, bool no_peel = false);
+// The host part of peel_plan, from the pattern already on the host (row
+// pointers rp[H + 1] and column indices cl of A's lower CSR).  No CUDA calls:
+// may run on any thread.
+int peel_plan_host(PeelFactor& P, int n, int m, const std::vector<int>& rp,
+                   const std::vector<int>& cl, bool no_peel = false);
 // Device buffers + upload of the plan (plan_only: the integer plan alone).
 int peel_upload(PeelFactor& P, cusolverDnHandle_t h, cudaStream_t st, bool plan_only = false);
 // Dense Schur complement S (k x k, the dense direction-solve path) assembled

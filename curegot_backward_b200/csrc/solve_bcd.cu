@@ -172,6 +172,8 @@ struct IoSlot {
   void* pinned;
   cudaEvent_t ev;
   int dev;
+  void* bulk;
+  size_t bulk_cap;
 };
 std::mutex g_io_mu;
 std::vector<IoSlot> g_io_free;
@@ -190,6 +192,8 @@ int TaskIO::init(cudaStream_t s) {
       if (g_io_free[k].dev == dev) {
         pinned = g_io_free[k].pinned;
         ev = g_io_free[k].ev;
+        bulk = g_io_free[k].bulk;
+        bulk_cap = g_io_free[k].bulk_cap;
         g_io_free.erase(g_io_free.begin() + k);
         return CG_OK;
       }
@@ -208,13 +212,28 @@ void TaskIO::release() {
   if (!pinned) return;
   int dev = 0;
   cudaGetDevice(&dev);
+  if (job_posted) {  // a task destroyed while its job runs: let the job finish
+    job.wait();
+    job_posted = false;
+  }
   std::lock_guard<std::mutex> lk(g_io_mu);
-  g_io_free.push_back({pinned, ev, dev});
+  g_io_free.push_back({pinned, ev, dev, bulk, bulk_cap});
   pinned = nullptr;
   ev = nullptr;
+  bulk = nullptr;
+  bulk_cap = 0;
 }
 
 int TaskIO::wait() {
+  if (job_posted) {
+    if (!t_wait_yield) {
+      job.wait();
+    } else {
+      while (job.wait_for(std::chrono::seconds(0)) != std::future_status::ready)
+        std::this_thread::yield();
+    }
+    return CG_OK;
+  }
   if (!posted) return CG_OK;
   if (!t_wait_yield) {
     CG_TRY_CUDA(cudaEventSynchronize(ev));
@@ -228,6 +247,32 @@ int TaskIO::wait() {
   }
 }
 
+TaskIO::Await TaskIO::read_spans_bulk(const ReadSpan* sp, int cnt) {
+  size_t total = 0;
+  for (int k = 0; k < cnt; ++k) total += sp[k].bytes;
+  if (cnt > kTaskMaxSpans) {
+    set_last_error("task read: too many spans", __FILE__, __LINE__);
+    err = CG_ERR_INVALID_ARG;
+    return Await{this};
+  }
+  if (total > bulk_cap) {  // no copy into bulk is pending: the task waits on each read
+    if (bulk) cudaFreeHost(bulk);
+    bulk = nullptr;
+    bulk_cap = 0;
+    const size_t cap = std::max<size_t>(total + total / 2, size_t(1) << 16);
+    const cudaError_t e = cudaHostAlloc(&bulk, cap, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+      bulk = nullptr;
+      set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
+      err = status_from_cuda(e);
+      return Await{this};
+    }
+    bulk_cap = cap;
+  }
+  use_bulk = true;
+  return post_reads(sp, cnt, static_cast<char*>(bulk));
+}
+
 TaskIO::Await TaskIO::read_spans(const ReadSpan* sp, int cnt) {
   size_t total = 0;
   for (int k = 0; k < cnt; ++k) total += sp[k].bytes;
@@ -236,8 +281,12 @@ TaskIO::Await TaskIO::read_spans(const ReadSpan* sp, int cnt) {
     err = CG_ERR_INVALID_ARG;
     return Await{this};
   }
+  use_bulk = false;
+  return post_reads(sp, cnt, static_cast<char*>(pinned));
+}
+
+TaskIO::Await TaskIO::post_reads(const ReadSpan* sp, int cnt, char* pin) {
   count = cnt;
-  char* pin = static_cast<char*>(pinned);
   size_t off = 0;
   for (int k = 0; k < cnt; ++k) {
     spans[k] = sp[k];

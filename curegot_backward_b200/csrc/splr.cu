@@ -774,6 +774,38 @@ SolveTask splr_task(TaskIO* io, const TM* M, const double* a, const double* b, d
     }
     return plan_dense();
   };
+  // The same plan from the pattern on the host, with no CUDA calls (runs off
+  // the driving thread): *want = 1 peel, 2 dense with contribution lists,
+  // 0 dense row-wise.  apply_plan uploads it on the solve's stream.
+  auto plan_host = [&](const std::vector<int>& rp, const std::vector<int>& cl,
+                       int* want) -> int {
+    *want = 0;
+    if (dir_mode != kDirDense) {
+      CG_TRY(peel_plan_host(*pf, n, m, rp, cl));
+      const bool fits = pf->rounds <= kMaxPeelRoundsUsed;
+      if (fits && (dir_mode == kDirPeel || 2 * pf->kc <= k || pf->kc <= kPeelSmallCore)) {
+        *want = 1;
+        return CG_OK;
+      }
+    }
+    if (k <= 0 || k > kPeelContribMax) return CG_OK;
+    CG_TRY(peel_plan_host(*pf, n, m, rp, cl, /*no_peel=*/true));
+    if (pf->contrib && pf->kc == k) *want = 2;
+    return CG_OK;
+  };
+  auto apply_plan = [&](int want) -> int {
+    path = kPathDense;
+    dense_planned = false;
+    if (want == 1) {
+      CG_TRY(peel_upload(*pf, sol, st));
+      path = kPathPeel;
+    } else if (want == 2) {
+      CG_TRY(peel_upload(*pf, sol, st, /*plan_only=*/true));
+      dense_planned = true;
+    }
+    pattern_new = false;
+    return CG_OK;
+  };
   // factor A (current values); *bad (host) = 1 when the sparse Cholesky met a
   // non-positive pivot.  The dense and peel paths report on the device
   // (read_factor_info after the next synchronization).
@@ -897,6 +929,21 @@ SolveTask splr_task(TaskIO* io, const TM* M, const double* a, const double* b, d
     // written by lowrank_kernel
     int sp_bad = 0;
     const int nrhs = (iter > 0) ? 2 : 1;
+    if (pattern_new && dir_mode != kDirSparse) {
+      // a new sparsity pattern: read it asynchronously and make the
+      // direction-solve plan (host graph work) off this thread, so a
+      // scheduler driving several solves keeps serving the others
+      const long long ncl = Kcur + H;
+      std::vector<int> prp((size_t)H + 1), pcl((size_t)std::max<long long>(ncl, 1));
+      const ReadSpan sp[2] = {{prp.data(), hb.A.rowptr, (size_t)(H + 1) * sizeof(int)},
+                              {pcl.data(), hb.A.col, (size_t)ncl * sizeof(int)}};
+      CO_TRY(co_await io->read_spans_bulk(sp, 2));
+      if (prp[H] == ncl) {  // else the blocking plan below reads it again
+        int want = 0;
+        CO_TRY(co_await io->run_job([&]() -> int { return plan_host(prp, pcl, &want); }));
+        CO_TRY(apply_plan(want));
+      }
+    }
     CO_TRY(factor_solve_direction(&sp_bad, hb.rhs2, hb.sol2, nrhs));
     g_last_dir = path;
     // Woodbury correction, scaling, <g, d>, and save_history (first H

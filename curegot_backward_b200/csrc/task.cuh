@@ -14,8 +14,11 @@
 // resuming whichever task's event has completed.
 #pragma once
 
+#include <chrono>
 #include <coroutine>
 #include <cstring>
+#include <functional>
+#include <future>
 
 #include "common.cuh"
 
@@ -34,12 +37,21 @@ struct TaskIO {
   int count = 0;
   int err = CG_OK;
   bool posted = false;
+  // larger reads (sparsity patterns) go through `bulk`, pinned, grown on
+  // demand and kept with the pooled buffer
+  void* bulk = nullptr;
+  size_t bulk_cap = 0;
+  bool use_bulk = false;
+  // host work run off the driving thread (run_job)
+  std::future<int> job;
+  bool job_posted = false;
 
   int init(cudaStream_t s);  // takes a buffer and an event from the pool
   void release();            // returns them (after the stream's work is done)
 
-  // True when nothing is pending or the posted copies have landed.
+  // True when nothing is pending or the posted copies / job have finished.
   bool ready() const {
+    if (job_posted) return job.wait_for(std::chrono::seconds(0)) == std::future_status::ready;
     if (!posted) return true;
     const cudaError_t q = cudaEventQuery(ev);
     return q != cudaErrorNotReady;
@@ -59,7 +71,7 @@ struct TaskIO {
       const cudaError_t q = cudaEventQuery(s.ev);
       if (q != cudaSuccess) return status_from_cuda(q == cudaErrorNotReady ? cudaEventSynchronize(s.ev) : q);
       size_t off = 0;
-      const char* pin = static_cast<const char*>(s.pinned);
+      const char* pin = static_cast<const char*>(s.use_bulk ? s.bulk : s.pinned);
       for (int k = 0; k < s.count; ++k) {
         if (s.spans[k].bytes) std::memcpy(s.spans[k].host, pin + off, s.spans[k].bytes);
         off += s.spans[k].bytes;
@@ -71,6 +83,27 @@ struct TaskIO {
   Await read(void* host, const void* dev, size_t bytes) {
     const ReadSpan one{host, dev, bytes};
     return read_spans(&one, 1);
+  }
+  // Any number of bytes, through `bulk` (grown on demand, outside the hot loop).
+  Await read_spans_bulk(const ReadSpan* sp, int cnt);
+  Await post_reads(const ReadSpan* sp, int cnt, char* pin);  // copies + event
+
+  // fn() on a separate thread; the task resumes with its status when it has
+  // returned.  fn must not touch the task's stream.
+  struct JobAwait {
+    TaskIO* io;
+    bool await_ready() const noexcept { return !io->job_posted; }
+    void await_suspend(std::coroutine_handle<>) const noexcept {}
+    int await_resume() const {
+      if (!io->job_posted) return io->err != CG_OK ? io->err : CG_ERR_CUDA;
+      io->job_posted = false;
+      return io->job.get();
+    }
+  };
+  JobAwait run_job(std::function<int()> fn) {
+    job = std::async(std::launch::async, std::move(fn));
+    job_posted = true;
+    return JobAwait{this};
   }
 };
 
