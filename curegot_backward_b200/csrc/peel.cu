@@ -74,23 +74,136 @@ PeelPtrs ptrs_of(const PeelFactor& P) {
   return p;
 }
 
+// Threads per node for a block-wide step over cnt nodes: the largest power
+// of two g <= 32 with cnt * g <= blockDim.x (1 once the nodes fill the
+// block).  A node's list (children, S-list, E-list) is then split over its g
+// lanes -- lane `sub` takes entries sub, sub + g, ... -- and the partial
+// sums meet in a shuffle tree, so a round with few nodes but long lists
+// (the core round: beta nodes holding dozens of peeled alpha leaves) does
+// not wait on one thread walking a list serially.  g depends only on cnt,
+// so the summation order is fixed for a given plan.
+__device__ __forceinline__ int group_width(int cnt) {
+  int g = 1;
+  while (g < 32 && cnt * (g * 2) <= (int)blockDim.x) g *= 2;
+  return g;
+}
+
+// Sum over the g lanes of a group (g a power of two <= 32; every lane of the
+// warp calls it).
+__device__ __forceinline__ double group_sum(double v, int g) {
+  for (int o = g >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Pivots (with_d) and forward values y = L^{-1} rhs (nrhs columns, stride H)
+// of the nodes of one round; every thread of the block calls it, and the
+// caller puts the round's barrier after it.  Node v's pivot is
+//   d_v = A_vv - sum over children ch of (a_ch,v / d_ch) a_ch,v
+// and its forward value y_v = rhs_v - sum (a_ch,v / d_ch) y_ch.
+// nrhs <= 2 is handled in one pass over the children.
+__device__ __forceinline__ void round_step(const double* __restrict__ val, const PeelPtrs& p,
+                                           int r, bool with_d, double* __restrict__ d,
+                                           const double* __restrict__ rhs, int nrhs, int H,
+                                           double* __restrict__ y, int* __restrict__ info) {
+  const int r0 = p.rptr[r], cnt = p.rptr[r + 1] - r0;
+  const int g = group_width(cnt), per = blockDim.x / g, sub = threadIdx.x & (g - 1);
+  for (int k0 = 0; k0 < cnt; k0 += per) {
+    const int k = k0 + (int)threadIdx.x / g;
+    const int v = k < cnt ? p.order[r0 + k] : -1;
+    const int q0 = v >= 0 ? p.cptr[v] : 0, q1 = v >= 0 ? p.cptr[v + 1] : 0;
+    if (nrhs <= 2) {
+      double sd = 0.0, s0 = 0.0, s1 = 0.0;
+      for (int q = q0 + sub; q < q1; q += g) {
+        const int ch = p.child[q];
+        const double a = val[p.childq[q]];
+        const double w = a / d[ch];
+        sd = fma(w, a, sd);
+        if (nrhs > 0) s0 = fma(w, y[ch], s0);
+        if (nrhs > 1) s1 = fma(w, y[(size_t)H + ch], s1);
+      }
+      if (with_d) sd = group_sum(sd, g);
+      if (nrhs > 0) s0 = group_sum(s0, g);
+      if (nrhs > 1) s1 = group_sum(s1, g);
+      if (v >= 0 && sub == 0) {
+        if (with_d) {
+          const double dv = val[p.diagq[v]] - sd;
+          d[v] = dv;
+          if (!(dv > 0.0) || !isfinite(dv)) info[1] = 1;
+        }
+        if (nrhs > 0) y[v] = rhs[v] - s0;
+        if (nrhs > 1) y[(size_t)H + v] = rhs[(size_t)H + v] - s1;
+      }
+    } else {
+      for (int c = 0; c < nrhs; ++c) {
+        const double* yc = y + (size_t)c * H;
+        double s = 0.0;
+        for (int q = q0 + sub; q < q1; q += g) {
+          const int ch = p.child[q];
+          s = fma(val[p.childq[q]] / d[ch], yc[ch], s);
+        }
+        s = group_sum(s, g);
+        if (v >= 0 && sub == 0) y[(size_t)c * H + v] = rhs[(size_t)c * H + v] - s;
+      }
+    }
+  }
+}
+
+// Core right-hand side reduced to the Schur side (kc core nodes t):
+//   z[c * kc + t] = y_{s_t} - sum over the S-list of t of (a_q / d_e) y_e.
+// Every thread calls it; no barrier inside.
+__device__ __forceinline__ void core_rhs_step(const double* __restrict__ val, const PeelPtrs& p,
+                                              const double* __restrict__ d,
+                                              const double* __restrict__ y, int nrhs, int H,
+                                              int kc, double* __restrict__ z) {
+  const int g = group_width(kc), per = blockDim.x / g, sub = threadIdx.x & (g - 1);
+  for (int k0 = 0; k0 < kc; k0 += per) {
+    const int t = k0 + (int)threadIdx.x / g;
+    const int q0 = t < kc ? p.sptr[t] : 0, q1 = t < kc ? p.sptr[t + 1] : 0;
+    for (int c = 0; c < nrhs; ++c) {
+      const double* yc = y + (size_t)c * H;
+      double s = 0.0;
+      for (int q = q0 + sub; q < q1; q += g) {
+        const int ev = p.enodes[p.sadj[q]];
+        s = fma(val[p.sq[q]] / d[ev], yc[ev], s);
+      }
+      s = group_sum(s, g);
+      if (t < kc && sub == 0) z[(size_t)c * kc + t] = yc[p.snodes[t]] - s;
+    }
+  }
+}
+
+// Core E-side back-substitution from the Schur-side solution zs (stride kc):
+//   x_e = (y_e - sum over the E-list of e of a_q zs_t) / d_e.
+// Every thread calls it; no barrier inside.
+__device__ __forceinline__ void core_back_step(const double* __restrict__ val, const PeelPtrs& p,
+                                               const double* __restrict__ d,
+                                               const double* __restrict__ y,
+                                               const double* __restrict__ zs, int nrhs, int H,
+                                               int kc, int ke, double* __restrict__ x) {
+  const int g = group_width(ke), per = blockDim.x / g, sub = threadIdx.x & (g - 1);
+  for (int k0 = 0; k0 < ke; k0 += per) {
+    const int e = k0 + (int)threadIdx.x / g;
+    const int q0 = e < ke ? p.eptr[e] : 0, q1 = e < ke ? p.eptr[e + 1] : 0;
+    for (int c = 0; c < nrhs; ++c) {
+      double s = 0.0;
+      for (int q = q0 + sub; q < q1; q += g) s = fma(val[p.eq[q]], zs[(size_t)c * kc + p.eadj[q]], s);
+      s = group_sum(s, g);
+      if (e < ke && sub == 0) {
+        const int ev = p.enodes[e];
+        x[(size_t)c * H + ev] = (y[(size_t)c * H + ev] - s) / d[ev];
+      }
+    }
+  }
+}
+
 
 // Pivots of every node, round by round; the core nodes come last (one round)
 // and receive their diagonal updated by their peeled children.
-__global__ void __launch_bounds__(kPeelThreads) peel_factor_kernel(
+__global__ void __launch_bounds__(kPeelThreads, 1) peel_factor_kernel(
     const double* __restrict__ val, PeelPtrs p, int rounds, double* __restrict__ d,
     int* __restrict__ info) {
   for (int r = 0; r <= rounds; ++r) {
-    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
-      const int v = p.order[idx];
-      double dv = val[p.diagq[v]];
-      for (int q = p.cptr[v]; q < p.cptr[v + 1]; ++q) {
-        const double a = val[p.childq[q]];
-        dv -= (a / d[p.child[q]]) * a;
-      }
-      d[v] = dv;
-      if (!(dv > 0.0) || !isfinite(dv)) info[1] = 1;
-    }
+    round_step(val, p, r, true, d, nullptr, 0, 0, nullptr, info);
     __syncthreads();
   }
 }
@@ -157,55 +270,25 @@ __global__ void dense_contrib_kernel(const double* __restrict__ val, PeelPtrs p,
 
 // Forward sweep (y = L^{-1} b over the peeled rounds and the core's own
 // children), then the reduction of the core right-hand side to the Schur side.
-__global__ void __launch_bounds__(kPeelThreads) peel_forward_kernel(
+__global__ void __launch_bounds__(kPeelThreads, 1) peel_forward_kernel(
     const double* __restrict__ val, PeelPtrs p, int rounds, const double* __restrict__ d,
     const double* __restrict__ rhs, int nrhs, int H, int kc, double* __restrict__ y,
     double* __restrict__ rs) {
   for (int r = 0; r <= rounds; ++r) {
-    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
-      const int v = p.order[idx];
-      for (int c = 0; c < nrhs; ++c) {
-        const double* yc = y + (size_t)c * H;
-        double yv = rhs[(size_t)c * H + v];
-        for (int q = p.cptr[v]; q < p.cptr[v + 1]; ++q) {
-          const int ch = p.child[q];
-          yv -= (val[p.childq[q]] / d[ch]) * yc[ch];
-        }
-        y[(size_t)c * H + v] = yv;
-      }
-    }
+    round_step(val, p, r, false, const_cast<double*>(d), rhs, nrhs, H, y, nullptr);
     __syncthreads();
   }
-  for (int t = threadIdx.x; t < kc; t += blockDim.x) {
-    const int s = p.snodes[t];
-    for (int c = 0; c < nrhs; ++c) {
-      const double* yc = y + (size_t)c * H;
-      double acc = yc[s];
-      for (int q = p.sptr[t]; q < p.sptr[t + 1]; ++q) {
-        const int ev = p.enodes[p.sadj[q]];
-        acc -= (val[p.sq[q]] / d[ev]) * yc[ev];
-      }
-      rs[(size_t)c * kc + t] = acc;
-    }
-  }
+  core_rhs_step(val, p, d, y, nrhs, H, kc, rs);
 }
 
 // Core back-substitution, then the backward sweep over the peeled rounds.
-__global__ void __launch_bounds__(kPeelThreads) peel_backward_kernel(
+__global__ void __launch_bounds__(kPeelThreads, 1) peel_backward_kernel(
     const double* __restrict__ val, PeelPtrs p, int rounds, const double* __restrict__ d,
     const double* __restrict__ y, const double* __restrict__ rs, int nrhs, int H, int kc,
     int ke, double* __restrict__ x) {
   for (int t = threadIdx.x; t < kc; t += blockDim.x)
     for (int c = 0; c < nrhs; ++c) x[(size_t)c * H + p.snodes[t]] = rs[(size_t)c * kc + t];
-  for (int e = threadIdx.x; e < ke; e += blockDim.x) {
-    const int ev = p.enodes[e];
-    for (int c = 0; c < nrhs; ++c) {
-      double acc = y[(size_t)c * H + ev];
-      for (int q = p.eptr[e]; q < p.eptr[e + 1]; ++q)
-        acc -= val[p.eq[q]] * rs[(size_t)c * kc + p.eadj[q]];
-      x[(size_t)c * H + ev] = acc / d[ev];
-    }
-  }
+  core_back_step(val, p, d, y, rs, nrhs, H, kc, ke, x);
   __syncthreads();
   for (int r = rounds - 1; r >= 0; --r) {
     for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
@@ -227,18 +310,7 @@ __device__ void dev_forward(const double* __restrict__ val, const PeelPtrs& p, i
                             const double* __restrict__ d, const double* __restrict__ rhs,
                             int nrhs, int H, double* __restrict__ y) {
   for (int r = 0; r <= rounds; ++r) {
-    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
-      const int v = p.order[idx];
-      for (int c = 0; c < nrhs; ++c) {
-        const double* yc = y + (size_t)c * H;
-        double yv = rhs[(size_t)c * H + v];
-        for (int q = p.cptr[v]; q < p.cptr[v + 1]; ++q) {
-          const int ch = p.child[q];
-          yv -= (val[p.childq[q]] / d[ch]) * yc[ch];
-        }
-        y[(size_t)c * H + v] = yv;
-      }
-    }
+    round_step(val, p, r, false, const_cast<double*>(d), rhs, nrhs, H, y, nullptr);
     __syncthreads();
   }
 }
@@ -247,18 +319,7 @@ __device__ void dev_forward(const double* __restrict__ val, const PeelPtrs& p, i
 __device__ void dev_core_rhs(const double* __restrict__ val, const PeelPtrs& p,
                              const double* __restrict__ d, const double* __restrict__ y,
                              int nrhs, int H, int kc, double* __restrict__ z) {
-  for (int t = threadIdx.x; t < kc; t += blockDim.x) {
-    const int s = p.snodes[t];
-    for (int c = 0; c < nrhs; ++c) {
-      const double* yc = y + (size_t)c * H;
-      double acc = yc[s];
-      for (int q = p.sptr[t]; q < p.sptr[t + 1]; ++q) {
-        const int ev = p.enodes[p.sadj[q]];
-        acc -= (val[p.sq[q]] / d[ev]) * yc[ev];
-      }
-      z[(size_t)c * kc + t] = acc;
-    }
-  }
+  core_rhs_step(val, p, d, y, nrhs, H, kc, z);
   __syncthreads();
 }
 
@@ -339,7 +400,7 @@ __device__ void dev_trisolve(const double* __restrict__ L, const double* __restr
 // continues with d = 1 (the last such column is reported).
 __device__ void dev_cholesky(double* __restrict__ S, double* __restrict__ idiag, int kc, int ld,
                              int* __restrict__ info) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
   for (int j0 = 0; j0 < kc; j0 += 32) {
     const int bw = min(32, kc - j0);
     if (warp == 0) warp_block_cholesky(S + (size_t)j0 * ld + j0, ld, bw, idiag + j0, j0, info);
@@ -399,15 +460,7 @@ __device__ void dev_backward(const double* __restrict__ val, const PeelPtrs& p, 
                              double* __restrict__ x) {
   for (int t = threadIdx.x; t < kc; t += blockDim.x)
     for (int c = 0; c < nrhs; ++c) x[(size_t)c * H + p.snodes[t]] = zc[(size_t)c * kc + t];
-  for (int e = threadIdx.x; e < ke; e += blockDim.x) {
-    const int ev = p.enodes[e];
-    for (int c = 0; c < nrhs; ++c) {
-      double acc = y[(size_t)c * H + ev];
-      for (int q = p.eptr[e]; q < p.eptr[e + 1]; ++q)
-        acc -= val[p.eq[q]] * zc[(size_t)c * kc + p.eadj[q]];
-      x[(size_t)c * H + ev] = acc / d[ev];
-    }
-  }
+  core_back_step(val, p, d, y, zc, nrhs, H, kc, ke, x);
   __syncthreads();
   for (int r = rounds - 1; r >= 0; --r) {
     for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
@@ -427,7 +480,7 @@ __device__ void dev_backward(const double* __restrict__ val, const PeelPtrs& p, 
 // solve x = A^{-1} rhs.  Dynamic shared memory: kc*ld + 3*kc doubles (ld =
 // core_ld(kc), the shared row stride of the core matrix; then 2 kc for the
 // reduced right-hand sides and kc for the inverse diagonal of the factor).
-__global__ void __launch_bounds__(kPeelThreads) peel_fused_kernel(
+__global__ void __launch_bounds__(kPeelThreads, 1) peel_fused_kernel(
     const double* __restrict__ val, PeelPtrs p, int rounds, int kc, int ke, int H,
     const double* __restrict__ rhs, int nrhs, double* __restrict__ x, double* __restrict__ d,
     double* __restrict__ y, double* __restrict__ Lout, int* __restrict__ info,
@@ -439,31 +492,18 @@ __global__ void __launch_bounds__(kPeelThreads) peel_fused_kernel(
   double* idiag = z + 2 * (size_t)kc;
   // pivots and forward values, round by round (core last)
   for (int r = 0; r <= rounds; ++r) {
-    for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
-      const int v = p.order[idx];
-      double dv = val[p.diagq[v]];
-      double y0 = nrhs > 0 ? rhs[v] : 0.0, y1 = nrhs > 1 ? rhs[(size_t)H + v] : 0.0;
-      for (int q = p.cptr[v]; q < p.cptr[v + 1]; ++q) {
-        const int ch = p.child[q];
-        const double a = val[p.childq[q]];
-        const double w = a / d[ch];
-        dv -= w * a;
-        if (nrhs > 0) y0 -= w * y[ch];
-        if (nrhs > 1) y1 -= w * y[(size_t)H + ch];
-      }
-      d[v] = dv;
-      if (nrhs > 0) y[v] = y0;
-      if (nrhs > 1) y[(size_t)H + v] = y1;
-      if (!(dv > 0.0) || !isfinite(dv)) info[1] = 1;
-    }
+    round_step(val, p, r, true, d, rhs, nrhs, H, y, info);
     __syncthreads();
   }
   if (kc > 0 && p.ccp != nullptr) {
-    // edge weights, then the core Schur complement from the contribution
-    // lists, one thread per entry
-    for (int e = threadIdx.x; e < ke; e += blockDim.x) {
-      const double de = d[p.enodes[e]];
-      for (int q = p.eptr[e]; q < p.eptr[e + 1]; ++q) W[q] = val[p.eq[q]] / de;
+    // edge weights (a node's E-list split over a lane group), then the core
+    // Schur complement from the contribution lists, one thread per entry
+    {
+      const int g = group_width(ke), per = blockDim.x / g, sub = threadIdx.x & (g - 1);
+      for (int e = (int)threadIdx.x / g; e < ke; e += per) {
+        const double rde = 1.0 / d[p.enodes[e]];
+        for (int q = p.eptr[e] + sub; q < p.eptr[e + 1]; q += g) W[q] = val[p.eq[q]] * rde;
+      }
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < kc * kc; idx += blockDim.x) {
@@ -508,7 +548,7 @@ __global__ void __launch_bounds__(kPeelThreads) peel_fused_kernel(
 }
 
 // Solve with a stored small-core factor (pivots d, L in global memory).
-__global__ void __launch_bounds__(kPeelThreads) peel_small_solve_kernel(
+__global__ void __launch_bounds__(kPeelThreads, 1) peel_small_solve_kernel(
     const double* __restrict__ val, PeelPtrs p, int rounds, int kc, int ke, int H,
     const double* __restrict__ rhs, int nrhs, double* __restrict__ x,
     const double* __restrict__ d, double* __restrict__ y, const double* __restrict__ Lin) {
