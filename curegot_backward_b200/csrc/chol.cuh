@@ -1,5 +1,5 @@
-// Warp-level Cholesky of a small diagonal block, shared by the in-shared-
-// memory factorizations (peel.cu small cores, dense.cu panels).
+// Warp-level Cholesky of a small diagonal block, used by the in-shared-
+// memory factorization of the small peel cores (peel.cu).
 #pragma once
 
 #include "common.cuh"

@@ -38,7 +38,7 @@ constexpr int kPeelThreads = 1024;
 constexpr int kSmallCore = kPeelSmallCore;  // in-shared-memory Cholesky
 
 struct PeelPtrs {
-  const int *order, *rptr, *diagq, *cptr, *child, *childq, *par, *parq;
+  const int *order, *rptr, *hcnt, *diagq, *cptr, *child, *childq, *par, *parq;
   const int *snodes, *enodes, *sptr, *sadj, *sq, *eptr, *eadj, *eq;
   // contribution lists of the core Schur complement (entry t * kc + t2):
   // eliminated node ce, E-list position cw of the edge (ce, t) (its weight
@@ -53,6 +53,7 @@ PeelPtrs ptrs_of(const PeelFactor& P) {
   PeelPtrs p;
   p.order = b + P.off_order;
   p.rptr = b + P.off_rptr;
+  p.hcnt = b + P.off_hcnt;
   p.diagq = b + P.off_diagq;
   p.cptr = b + P.off_cptr;
   p.child = b + P.off_child;
@@ -95,56 +96,77 @@ __device__ __forceinline__ double group_sum(double v, int g) {
   return v;
 }
 
-// Pivots (with_d) and forward values y = L^{-1} rhs (nrhs columns, stride H)
-// of the nodes of one round; every thread of the block calls it, and the
-// caller puts the round's barrier after it.  Node v's pivot is
+// Pivot (with_d) and forward values y = L^{-1} rhs (nrhs columns, stride H)
+// of node v (v < 0: none), its child list split over the g lanes of a group
+// (this lane is `sub`; every lane of the warp calls it).  Node v's pivot is
 //   d_v = A_vv - sum over children ch of (a_ch,v / d_ch) a_ch,v
 // and its forward value y_v = rhs_v - sum (a_ch,v / d_ch) y_ch.
 // nrhs <= 2 is handled in one pass over the children.
+__device__ __forceinline__ void node_step(const double* __restrict__ val, const PeelPtrs& p,
+                                          int v, int sub, int g, bool with_d,
+                                          double* __restrict__ d, const double* __restrict__ rhs,
+                                          int nrhs, int H, double* __restrict__ y,
+                                          int* __restrict__ info) {
+  const int q0 = v >= 0 ? p.cptr[v] : 0, q1 = v >= 0 ? p.cptr[v + 1] : 0;
+  if (nrhs <= 2) {
+    double sd = 0.0, s0 = 0.0, s1 = 0.0;
+    for (int q = q0 + sub; q < q1; q += g) {
+      const int ch = p.child[q];
+      const double a = val[p.childq[q]];
+      const double w = a / d[ch];
+      sd = fma(w, a, sd);
+      if (nrhs > 0) s0 = fma(w, y[ch], s0);
+      if (nrhs > 1) s1 = fma(w, y[(size_t)H + ch], s1);
+    }
+    if (with_d) sd = group_sum(sd, g);
+    if (nrhs > 0) s0 = group_sum(s0, g);
+    if (nrhs > 1) s1 = group_sum(s1, g);
+    if (v >= 0 && sub == 0) {
+      if (with_d) {
+        const double dv = val[p.diagq[v]] - sd;
+        d[v] = dv;
+        if (!(dv > 0.0) || !isfinite(dv)) info[1] = 1;
+      }
+      if (nrhs > 0) y[v] = rhs[v] - s0;
+      if (nrhs > 1) y[(size_t)H + v] = rhs[(size_t)H + v] - s1;
+    }
+  } else {
+    for (int c = 0; c < nrhs; ++c) {
+      const double* yc = y + (size_t)c * H;
+      double s = 0.0;
+      for (int q = q0 + sub; q < q1; q += g) {
+        const int ch = p.child[q];
+        s = fma(val[p.childq[q]] / d[ch], yc[ch], s);
+      }
+      s = group_sum(s, g);
+      if (v >= 0 && sub == 0) y[(size_t)c * H + v] = rhs[(size_t)c * H + v] - s;
+    }
+  }
+}
+
+// One round (every thread of the block calls it; the caller puts the round's
+// barrier after it).  The plan lists a round's nodes by descending child
+// count and marks the first hcnt[r] as heavy: those take one warp each
+// (lanes over the children), the others a lane group sized by their number.
+// The host picks hcnt[r] from the child counts so that neither the few
+// long lists (a core beta node holding dozens of peeled alpha leaves) nor
+// the many short ones set the round's latency alone.
 __device__ __forceinline__ void round_step(const double* __restrict__ val, const PeelPtrs& p,
                                            int r, bool with_d, double* __restrict__ d,
                                            const double* __restrict__ rhs, int nrhs, int H,
                                            double* __restrict__ y, int* __restrict__ info) {
-  const int r0 = p.rptr[r], cnt = p.rptr[r + 1] - r0;
-  const int g = group_width(cnt), per = blockDim.x / g, sub = threadIdx.x & (g - 1);
-  for (int k0 = 0; k0 < cnt; k0 += per) {
+  const int r0 = p.rptr[r], cnt = p.rptr[r + 1] - r0, nh = p.hcnt[r];
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int k0 = 0; k0 < nh; k0 += nw) {
+    const int k = k0 + warp;
+    node_step(val, p, k < nh ? p.order[r0 + k] : -1, threadIdx.x & 31, 32, with_d, d, rhs, nrhs,
+              H, y, info);
+  }
+  const int nl = cnt - nh, l0 = r0 + nh;
+  const int g = group_width(nl), per = blockDim.x / g, sub = threadIdx.x & (g - 1);
+  for (int k0 = 0; k0 < nl; k0 += per) {
     const int k = k0 + (int)threadIdx.x / g;
-    const int v = k < cnt ? p.order[r0 + k] : -1;
-    const int q0 = v >= 0 ? p.cptr[v] : 0, q1 = v >= 0 ? p.cptr[v + 1] : 0;
-    if (nrhs <= 2) {
-      double sd = 0.0, s0 = 0.0, s1 = 0.0;
-      for (int q = q0 + sub; q < q1; q += g) {
-        const int ch = p.child[q];
-        const double a = val[p.childq[q]];
-        const double w = a / d[ch];
-        sd = fma(w, a, sd);
-        if (nrhs > 0) s0 = fma(w, y[ch], s0);
-        if (nrhs > 1) s1 = fma(w, y[(size_t)H + ch], s1);
-      }
-      if (with_d) sd = group_sum(sd, g);
-      if (nrhs > 0) s0 = group_sum(s0, g);
-      if (nrhs > 1) s1 = group_sum(s1, g);
-      if (v >= 0 && sub == 0) {
-        if (with_d) {
-          const double dv = val[p.diagq[v]] - sd;
-          d[v] = dv;
-          if (!(dv > 0.0) || !isfinite(dv)) info[1] = 1;
-        }
-        if (nrhs > 0) y[v] = rhs[v] - s0;
-        if (nrhs > 1) y[(size_t)H + v] = rhs[(size_t)H + v] - s1;
-      }
-    } else {
-      for (int c = 0; c < nrhs; ++c) {
-        const double* yc = y + (size_t)c * H;
-        double s = 0.0;
-        for (int q = q0 + sub; q < q1; q += g) {
-          const int ch = p.child[q];
-          s = fma(val[p.childq[q]] / d[ch], yc[ch], s);
-        }
-        s = group_sum(s, g);
-        if (v >= 0 && sub == 0) y[(size_t)c * H + v] = rhs[(size_t)c * H + v] - s;
-      }
-    }
+    node_step(val, p, k < nl ? p.order[l0 + k] : -1, sub, g, with_d, d, rhs, nrhs, H, y, info);
   }
 }
 
@@ -391,8 +413,10 @@ __device__ void dev_trisolve(const double* __restrict__ L, const double* __restr
 // per panel; idiag[j] <- 1 / L_jj.
 //   1. the 32 x 32 diagonal block, by warp 0 alone (warp_block_cholesky:
 //      left-looking, lane r computes row r of the block);
-//   2. the panel below it, L21 = S21 L11^{-T}: each thread solves whole rows,
-//      entry k as a dot product over the row's earlier entries;
+//   2. the panel below it, L21 = S21 L11^{-T}: one warp per two rows, a
+//      row's 32 entries in the lanes, each solved column broadcast by a
+//      shuffle and subtracted from the later lanes (32 short steps instead of
+//      a thread walking 528 dependent multiply-adds per row);
 //   3. the trailing update S22 -= L21 L21^T on the lower triangle: a work
 //      item is one column c of a 4-row tile (rows i0..i0+3, c <= i), its
 //      four dot products over the panel accumulated in registers.
@@ -400,24 +424,42 @@ __device__ void dev_trisolve(const double* __restrict__ L, const double* __restr
 // continues with d = 1 (the last such column is reported).
 __device__ void dev_cholesky(double* __restrict__ S, double* __restrict__ idiag, int kc, int ld,
                              int* __restrict__ info) {
-  const int warp = threadIdx.x >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int j0 = 0; j0 < kc; j0 += 32) {
     const int bw = min(32, kc - j0);
     if (warp == 0) warp_block_cholesky(S + (size_t)j0 * ld + j0, ld, bw, idiag + j0, j0, info);
     __syncthreads();
     const int r0 = j0 + bw;  // first row below the block
-    for (int i = r0 + threadIdx.x; i < kc; i += blockDim.x) {
-      double* Si = S + (size_t)i * ld + j0;
-      for (int k = 0; k < bw; ++k) {
-        const double* Lk = S + (size_t)(j0 + k) * ld + j0;
-        double a0 = Si[k], a1 = 0.0;
-        int c = 0;
-        for (; c + 1 < k; c += 2) {
-          a0 = fma(-Si[c], Lk[c], a0);
-          a1 = fma(-Si[c + 1], Lk[c + 1], a1);
+    // panel rows, two per warp: lane k holds entry k of each row; column jj
+    // is final once the earlier columns are subtracted, is broadcast by a
+    // shuffle and subtracted from the lanes k > jj (L11[k][jj] read by lane
+    // k: consecutive rows, distinct banks under the odd row stride)
+    {
+      const int nw = blockDim.x >> 5;
+      const double* L11 = S + (size_t)j0 * ld + j0;
+      for (int i = r0 + 2 * warp; i < kc; i += 2 * nw) {
+        const bool two = i + 1 < kc;
+        double* Si = S + (size_t)i * ld + j0;
+        double* Sj = Si + ld;
+        double s0 = lane < bw ? Si[lane] : 0.0;
+        double s1 = (two && lane < bw) ? Sj[lane] : 0.0;
+        for (int jj = 0; jj < bw; ++jj) {
+          const double l = (lane > jj && lane < bw) ? L11[(size_t)lane * ld + jj] : 0.0;
+          const double dj = idiag[j0 + jj];
+          const double x0 = __shfl_sync(0xffffffffu, s0, jj) * dj;
+          const double x1 = __shfl_sync(0xffffffffu, s1, jj) * dj;
+          if (lane == jj) {
+            s0 = x0;
+            s1 = x1;
+          } else if (lane > jj) {
+            s0 = fma(-l, x0, s0);
+            s1 = fma(-l, x1, s1);
+          }
         }
-        if (c < k) a0 = fma(-Si[c], Lk[c], a0);
-        Si[k] = (a0 + a1) * idiag[j0 + k];
+        if (lane < bw) {
+          Si[lane] = s0;
+          if (two) Sj[lane] = s1;
+        }
       }
     }
     __syncthreads();
@@ -722,6 +764,42 @@ int peel_plan_host(PeelFactor& P, int n, int m, const std::vector<int>& rp,
       (v < n ? core_a : core_b).push_back(v);
     }
   rptr.push_back((int)order.size());
+  // child counts; each round's nodes by descending count, the first hcnt[r]
+  // of them heavy (one warp each on the device).  hcnt[r] minimises an
+  // estimate of the round's latency in dependent child steps: a pass of
+  // kWarps heavy nodes costs 1.5 + ceil(c_first / 32), a pass of the light
+  // nodes (lane groups of g, as group_width sizes them) 1 + ceil(c_max / g),
+  // plus 0.5 for the shuffle reduction when g > 1.
+  std::vector<int> ccount(H, 0);
+  for (int k = 0; k < npeel; ++k)
+    if (par[order[k]] >= 0) ccount[par[order[k]]]++;
+  std::vector<int> hcnt(rounds + 1, 0);
+  {
+    constexpr int kWarps = kPeelThreads / 32;
+    for (int r = 0; r <= rounds; ++r) {
+      const int b0 = rptr[r], cnt = rptr[r + 1] - b0;
+      std::stable_sort(order.begin() + b0, order.begin() + b0 + cnt,
+                       [&](int x, int y) { return ccount[x] > ccount[y]; });
+      double best = 0.0, heavy = 0.0;
+      int bnh = 0;
+      for (int nh = 0; nh <= cnt; ++nh) {
+        if (nh > 0 && (nh - 1) % kWarps == 0) heavy += 1.5 + (ccount[order[b0 + nh - 1]] + 31) / 32;
+        const int nl = cnt - nh;
+        double light = 0.0;
+        if (nl > 0) {
+          int g = 1;
+          while (g < 32 && nl * (g * 2) <= kPeelThreads) g *= 2;
+          const int per = kPeelThreads / g, passes = (nl + per - 1) / per;
+          light = passes * (1.0 + (ccount[order[b0 + nh]] + g - 1) / g + (g > 1 ? 0.5 : 0.0));
+        }
+        if (nh == 0 || heavy + light < best) {
+          best = heavy + light;
+          bnh = nh;
+        }
+      }
+      hcnt[r] = bnh;
+    }
+  }
   const bool elim_a = core_a.size() >= core_b.size();
   const std::vector<int>& snodes = elim_a ? core_b : core_a;
   const std::vector<int>& enodes = elim_a ? core_a : core_b;
@@ -730,9 +808,6 @@ int peel_plan_host(PeelFactor& P, int n, int m, const std::vector<int>& rp,
   for (int t = 0; t < kc; ++t) loc[snodes[t]] = t;
   for (int e = 0; e < ke; ++e) loc[enodes[e]] = e;
   // children lists (eliminated neighbours of every node), in round order
-  std::vector<int> ccount(H, 0);
-  for (int k = 0; k < npeel; ++k)
-    if (par[order[k]] >= 0) ccount[par[order[k]]]++;
   std::vector<int> cptr(H + 1, 0);
   for (int v = 0; v < H; ++v) cptr[v + 1] = cptr[v] + ccount[v];
   std::vector<int> child(std::max(cptr[H], 1)), childq(std::max(cptr[H], 1));
@@ -776,6 +851,7 @@ int peel_plan_host(PeelFactor& P, int n, int m, const std::vector<int>& rp,
   };
   P.off_order = put(order, order.size());
   P.off_rptr = put(rptr, rptr.size());
+  P.off_hcnt = put(hcnt, hcnt.size());
   P.off_diagq = put(diagq, H);
   P.off_cptr = put(cptr, H + 1);
   P.off_child = put(child, cptr[H]);
