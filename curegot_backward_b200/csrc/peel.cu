@@ -14,7 +14,8 @@
 //   node's pivot pulls its children's contributions in a fixed order, so
 //   the result is deterministic), one CTA per Schur row assembles the core
 //   Schur complement, cuSOLVER potrf factors it.  The solve is a forward
-//   sweep over the rounds, potrs on the core, and a backward sweep.
+//   sweep over the rounds with the core's triangular solves in the same
+//   single-CTA kernel (potrs above kPeelTriMax), and a backward sweep.
 // Small cores (kc <= kPeelSmallCore = 160, 204 KB of shared memory for the
 //   dense core factor): the whole factorization and solve run in
 //   ONE single-CTA kernel -- pivots and forward values in the same rounds,
@@ -290,17 +291,112 @@ __global__ void dense_contrib_kernel(const double* __restrict__ val, PeelPtrs p,
   }
 }
 
+// z <- (L L^T)^{-1} z in shared memory (nrhs <= 2 columns of kc entries),
+// with L the potrf factor in global memory (column-major kc x kc, lower:
+// L(i, j) = L[j * kc + i]), by the whole block, 32-row blocks at a time:
+//   - the block's diagonal 32 x 32 part of L is staged in shared memory
+//     (coalesced over rows) and solved by one warp per right-hand side with
+//     shuffles (lane r holds z_r);
+//   - forward: the rows below take the block's contribution, one thread per
+//     row (loads coalesced over rows for each column of the block);
+//   - backward: the rows above take it, one thread per row (a row's 32
+//     entries are contiguous in its column of L).
+// idiag[kc] and blk[32 * 33] are shared scratch.  Replaces cuSOLVER potrs:
+// two library trsm launches of ~90 us each at these sizes, latency-bound.
+__device__ void dev_trisolve_cm(const double* __restrict__ L, int kc, double* __restrict__ z,
+                                int nrhs, double* __restrict__ idiag, double* __restrict__ blk) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* z0 = z;
+  double* z1 = z + kc;
+  for (int t = threadIdx.x; t < kc; t += blockDim.x) idiag[t] = 1.0 / L[(size_t)t * kc + t];
+  auto stage = [&](int j0, int bw) {  // blk[r * 33 + c] = L(j0 + r, j0 + c)
+    for (int e = threadIdx.x; e < 32 * 32; e += blockDim.x) {
+      const int c = e >> 5, r = e & 31;
+      if (r < bw && c < bw) blk[r * 33 + c] = L[(size_t)(j0 + c) * kc + j0 + r];
+    }
+  };
+  for (int j0 = 0; j0 < kc; j0 += 32) {  // L y = z
+    const int bw = min(32, kc - j0);
+    stage(j0, bw);
+    __syncthreads();
+    if (warp < nrhs) {
+      double* zc = z + (size_t)warp * kc;
+      double zr = lane < bw ? zc[j0 + lane] : 0.0;
+      for (int jj = 0; jj < bw; ++jj) {
+        const double zj = __shfl_sync(0xffffffffu, zr, jj) * idiag[j0 + jj];
+        if (lane == jj) zr = zj;
+        else if (lane > jj && lane < bw) zr = fma(-blk[lane * 33 + jj], zj, zr);
+      }
+      if (lane < bw) zc[j0 + lane] = zr;
+    }
+    __syncthreads();
+    for (int i = j0 + bw + threadIdx.x; i < kc; i += blockDim.x) {
+      double a0 = z0[i], a1 = nrhs > 1 ? z1[i] : 0.0;
+      for (int c = 0; c < bw; ++c) {
+        const double l = L[(size_t)(j0 + c) * kc + i];
+        a0 = fma(-l, z0[j0 + c], a0);
+        if (nrhs > 1) a1 = fma(-l, z1[j0 + c], a1);
+      }
+      z0[i] = a0;
+      if (nrhs > 1) z1[i] = a1;
+    }
+    __syncthreads();
+  }
+  for (int j1 = kc; j1 > 0; j1 -= 32) {  // L^T x = y
+    const int j0 = max(0, j1 - 32), bw = j1 - j0;
+    stage(j0, bw);
+    __syncthreads();
+    if (warp < nrhs) {
+      double* zc = z + (size_t)warp * kc;
+      double zr = lane < bw ? zc[j0 + lane] : 0.0;
+      for (int jj = bw - 1; jj >= 0; --jj) {
+        const double zj = __shfl_sync(0xffffffffu, zr, jj) * idiag[j0 + jj];
+        if (lane == jj) zr = zj;
+        else if (lane < jj) zr = fma(-blk[jj * 33 + lane], zj, zr);
+      }
+      if (lane < bw) zc[j0 + lane] = zr;
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < j0; j += blockDim.x) {
+      const double* Lj = L + (size_t)j * kc + j0;  // L(j0 + c, j)
+      double a0 = z0[j], a1 = nrhs > 1 ? z1[j] : 0.0;
+      for (int c = 0; c < bw; ++c) {
+        const double l = Lj[c];
+        a0 = fma(-l, z0[j0 + c], a0);
+        if (nrhs > 1) a1 = fma(-l, z1[j0 + c], a1);
+      }
+      z0[j] = a0;
+      if (nrhs > 1) z1[j] = a1;
+    }
+    __syncthreads();
+  }
+}
+
 // Forward sweep (y = L^{-1} b over the peeled rounds and the core's own
-// children), then the reduction of the core right-hand side to the Schur side.
+// children), then the reduction of the core right-hand side to the Schur
+// side, rs.  With Lcm (the core's potrf factor, kc <= kPeelTriMax) the core
+// solve rs <- S^{-1} rs runs here too, in shared memory (dynamic shared
+// memory: tri_smem(kc)); without it the caller runs potrs.
 __global__ void __launch_bounds__(kPeelThreads, 1) peel_forward_kernel(
     const double* __restrict__ val, PeelPtrs p, int rounds, const double* __restrict__ d,
     const double* __restrict__ rhs, int nrhs, int H, int kc, double* __restrict__ y,
-    double* __restrict__ rs) {
+    double* __restrict__ rs, const double* __restrict__ Lcm) {
+  extern __shared__ double tsm[];
   for (int r = 0; r <= rounds; ++r) {
     round_step(val, p, r, false, const_cast<double*>(d), rhs, nrhs, H, y, nullptr);
     __syncthreads();
   }
-  core_rhs_step(val, p, d, y, nrhs, H, kc, rs);
+  if (Lcm == nullptr) {
+    core_rhs_step(val, p, d, y, nrhs, H, kc, rs);
+    return;
+  }
+  double* z = tsm;                // [2 kc]
+  double* idiag = tsm + 2 * kc;   // [kc]
+  double* blk = idiag + kc;       // [32 * 33]
+  core_rhs_step(val, p, d, y, nrhs, H, kc, z);
+  __syncthreads();
+  dev_trisolve_cm(Lcm, kc, z, nrhs, idiag, blk);
+  for (int e = threadIdx.x; e < nrhs * kc; e += blockDim.x) rs[e] = z[e];
 }
 
 // Core back-substitution, then the backward sweep over the peeled rounds.
@@ -612,6 +708,8 @@ __global__ void __launch_bounds__(kPeelThreads, 1) peel_small_solve_kernel(
   dev_backward(val, p, rounds, d, y, z, nrhs, H, kc, ke, x);
 }
 
+size_t tri_smem(int kc) { return ((size_t)3 * std::max(kc, 1) + 32 * 33) * sizeof(double); }
+
 size_t small_smem(int kc) {
   return ((size_t)kc * core_ld(kc) + 3 * (size_t)std::max(kc, 1)) * sizeof(double);
 }
@@ -625,6 +723,8 @@ int ensure_small_smem() {
   CG_TRY_CUDA(cudaFuncSetAttribute(peel_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   CG_TRY_CUDA(cudaFuncSetAttribute(peel_small_solve_kernel,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  CG_TRY_CUDA(cudaFuncSetAttribute(peel_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)tri_smem(kPeelTriMax)));
   done_dev = dev;
   return CG_OK;
 }
@@ -996,10 +1096,15 @@ int peel_solve(PeelFactor& P, const SpHess& A, cusolverDnHandle_t h, const doubl
     CG_TRY_CUDA(cudaGetLastError());
     return CG_OK;
   }
-  { peel_forward_kernel<<<1, kPeelThreads, 0, st>>>(A.val, pp, P.rounds, P.d, rhs, nrhs, P.H,
-                                                    P.kc, P.y, P.rs); count_launch(); }
+  // cores up to kPeelTriMax: the triangular solves with the potrf factor in
+  // the forward kernel; larger ones: potrs
+  const bool tri = P.kc > 0 && P.kc <= kPeelTriMax;
+  if (tri) CG_TRY(ensure_small_smem());
+  { peel_forward_kernel<<<1, kPeelThreads, tri ? tri_smem(P.kc) : 0, st>>>(
+        A.val, pp, P.rounds, P.d, rhs, nrhs, P.H, P.kc, P.y, P.rs, tri ? P.S : nullptr);
+    count_launch(); }
   CG_TRY_CUDA(cudaGetLastError());
-  if (P.kc > 0) {
+  if (P.kc > 0 && !tri) {
     if (cusolverDnSetStream(h, st) != CUSOLVER_STATUS_SUCCESS) return CG_ERR_SOLVER;
     if (cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, P.kc, nrhs, P.S, P.kc, P.rs, P.kc,
                          P.info + 2) != CUSOLVER_STATUS_SUCCESS) {

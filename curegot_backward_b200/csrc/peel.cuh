@@ -24,6 +24,9 @@ namespace cg {
 
 // Largest core Schur complement factored in shared memory inside one kernel.
 constexpr int kPeelSmallCore = 160;
+// Largest core whose triangular solves with the potrf factor run inside the
+// single-CTA forward kernel (shared-memory right-hand sides) instead of potrs.
+constexpr int kPeelTriMax = 1024;
 // Largest core Schur complement assembled from host-planned contribution
 // lists (one thread per entry); larger ones use the row-wise assembly.
 constexpr int kPeelContribMax = 1024;
