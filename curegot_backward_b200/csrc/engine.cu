@@ -314,9 +314,18 @@ void bcd_loop(cg_engine_s* E, int cls) {
   cudaEvent_t ev0, ev1;
   cudaEventCreate(&ev0);
   cudaEventCreate(&ev1);
-  // host-input copies run on their own stream, overlapping the chunks
-  cudaStream_t cst;
+  // host-input copies run on their own streams, overlapping the chunks: one
+  // for cost matrices of at least kBigCopy bytes and one for the rest, so a
+  // small request's copy is not queued behind a large one (a 8192 x 8192
+  // FP32 matrix takes ~5 ms over PCIe); the two share the link
+  constexpr size_t kBigCopy = size_t(16) << 20;
+  cudaStream_t cst, cst_big;
   cudaStreamCreateWithFlags(&cst, cudaStreamNonBlocking);
+  cudaStreamCreateWithFlags(&cst_big, cudaStreamNonBlocking);
+  auto copy_stream_of = [&](const Req* q) {
+    const size_t mb = (size_t)q->r.n * q->r.m * (q->r.m_f32 ? 4 : 8);
+    return (q->r.host_inputs && mb >= kBigCopy) ? cst_big : cst;
+  };
   std::vector<cudaEvent_t> ev_pool;
   auto take_event = [&]() -> cudaEvent_t {
     if (!ev_pool.empty()) {
@@ -393,11 +402,12 @@ void bcd_loop(cg_engine_s* E, int cls) {
         q->t_admit = now_s();
         if (none) batch_f32 = q->r.m_f32 != 0;
         cudaEvent_t evq = take_event(), used = nullptr;
-        int rc = evq ? bcd_stage(q, cst, evq, &used) : CG_ERR_CUDA;
+        const cudaStream_t qcs = copy_stream_of(q);
+        int rc = evq ? bcd_stage(q, qcs, evq, &used) : CG_ERR_CUDA;
         if (evq && !used) ev_pool.push_back(evq);
         lk.lock();
         if (rc != CG_OK) {
-          if (q->block) cudaFreeAsync(q->block, cst);
+          if (q->block) cudaFreeAsync(q->block, qcs);
           q->block = nullptr;
           q->status = rc;
           E->in_use -= q->footprint;
@@ -649,7 +659,9 @@ void bcd_loop(cg_engine_s* E, int cls) {
   if (gexec) cudaGraphExecDestroy(gexec);
   for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
   cudaStreamSynchronize(cst);
+  cudaStreamSynchronize(cst_big);
   cudaStreamDestroy(cst);
+  cudaStreamDestroy(cst_big);
   if (d_states) cudaFreeAsync(d_states, st);
   if (h_states) cudaFreeHost(h_states);
   if (d_probs) cudaFreeAsync(d_probs, st);

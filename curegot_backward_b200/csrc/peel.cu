@@ -35,11 +35,18 @@ namespace cg {
 namespace {
 
 constexpr int kMaxPeelRounds = 512;
-constexpr int kPeelThreads = 1024;
+#ifndef CG_PEEL_THREADS
+#define CG_PEEL_THREADS 1024
+#endif
+constexpr int kPeelThreads = CG_PEEL_THREADS;  // threads of the single-CTA peel kernels
 constexpr int kSmallCore = kPeelSmallCore;  // in-shared-memory Cholesky
 
 struct PeelPtrs {
-  const int *order, *rptr, *hcnt, *diagq, *cptr, *child, *childq, *par, *parq;
+  // order: nodes round by round; per order position k: cpos[k]..cpos[k+1]
+  // its children (child node, value index of the edge), dqo[k] the value
+  // index of its diagonal, ppar[k] / pparq[k] its parent and the edge's
+  // value index (-1: none).  diagq: diagonal value index by node id.
+  const int *order, *rptr, *hcnt, *diagq, *cpos, *child, *childq, *dqo, *ppar, *pparq;
   const int *snodes, *enodes, *sptr, *sadj, *sq, *eptr, *eadj, *eq;
   // contribution lists of the core Schur complement (entry t * kc + t2):
   // eliminated node ce, E-list position cw of the edge (ce, t) (its weight
@@ -56,11 +63,12 @@ PeelPtrs ptrs_of(const PeelFactor& P) {
   p.rptr = b + P.off_rptr;
   p.hcnt = b + P.off_hcnt;
   p.diagq = b + P.off_diagq;
-  p.cptr = b + P.off_cptr;
+  p.cpos = b + P.off_cpos;
   p.child = b + P.off_child;
   p.childq = b + P.off_childq;
-  p.par = b + P.off_par;
-  p.parq = b + P.off_parq;
+  p.dqo = b + P.off_dqo;
+  p.ppar = b + P.off_ppar;
+  p.pparq = b + P.off_pparq;
   p.snodes = b + P.off_snodes;
   p.enodes = b + P.off_enodes;
   p.sptr = b + P.off_sptr;
@@ -98,17 +106,20 @@ __device__ __forceinline__ double group_sum(double v, int g) {
 }
 
 // Pivot (with_d) and forward values y = L^{-1} rhs (nrhs columns, stride H)
-// of node v (v < 0: none), its child list split over the g lanes of a group
-// (this lane is `sub`; every lane of the warp calls it).  Node v's pivot is
+// of node v at order position k (k < 0: none), its child list split over
+// the g lanes of a group (this lane is `sub`; every lane of the warp calls
+// it).  The child range and the diagonal index are read by position, in
+// parallel with order[k], not after it.  Node v's pivot is
 //   d_v = A_vv - sum over children ch of (a_ch,v / d_ch) a_ch,v
 // and its forward value y_v = rhs_v - sum (a_ch,v / d_ch) y_ch.
 // nrhs <= 2 is handled in one pass over the children.
 __device__ __forceinline__ void node_step(const double* __restrict__ val, const PeelPtrs& p,
-                                          int v, int sub, int g, bool with_d,
+                                          int k, int sub, int g, bool with_d,
                                           double* __restrict__ d, const double* __restrict__ rhs,
                                           int nrhs, int H, double* __restrict__ y,
                                           int* __restrict__ info) {
-  const int q0 = v >= 0 ? p.cptr[v] : 0, q1 = v >= 0 ? p.cptr[v + 1] : 0;
+  const int v = k >= 0 ? p.order[k] : -1;
+  const int q0 = k >= 0 ? p.cpos[k] : 0, q1 = k >= 0 ? p.cpos[k + 1] : 0;
   if (nrhs <= 2) {
     double sd = 0.0, s0 = 0.0, s1 = 0.0;
     for (int q = q0 + sub; q < q1; q += g) {
@@ -124,7 +135,7 @@ __device__ __forceinline__ void node_step(const double* __restrict__ val, const 
     if (nrhs > 1) s1 = group_sum(s1, g);
     if (v >= 0 && sub == 0) {
       if (with_d) {
-        const double dv = val[p.diagq[v]] - sd;
+        const double dv = val[p.dqo[k]] - sd;
         d[v] = dv;
         if (!(dv > 0.0) || !isfinite(dv)) info[1] = 1;
       }
@@ -160,14 +171,14 @@ __device__ __forceinline__ void round_step(const double* __restrict__ val, const
   const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int k0 = 0; k0 < nh; k0 += nw) {
     const int k = k0 + warp;
-    node_step(val, p, k < nh ? p.order[r0 + k] : -1, threadIdx.x & 31, 32, with_d, d, rhs, nrhs,
-              H, y, info);
+    node_step(val, p, k < nh ? r0 + k : -1, threadIdx.x & 31, 32, with_d, d, rhs, nrhs, H, y,
+              info);
   }
   const int nl = cnt - nh, l0 = r0 + nh;
   const int g = group_width(nl), per = blockDim.x / g, sub = threadIdx.x & (g - 1);
   for (int k0 = 0; k0 < nl; k0 += per) {
     const int k = k0 + (int)threadIdx.x / g;
-    node_step(val, p, k < nl ? p.order[l0 + k] : -1, sub, g, with_d, d, rhs, nrhs, H, y, info);
+    node_step(val, p, k < nl ? l0 + k : -1, sub, g, with_d, d, rhs, nrhs, H, y, info);
   }
 }
 
@@ -411,10 +422,10 @@ __global__ void __launch_bounds__(kPeelThreads, 1) peel_backward_kernel(
   for (int r = rounds - 1; r >= 0; --r) {
     for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
       const int v = p.order[idx];
-      const int u = p.par[v];
+      const int u = p.ppar[idx];
       for (int c = 0; c < nrhs; ++c) {
         double xv = y[(size_t)c * H + v];
-        if (u >= 0) xv -= val[p.parq[v]] * x[(size_t)c * H + u];
+        if (u >= 0) xv -= val[p.pparq[idx]] * x[(size_t)c * H + u];
         x[(size_t)c * H + v] = xv / d[v];
       }
     }
@@ -523,7 +534,10 @@ __device__ void dev_cholesky(double* __restrict__ S, double* __restrict__ idiag,
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int j0 = 0; j0 < kc; j0 += 32) {
     const int bw = min(32, kc - j0);
-    if (warp == 0) warp_block_cholesky(S + (size_t)j0 * ld + j0, ld, bw, idiag + j0, j0, info);
+    if (warp == 0) {
+      if (bw == 32) warp_block_cholesky32(S + (size_t)j0 * ld + j0, ld, idiag + j0, j0, info);
+      else warp_block_cholesky(S + (size_t)j0 * ld + j0, ld, bw, idiag + j0, j0, info);
+    }
     __syncthreads();
     const int r0 = j0 + bw;  // first row below the block
     // panel rows, two per warp: lane k holds entry k of each row; column jj
@@ -603,10 +617,10 @@ __device__ void dev_backward(const double* __restrict__ val, const PeelPtrs& p, 
   for (int r = rounds - 1; r >= 0; --r) {
     for (int idx = p.rptr[r] + threadIdx.x; idx < p.rptr[r + 1]; idx += blockDim.x) {
       const int v = p.order[idx];
-      const int u = p.par[v];
+      const int u = p.ppar[idx];
       for (int c = 0; c < nrhs; ++c) {
         double xv = y[(size_t)c * H + v];
-        if (u >= 0) xv -= val[p.parq[v]] * x[(size_t)c * H + u];
+        if (u >= 0) xv -= val[p.pparq[idx]] * x[(size_t)c * H + u];
         x[(size_t)c * H + v] = xv / d[v];
       }
     }
@@ -908,17 +922,31 @@ int peel_plan_host(PeelFactor& P, int n, int m, const std::vector<int>& rp,
   for (int t = 0; t < kc; ++t) loc[snodes[t]] = t;
   for (int e = 0; e < ke; ++e) loc[enodes[e]] = e;
   // children lists (eliminated neighbours of every node), in round order
-  std::vector<int> cptr(H + 1, 0);
-  for (int v = 0; v < H; ++v) cptr[v + 1] = cptr[v] + ccount[v];
-  std::vector<int> child(std::max(cptr[H], 1)), childq(std::max(cptr[H], 1));
+  // children by order position: the children of the node at position k
+  // occupy [cpos[k], cpos[k + 1]), in round order; per position also the
+  // diagonal value index and the parent edge
+  const int npos = (int)order.size();  // every node: peeled rounds + core
+  std::vector<int> posof(H, -1);
+  for (int k = 0; k < npos; ++k) posof[order[k]] = k;
+  std::vector<int> cpos(npos + 1, 0);
+  for (int k = 0; k < npos; ++k) cpos[k + 1] = cpos[k] + ccount[order[k]];
+  std::vector<int> child(std::max(cpos[npos], 1)), childq(std::max(cpos[npos], 1));
   {
-    std::vector<int> fill(cptr.begin(), cptr.end() - 1);
+    std::vector<int> fill(cpos.begin(), cpos.end() - 1);
     for (int k = 0; k < npeel; ++k) {
       const int v = order[k], u = par[v];
       if (u < 0) continue;
-      child[fill[u]] = v;
-      childq[fill[u]++] = parq[v];
+      const int pu = posof[u];
+      child[fill[pu]] = v;
+      childq[fill[pu]++] = parq[v];
     }
+  }
+  std::vector<int> dqo(npos), ppar(npos), pparq(npos);
+  for (int k = 0; k < npos; ++k) {
+    const int v = order[k];
+    dqo[k] = diagq[v];
+    ppar[k] = par[v];
+    pparq[k] = parq[v];
   }
   // core adjacency restricted to alive neighbours, as local indices
   auto core_lists = [&](const std::vector<int>& nodes, std::vector<int>& ptr, std::vector<int>& ladj,
@@ -953,11 +981,12 @@ int peel_plan_host(PeelFactor& P, int n, int m, const std::vector<int>& rp,
   P.off_rptr = put(rptr, rptr.size());
   P.off_hcnt = put(hcnt, hcnt.size());
   P.off_diagq = put(diagq, H);
-  P.off_cptr = put(cptr, H + 1);
-  P.off_child = put(child, cptr[H]);
-  P.off_childq = put(childq, cptr[H]);
-  P.off_par = put(par, H);
-  P.off_parq = put(parq, H);
+  P.off_cpos = put(cpos, npos + 1);
+  P.off_child = put(child, cpos[npos]);
+  P.off_childq = put(childq, cpos[npos]);
+  P.off_dqo = put(dqo, npos);
+  P.off_ppar = put(ppar, npos);
+  P.off_pparq = put(pparq, npos);
   P.off_snodes = put(snodes, kc);
   P.off_enodes = put(enodes, ke);
   P.off_sptr = put(sptr, kc + 1);
@@ -996,7 +1025,7 @@ int peel_plan_host(PeelFactor& P, int n, int m, const std::vector<int>& rp,
   P.npeel = npeel;
   P.kc = kc;
   P.ke = ke;
-  P.nchild = cptr[H];
+  P.nchild = cpos[npos];
   P.ns_adj = (long long)sadj.size();
   P.ne_adj = (long long)eadj.size();
   return CG_OK;

@@ -39,10 +39,10 @@ struct PeelFactor {
   long long nchild = 0, ns_adj = 0, ne_adj = 0;
   // host plan
   std::vector<int> h_ints;  // every int array below, packed in device order
-  size_t off_order = 0, off_rptr = 0, off_hcnt = 0, off_diagq = 0, off_cptr = 0, off_child = 0, off_childq = 0,
-         off_par = 0, off_parq = 0, off_snodes = 0, off_enodes = 0, off_sptr = 0, off_sadj = 0,
-         off_sq = 0, off_eptr = 0, off_eadj = 0, off_eq = 0, off_ccp = 0, off_ce = 0, off_cq1 = 0,
-         off_cq2 = 0;
+  size_t off_order = 0, off_rptr = 0, off_hcnt = 0, off_diagq = 0, off_cpos = 0, off_child = 0,
+         off_childq = 0, off_dqo = 0, off_ppar = 0, off_pparq = 0, off_snodes = 0, off_enodes = 0,
+         off_sptr = 0, off_sadj = 0, off_sq = 0, off_eptr = 0, off_eadj = 0, off_eq = 0, off_ccp = 0,
+         off_ce = 0, off_cq1 = 0, off_cq2 = 0;
   bool contrib = false;  // per-entry contribution lists of the core Schur complement
   // device
   void* block = nullptr;
