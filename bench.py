@@ -40,6 +40,14 @@ import time
 
 import numpy as np
 
+# Every kernel is loaded when the CUDA context starts, not at its first
+# launch: with lazy loading (the CUDA 12 default) the first launch of a
+# kernel variant inside the timed region (a cuSOLVER potrf size class, a
+# pass template) held every stream of the process for 0.3-1 s on a fresh
+# box.  A serving process pays this once at start-up (2-5 s).  Set
+# CUDA_MODULE_LOADING=LAZY to measure without it.
+os.environ.setdefault("CUDA_MODULE_LOADING", "EAGER")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)

@@ -39,6 +39,10 @@ constexpr int kMaxPeelRounds = 512;
 #define CG_PEEL_THREADS 1024
 #endif
 constexpr int kPeelThreads = CG_PEEL_THREADS;  // threads of the single-CTA peel kernels
+#ifndef CG_PEEL_MINB
+#define CG_PEEL_MINB 1
+#endif
+constexpr int kPeelMinBlocks = CG_PEEL_MINB;  // launch-bounds residency hint
 constexpr int kSmallCore = kPeelSmallCore;  // in-shared-memory Cholesky
 
 struct PeelPtrs {
@@ -233,7 +237,7 @@ __device__ __forceinline__ void core_back_step(const double* __restrict__ val, c
 
 // Pivots of every node, round by round; the core nodes come last (one round)
 // and receive their diagonal updated by their peeled children.
-__global__ void __launch_bounds__(kPeelThreads, 1) peel_factor_kernel(
+__global__ void __launch_bounds__(kPeelThreads, kPeelMinBlocks) peel_factor_kernel(
     const double* __restrict__ val, PeelPtrs p, int rounds, double* __restrict__ d,
     int* __restrict__ info) {
   for (int r = 0; r <= rounds; ++r) {
@@ -388,7 +392,7 @@ __device__ void dev_trisolve_cm(const double* __restrict__ L, int kc, double* __
 // side, rs.  With Lcm (the core's potrf factor, kc <= kPeelTriMax) the core
 // solve rs <- S^{-1} rs runs here too, in shared memory (dynamic shared
 // memory: tri_smem(kc)); without it the caller runs potrs.
-__global__ void __launch_bounds__(kPeelThreads, 1) peel_forward_kernel(
+__global__ void __launch_bounds__(kPeelThreads, kPeelMinBlocks) peel_forward_kernel(
     const double* __restrict__ val, PeelPtrs p, int rounds, const double* __restrict__ d,
     const double* __restrict__ rhs, int nrhs, int H, int kc, double* __restrict__ y,
     double* __restrict__ rs, const double* __restrict__ Lcm) {
@@ -411,7 +415,7 @@ __global__ void __launch_bounds__(kPeelThreads, 1) peel_forward_kernel(
 }
 
 // Core back-substitution, then the backward sweep over the peeled rounds.
-__global__ void __launch_bounds__(kPeelThreads, 1) peel_backward_kernel(
+__global__ void __launch_bounds__(kPeelThreads, kPeelMinBlocks) peel_backward_kernel(
     const double* __restrict__ val, PeelPtrs p, int rounds, const double* __restrict__ d,
     const double* __restrict__ y, const double* __restrict__ rs, int nrhs, int H, int kc,
     int ke, double* __restrict__ x) {
@@ -534,10 +538,7 @@ __device__ void dev_cholesky(double* __restrict__ S, double* __restrict__ idiag,
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int j0 = 0; j0 < kc; j0 += 32) {
     const int bw = min(32, kc - j0);
-    if (warp == 0) {
-      if (bw == 32) warp_block_cholesky32(S + (size_t)j0 * ld + j0, ld, idiag + j0, j0, info);
-      else warp_block_cholesky(S + (size_t)j0 * ld + j0, ld, bw, idiag + j0, j0, info);
-    }
+    if (warp == 0) warp_block_cholesky(S + (size_t)j0 * ld + j0, ld, bw, idiag + j0, j0, info);
     __syncthreads();
     const int r0 = j0 + bw;  // first row below the block
     // panel rows, two per warp: lane k holds entry k of each row; column jj
@@ -632,7 +633,7 @@ __device__ void dev_backward(const double* __restrict__ val, const PeelPtrs& p, 
 // solve x = A^{-1} rhs.  Dynamic shared memory: kc*ld + 3*kc doubles (ld =
 // core_ld(kc), the shared row stride of the core matrix; then 2 kc for the
 // reduced right-hand sides and kc for the inverse diagonal of the factor).
-__global__ void __launch_bounds__(kPeelThreads, 1) peel_fused_kernel(
+__global__ void __launch_bounds__(kPeelThreads, kPeelMinBlocks) peel_fused_kernel(
     const double* __restrict__ val, PeelPtrs p, int rounds, int kc, int ke, int H,
     const double* __restrict__ rhs, int nrhs, double* __restrict__ x, double* __restrict__ d,
     double* __restrict__ y, double* __restrict__ Lout, int* __restrict__ info,
@@ -700,7 +701,7 @@ __global__ void __launch_bounds__(kPeelThreads, 1) peel_fused_kernel(
 }
 
 // Solve with a stored small-core factor (pivots d, L in global memory).
-__global__ void __launch_bounds__(kPeelThreads, 1) peel_small_solve_kernel(
+__global__ void __launch_bounds__(kPeelThreads, kPeelMinBlocks) peel_small_solve_kernel(
     const double* __restrict__ val, PeelPtrs p, int rounds, int kc, int ke, int H,
     const double* __restrict__ rhs, int nrhs, double* __restrict__ x,
     const double* __restrict__ d, double* __restrict__ y, const double* __restrict__ Lin) {

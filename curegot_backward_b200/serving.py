@@ -9,6 +9,11 @@ device dual tensor) or CPU tensors / NumPy arrays (the engine copies them in
 and the duals back out; pinned memory makes those copies asynchronous).  An
 FP32 cost matrix selects the mixed-precision passes (FP32 M, FP64 duals,
 FP64-confirmed stopping test); FP64 selects the plain FP64 passes.
+
+Start serving processes with CUDA_MODULE_LOADING=EAGER: under lazy loading
+the first launch of each kernel variant (pass templates, cuSOLVER size
+classes) happens mid-stream and held every stream of the process for
+0.3-1 s on a fresh machine.
 """
 
 from __future__ import annotations
