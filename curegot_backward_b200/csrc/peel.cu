@@ -309,44 +309,52 @@ __global__ void dense_contrib_kernel(const double* __restrict__ val, PeelPtrs p,
 // z <- (L L^T)^{-1} z in shared memory (nrhs <= 2 columns of kc entries),
 // with L the potrf factor in global memory (column-major kc x kc, lower:
 // L(i, j) = L[j * kc + i]), by the whole block, 32-row blocks at a time:
-//   - the block's diagonal 32 x 32 part of L is staged in shared memory
-//     (coalesced over rows) and solved by one warp per right-hand side with
-//     shuffles (lane r holds z_r);
+//   - a block's diagonal 32 x 32 part of L is staged in shared memory
+//     (coalesced over rows; double-buffered: the next block's is staged
+//     while the current block's contribution is applied) and solved by one
+//     warp per right-hand side with shuffles (lane r holds z_r);
 //   - forward: the rows below take the block's contribution, one thread per
 //     row (loads coalesced over rows for each column of the block);
 //   - backward: the rows above take it, one thread per row (a row's 32
 //     entries are contiguous in its column of L).
-// idiag[kc] and blk[32 * 33] are shared scratch.  Replaces cuSOLVER potrs:
-// two library trsm launches of ~90 us each at these sizes, latency-bound.
+// Two block barriers per 32-row block.  idiag[kc] and blk[2 * 32 * 33] are
+// shared scratch.  Replaces cuSOLVER potrs, whose two trsm launches took
+// 90-450 us each at these sizes (latency-bound).
 __device__ void dev_trisolve_cm(const double* __restrict__ L, int kc, double* __restrict__ z,
                                 int nrhs, double* __restrict__ idiag, double* __restrict__ blk) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double* z0 = z;
   double* z1 = z + kc;
   for (int t = threadIdx.x; t < kc; t += blockDim.x) idiag[t] = 1.0 / L[(size_t)t * kc + t];
-  auto stage = [&](int j0, int bw) {  // blk[r * 33 + c] = L(j0 + r, j0 + c)
+  auto stage = [&](double* B, int j0, int bw) {  // B[r * 33 + c] = L(j0 + r, j0 + c)
     for (int e = threadIdx.x; e < 32 * 32; e += blockDim.x) {
       const int c = e >> 5, r = e & 31;
-      if (r < bw && c < bw) blk[r * 33 + c] = L[(size_t)(j0 + c) * kc + j0 + r];
+      if (r < bw && c < bw) B[r * 33 + c] = L[(size_t)(j0 + c) * kc + j0 + r];
     }
   };
-  for (int j0 = 0; j0 < kc; j0 += 32) {  // L y = z
-    const int bw = min(32, kc - j0);
-    stage(j0, bw);
-    __syncthreads();
+  const int nb = (kc + 31) / 32;
+  stage(blk, 0, min(32, kc));
+  __syncthreads();
+  for (int b = 0; b < nb; ++b) {  // L y = z
+    const int j0 = b * 32, bw = min(32, kc - j0);
+    const double* B = blk + (b & 1) * (32 * 33);
     if (warp < nrhs) {
       double* zc = z + (size_t)warp * kc;
       double zr = lane < bw ? zc[j0 + lane] : 0.0;
       for (int jj = 0; jj < bw; ++jj) {
         const double zj = __shfl_sync(0xffffffffu, zr, jj) * idiag[j0 + jj];
         if (lane == jj) zr = zj;
-        else if (lane > jj && lane < bw) zr = fma(-blk[lane * 33 + jj], zj, zr);
+        else if (lane > jj && lane < bw) zr = fma(-B[lane * 33 + jj], zj, zr);
       }
       if (lane < bw) zc[j0 + lane] = zr;
     }
     __syncthreads();
+    if (b + 1 < nb) stage(blk + ((b + 1) & 1) * (32 * 33), j0 + 32, min(32, kc - j0 - 32));
+    // (unrolled: the block's L loads of a row are independent and must be in
+    // flight together -- one at a time, each waited ~L2 latency)
     for (int i = j0 + bw + threadIdx.x; i < kc; i += blockDim.x) {
       double a0 = z0[i], a1 = nrhs > 1 ? z1[i] : 0.0;
+#pragma unroll 8
       for (int c = 0; c < bw; ++c) {
         const double l = L[(size_t)(j0 + c) * kc + i];
         a0 = fma(-l, z0[j0 + c], a0);
@@ -357,24 +365,32 @@ __device__ void dev_trisolve_cm(const double* __restrict__ L, int kc, double* __
     }
     __syncthreads();
   }
-  for (int j1 = kc; j1 > 0; j1 -= 32) {  // L^T x = y
-    const int j0 = max(0, j1 - 32), bw = j1 - j0;
-    stage(j0, bw);
-    __syncthreads();
+  // L^T x = y, blocks from the last; the last block's diagonal part is
+  // staged again into the buffer the forward sweep ends on
+  {
+    const int j0 = (nb - 1) * 32;
+    stage(blk + (nb & 1) * (32 * 33), j0, kc - j0);
+  }
+  __syncthreads();
+  for (int q = 0; q < nb; ++q) {
+    const int b = nb - 1 - q, j0 = b * 32, bw = min(32, kc - j0);
+    const double* B = blk + ((nb + q) & 1) * (32 * 33);
     if (warp < nrhs) {
       double* zc = z + (size_t)warp * kc;
       double zr = lane < bw ? zc[j0 + lane] : 0.0;
       for (int jj = bw - 1; jj >= 0; --jj) {
         const double zj = __shfl_sync(0xffffffffu, zr, jj) * idiag[j0 + jj];
         if (lane == jj) zr = zj;
-        else if (lane < jj) zr = fma(-blk[jj * 33 + lane], zj, zr);
+        else if (lane < jj) zr = fma(-B[jj * 33 + lane], zj, zr);
       }
       if (lane < bw) zc[j0 + lane] = zr;
     }
     __syncthreads();
+    if (b > 0) stage(blk + ((nb + q + 1) & 1) * (32 * 33), j0 - 32, 32);
     for (int j = threadIdx.x; j < j0; j += blockDim.x) {
       const double* Lj = L + (size_t)j * kc + j0;  // L(j0 + c, j)
       double a0 = z0[j], a1 = nrhs > 1 ? z1[j] : 0.0;
+#pragma unroll 8
       for (int c = 0; c < bw; ++c) {
         const double l = Lj[c];
         a0 = fma(-l, z0[j0 + c], a0);
@@ -407,7 +423,7 @@ __global__ void __launch_bounds__(kPeelThreads, kPeelMinBlocks) peel_forward_ker
   }
   double* z = tsm;                // [2 kc]
   double* idiag = tsm + 2 * kc;   // [kc]
-  double* blk = idiag + kc;       // [32 * 33]
+  double* blk = idiag + kc;       // [2 * 32 * 33]
   core_rhs_step(val, p, d, y, nrhs, H, kc, z);
   __syncthreads();
   dev_trisolve_cm(Lcm, kc, z, nrhs, idiag, blk);
@@ -662,6 +678,7 @@ __global__ void __launch_bounds__(kPeelThreads, kPeelMinBlocks) peel_fused_kerne
     for (int idx = threadIdx.x; idx < kc * kc; idx += blockDim.x) {
       const int t = idx / kc, t2 = idx - t * kc;
       double acc = (t == t2) ? d[p.snodes[t]] : 0.0;
+#pragma unroll 4
       for (int q = p.ccp[idx]; q < p.ccp[idx + 1]; ++q) acc -= W[p.cw[q]] * val[p.cq2[q]];
       S[(size_t)t * ld + t2] = acc;
     }
@@ -723,7 +740,7 @@ __global__ void __launch_bounds__(kPeelThreads, kPeelMinBlocks) peel_small_solve
   dev_backward(val, p, rounds, d, y, z, nrhs, H, kc, ke, x);
 }
 
-size_t tri_smem(int kc) { return ((size_t)3 * std::max(kc, 1) + 32 * 33) * sizeof(double); }
+size_t tri_smem(int kc) { return ((size_t)3 * std::max(kc, 1) + 2 * 32 * 33) * sizeof(double); }
 
 size_t small_smem(int kc) {
   return ((size_t)kc * core_ld(kc) + 3 * (size_t)std::max(kc, 1)) * sizeof(double);

@@ -26,7 +26,7 @@ namespace cg {
 constexpr int kPeelSmallCore = 160;
 // Largest core whose triangular solves with the potrf factor run inside the
 // single-CTA forward kernel (shared-memory right-hand sides) instead of potrs.
-constexpr int kPeelTriMax = 1024;
+constexpr int kPeelTriMax = 2048;
 // Largest core Schur complement assembled from host-planned contribution
 // lists (one thread per entry); larger ones use the row-wise assembly.
 constexpr int kPeelContribMax = 1024;
