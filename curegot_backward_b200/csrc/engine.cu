@@ -420,11 +420,20 @@ void bcd_loop(cg_engine_s* E, int cls) {
       }
     }
     // ---- staged problems whose copies have landed join the batch ------------
+    // A copy of at most kJoinWaitBytes lands within ~100 us: it is waited for
+    // here, so its problem joins the chunk about to start instead of the one
+    // after it (a chunk lasts ~1 ms); larger copies join when they land.
+    constexpr size_t kJoinWaitBytes = size_t(4) << 20;
     for (size_t k = 0; k < staging.size();) {
       const Staged sg = staging[k];
       if (sg.ev && cudaEventQuery(sg.ev) == cudaErrorNotReady) {
-        ++k;
-        continue;
+        const cg_request_t& r = sg.q->r;
+        const size_t bytes = (size_t)r.n * r.m * (r.m_f32 ? 4 : 8) + 8 * (size_t)(r.n + r.m);
+        if (bytes > kJoinWaitBytes) {
+          ++k;
+          continue;
+        }
+        while (cudaEventQuery(sg.ev) == cudaErrorNotReady) std::this_thread::yield();
       }
       staging.erase(staging.begin() + (long)k);
       const int rc = bcd_admit(E, sg.q, st, sg.ev);

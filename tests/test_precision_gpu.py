@@ -50,8 +50,8 @@ def test_bcd_mixed_fp64_errors(problem):
     assert niter < 100000
     row, col, _ = _oracle_errors(M, a, b, dual, eta)
     # the stopping rule: FP64 row-marginal error of the returned iterate
-    assert row <= 1e-8
-    assert col <= 1e-12
+    assert row <= 1e-8, (niter, row, col)
+    assert col <= 1e-12, (niter, row, col)
     # the torch FP64 evaluation used by the profiling case agrees with the oracle
     r2, c2 = fp64_marginal_errors(M, a, b, dual, eta)
     assert abs(r2 - row) <= 1e-12 and abs(c2 - col) <= 1e-12
